@@ -1,0 +1,189 @@
+"""Mesh generators: node / cell / face-node arrays fed to the face-connectivity builder.
+
+The structured generators produce exactly the arrays of the reference generators
+(node numbering, cell order, per-cell face node order, boundary dict order):
+  * quad_box_arrays      -- mesh/mesh_generator.py:13-93 (_make_structured_quad_mesh)
+  * tri_channel_arrays   -- mesh/mesh_generator.py:266-325
+  * hex_box_arrays       -- mesh/mesh_generator_3d.py:12-159 (generate_3d_channel_mesh)
+Synthetic generators for the workloads the reference has no generator for:
+  * jitter_interior      -- interior nodes displaced by U(-a, a) x spacing (seeded)
+  * delaunay_tri_arrays  -- Delaunay triangulation of uniform random points
+  * delaunay_tet_arrays  -- Delaunay tetrahedralisation of a jittered lattice
+Everything here is vectorised numpy; the meshes are built from these arrays by
+kcfd.mesh.build_mesh (native face discovery).
+"""
+from __future__ import annotations
+
+import numpy as np
+
+CAVITY_2D_NAMES = {"bottom": "wall_bottom", "top": "lid", "left": "wall_left", "right": "wall_right"}
+CHANNEL_2D_NAMES = {"bottom": "wall_bottom", "top": "wall_top", "left": "inlet", "right": "outlet"}
+CAVITY_3D_NAMES = {"x_min": "wall_left", "x_max": "wall_right", "y_min": "wall_bottom",
+                   "y_max": "lid", "z_min": "wall_front", "z_max": "wall_back"}
+CHANNEL_3D_NAMES = {"x_min": "inlet", "x_max": "outlet", "y_min": "wall_bottom",
+                    "y_max": "wall_top", "z_min": "wall_front", "z_max": "wall_back"}
+
+
+def quad_box_arrays(x0, y0, x1, y1, nx, ny, names=None):
+    """Structured quads; cells [n0,n1,n2,n3] counter-clockwise, j-major."""
+    names = names or {"bottom": "bottom", "top": "top", "left": "left", "right": "right"}
+    dx = (x1 - x0) / nx
+    dy = (y1 - y0) / ny
+    j, i = np.meshgrid(np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    nodes = np.stack([x0 + i.reshape(-1) * dx, y0 + j.reshape(-1) * dy], axis=1)
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    n0 = (jj * (nx + 1) + ii).reshape(-1)
+    cells = np.stack([n0, n0 + 1, n0 + 1 + (nx + 1), n0 + (nx + 1)], axis=1)
+    ar = np.arange(nx)
+    bd = {}
+    bd[names.get("bottom", "bottom")] = list(np.stack([ar, ar + 1], 1))
+    top0 = ny * (nx + 1) + ar
+    bd[names.get("top", "top")] = list(np.stack([top0, top0 + 1], 1))
+    aj = np.arange(ny)
+    bd[names.get("left", "left")] = list(np.stack([aj * (nx + 1), (aj + 1) * (nx + 1)], 1))
+    bd[names.get("right", "right")] = list(np.stack([aj * (nx + 1) + nx, (aj + 1) * (nx + 1) + nx], 1))
+    return nodes, cells, bd
+
+
+def tri_channel_arrays(Lx, Ly, nx, ny):
+    """Quads split along n0-n2 into (n0,n1,n2) and (n0,n2,n3)."""
+    def nid(i, j):
+        return j * (nx + 1) + i
+    dx, dy = Lx / nx, Ly / ny
+    j, i = np.meshgrid(np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    nodes = np.stack([i.reshape(-1) * dx, j.reshape(-1) * dy], axis=1)
+    jj, ii = np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij")
+    jj, ii = jj.reshape(-1), ii.reshape(-1)
+    n0, n1, n2, n3 = nid(ii, jj), nid(ii + 1, jj), nid(ii + 1, jj + 1), nid(ii, jj + 1)
+    cells = np.stack([np.stack([n0, n1, n2], 1), np.stack([n0, n2, n3], 1)], axis=1).reshape(-1, 3)
+    aj, ai = np.arange(ny), np.arange(nx)
+    bd = {"inlet": list(np.stack([nid(0, aj), nid(0, aj + 1)], 1)),
+          "outlet": list(np.stack([nid(nx, aj), nid(nx, aj + 1)], 1)),
+          "wall_bottom": list(np.stack([nid(ai, 0), nid(ai + 1, 0)], 1)),
+          "wall_top": list(np.stack([nid(ai, ny), nid(ai + 1, ny)], 1))}
+    return nodes, cells, bd
+
+
+def hex_box_arrays(Lx, Ly, Lz, nx, ny, nz, names=None):
+    """Structured hexes (k, j, i order), six faces per cell in the reference order."""
+    names = names or CHANNEL_3D_NAMES
+    dx, dy, dz = Lx / nx, Ly / ny, Lz / nz
+
+    def nid(i, j, k):
+        return k * (ny + 1) * (nx + 1) + j * (nx + 1) + i
+
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    nodes = np.stack([i.reshape(-1) * dx, j.reshape(-1) * dy, k.reshape(-1) * dz], axis=1)
+    kk, jj, ii = (a.reshape(-1) for a in np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij"))
+    n0, n1, n2, n3 = nid(ii, jj, kk), nid(ii + 1, jj, kk), nid(ii + 1, jj + 1, kk), nid(ii, jj + 1, kk)
+    n4, n5, n6, n7 = nid(ii, jj, kk + 1), nid(ii + 1, jj, kk + 1), nid(ii + 1, jj + 1, kk + 1), nid(ii, jj + 1, kk + 1)
+    cells = np.stack([n0, n1, n2, n3, n4, n5, n6, n7], axis=1)
+    cfaces = np.stack([np.stack([n0, n3, n2, n1], 1), np.stack([n4, n5, n6, n7], 1),
+                       np.stack([n0, n1, n5, n4], 1), np.stack([n2, n3, n7, n6], 1),
+                       np.stack([n0, n4, n7, n3], 1), np.stack([n1, n2, n6, n5], 1)], axis=1)
+    bd = {}
+    K, J = (a.reshape(-1) for a in np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij"))
+    bd[names.get("x_min", "inlet")] = np.stack([nid(0, J, K), nid(0, J, K + 1), nid(0, J + 1, K + 1), nid(0, J + 1, K)], 1)
+    bd[names.get("x_max", "outlet")] = np.stack([nid(nx, J, K), nid(nx, J + 1, K), nid(nx, J + 1, K + 1), nid(nx, J, K + 1)], 1)
+    K, I = (a.reshape(-1) for a in np.meshgrid(np.arange(nz), np.arange(nx), indexing="ij"))
+    bd[names.get("y_min", "wall_bottom")] = np.stack([nid(I, 0, K), nid(I + 1, 0, K), nid(I + 1, 0, K + 1), nid(I, 0, K + 1)], 1)
+    bd[names.get("y_max", "wall_top")] = np.stack([nid(I + 1, ny, K), nid(I, ny, K), nid(I, ny, K + 1), nid(I + 1, ny, K + 1)], 1)
+    J, I = (a.reshape(-1) for a in np.meshgrid(np.arange(ny), np.arange(nx), indexing="ij"))
+    bd[names.get("z_min", "wall_front")] = np.stack([nid(I, J, 0), nid(I, J + 1, 0), nid(I + 1, J + 1, 0), nid(I + 1, J, 0)], 1)
+    bd[names.get("z_max", "wall_back")] = np.stack([nid(I, J, nz), nid(I + 1, J, nz), nid(I + 1, J + 1, nz), nid(I, J + 1, nz)], 1)
+    return nodes, cells, cfaces, bd
+
+
+def jitter_interior(nodes, shape, spacing, amp=0.2, seed=0):
+    """Displace nodes not on any boundary plane by U(-amp, amp) x spacing per axis.
+
+    shape = (nx, ny[, nz]) cell counts; nodes are numbered i fastest. The draw covers
+    every node (rng.uniform(-amp, amp, (n_nodes, ndim))) so the field is a function of
+    the seed and the lattice only.
+    """
+    ndim = len(shape)
+    rng = np.random.default_rng(seed)
+    disp = rng.uniform(-amp, amp, (len(nodes), ndim)) * np.asarray(spacing)[None, :]
+    grids = np.meshgrid(*[np.arange(s + 1) for s in reversed(shape)], indexing="ij")
+    idx = [g.reshape(-1) for g in reversed(grids)]  # i, j, k per node
+    interior = np.ones(len(nodes), dtype=bool)
+    for a, s in zip(idx, shape):
+        interior &= (a > 0) & (a < s)
+    out = nodes.copy()
+    out[interior] += disp[interior]
+    return out
+
+
+def _morton_order(pts):
+    """Cell order along a Morton curve of the centroids (locality for gathers)."""
+    lo, hi = pts.min(0), pts.max(0)
+    q = ((pts - lo) / np.maximum(hi - lo, 1e-300) * 1023.0).astype(np.int64)
+    code = np.zeros(len(pts), dtype=np.int64)
+    for bit in range(10):
+        for d in range(pts.shape[1]):
+            code |= ((q[:, d] >> bit) & 1) << (bit * pts.shape[1] + d)
+    return np.argsort(code, kind="stable")
+
+
+def delaunay_tri_arrays(n_points, rng, dirichlet_name="dirichlet", wall_name="wall"):
+    """Delaunay triangles of n_points uniform points in the unit square plus its corners.
+
+    Cells are ordered along a Morton curve of their centroids. Boundary edges are
+    the convex hull; hull edges whose midpoint has x < 1e-9 form the Dirichlet
+    segment, the rest the wall patch.
+    """
+    from scipy.spatial import Delaunay
+    pts = np.vstack([rng.uniform(0.0, 1.0, (n_points, 2)), [[0, 0], [1, 0], [1, 1], [0, 1]]])
+    tri = Delaunay(pts)
+    cells = tri.simplices.astype(np.int64)
+    order = _morton_order(pts[cells].mean(axis=1))
+    cells = cells[order]
+    hull = tri.convex_hull.astype(np.int64)
+    mid_x = pts[hull].mean(axis=1)[:, 0]
+    left = mid_x < 1e-9
+    bd = {dirichlet_name: list(hull[left]), wall_name: list(hull[~left])}
+    return pts, cells, bd
+
+
+def delaunay_tet_arrays(box, n_target, rng, jitter=0.25):
+    """Delaunay tetrahedra of a jittered lattice in box = (Lx, Ly, Lz).
+
+    The lattice spacing is chosen so that the tetrahedralisation has about n_target
+    cells (a Delaunay mesh of a jittered lattice has ~5.2-6 tets per point).
+    Face node lists follow the reference's tet face order (_tet_faces in
+    mesh/hybrid_mesh_generator.py:64-72); cells are ordered along a Morton curve.
+    Boundary faces are the convex hull, tagged by face-centroid position: bottom
+    (z = 0) 'inlet_gas', top (z = Lz) 'outlet', the rest 'wall'.
+    """
+    from scipy.spatial import Delaunay
+    Lx, Ly, Lz = box
+    vol = Lx * Ly * Lz
+    n_pts = n_target / 5.6
+    h = (vol / n_pts) ** (1.0 / 3.0)
+    nx, ny, nz = max(2, round(Lx / h)), max(2, round(Ly / h)), max(2, round(Lz / h))
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    sp = np.array([Lx / nx, Ly / ny, Lz / nz])
+    pts = np.stack([i.reshape(-1) * sp[0], j.reshape(-1) * sp[1], k.reshape(-1) * sp[2]], axis=1)
+    pts = jitter_interior(pts, (nx, ny, nz), sp, amp=jitter, seed=int(rng.integers(0, 2**31)))
+    tet = Delaunay(pts, qhull_options="Qbb Qc Qz Q12")
+    cells = tet.simplices.astype(np.int64)
+    # drop slivers of (near) zero volume that Qhull can leave on a lattice
+    p = pts[cells]
+    v6 = np.abs(np.einsum("ij,ij->i", p[:, 1] - p[:, 0], np.cross(p[:, 2] - p[:, 0], p[:, 3] - p[:, 0])))
+    cells = cells[v6 > 1e-12 * sp.prod()]
+    order = _morton_order(pts[cells].mean(axis=1))
+    cells = cells[order]
+    n0, n1, n2, n3 = cells[:, 0], cells[:, 1], cells[:, 2], cells[:, 3]
+    cfaces = np.stack([np.stack([n0, n2, n1], 1), np.stack([n0, n1, n3], 1),
+                       np.stack([n1, n2, n3], 1), np.stack([n0, n3, n2], 1)], axis=1)
+    # boundary = faces used once
+    allf = np.sort(cfaces.reshape(-1, 3), axis=1)
+    key = (allf[:, 0] * (len(pts) + 1) + allf[:, 1]) * (len(pts) + 1) + allf[:, 2]
+    uk, inv, cnt = np.unique(key, return_inverse=True, return_counts=True)
+    once = cnt[inv] == 1
+    bf = cfaces.reshape(-1, 3)[once]
+    zc = pts[bf][:, :, 2].mean(axis=1)
+    bd = {"inlet_gas": list(bf[zc < 1e-9 * Lz + 1e-12]), "outlet": list(bf[zc > Lz * (1 - 1e-9) - 1e-12])}
+    rest = ~((zc < 1e-9 * Lz + 1e-12) | (zc > Lz * (1 - 1e-9) - 1e-12))
+    bd["wall"] = list(bf[rest])
+    return pts, cells, cfaces, bd

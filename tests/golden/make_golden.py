@@ -1,0 +1,296 @@
+"""Generate the golden fixtures in tests/golden/ by running the K-CFD reference itself.
+
+Run in a container that holds the reference checkout (it is read, never modified):
+
+    python tests/golden/make_golden.py [--ref /root/reference]
+
+The reference is pure Python. Its mesh package imports ``gmsh`` at module level
+without using it (mesh/mesh_generator.py:8), and its verification cases import
+matplotlib for plotting only, so both are replaced by empty stub modules before
+the import. Every fixture is small (kilobytes) and is written with
+numpy.savez_compressed; tests/test_oracle_golden.py checks the oracle against
+them and the GPU tests reuse the generator inputs recorded here.
+"""
+from __future__ import annotations
+
+import argparse
+import os
+import sys
+import types
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+
+
+def _install_stubs():
+    sys.modules.setdefault("gmsh", types.ModuleType("gmsh"))
+    mpl = types.ModuleType("matplotlib")
+    mpl.use = lambda *a, **k: None
+    plt = types.ModuleType("matplotlib.pyplot")
+    mpl.pyplot = plt
+    sys.modules["matplotlib"] = mpl
+    sys.modules["matplotlib.pyplot"] = plt
+    pc = types.ModuleType("verification.plot_config")
+    pc._FONT_NAME = None
+    sys.modules["verification.plot_config"] = pc
+
+
+def _mesh_arrays(mesh, prefix=""):
+    F = mesh.n_faces
+    ndim = mesh.ndim
+    names = list(mesh.boundary_patches.keys())
+    ptr = [0]
+    fids = []
+    for nm in names:
+        fids.extend(mesh.boundary_patches[nm])
+        ptr.append(len(fids))
+    kmax = max(len(c.faces) for c in mesh.cells)
+    cf = -np.ones((mesh.n_cells, kmax), dtype=np.int64)
+    for ci, c in enumerate(mesh.cells):
+        cf[ci, :len(c.faces)] = c.faces
+    return {
+        prefix + "ndim": np.int64(ndim),
+        prefix + "owner": np.array([f.owner for f in mesh.faces], dtype=np.int64),
+        prefix + "neighbour": np.array([f.neighbour for f in mesh.faces], dtype=np.int64),
+        prefix + "area": np.array([f.area for f in mesh.faces]),
+        prefix + "normal": np.array([np.asarray(f.normal)[:ndim] for f in mesh.faces]).reshape(F, ndim),
+        prefix + "fcenter": np.array([np.asarray(f.center)[:ndim] for f in mesh.faces]).reshape(F, ndim),
+        prefix + "ccenter": np.array([np.asarray(c.center)[:ndim] for c in mesh.cells]),
+        prefix + "volume": np.array([c.volume for c in mesh.cells]),
+        prefix + "cell_faces": cf,
+        prefix + "patch_names": np.array(names),
+        prefix + "patch_ptr": np.array(ptr, dtype=np.int64),
+        prefix + "patch_fids": np.array(fids, dtype=np.int64),
+    }
+
+
+class _Recorder:
+    """Wraps build_fvmesh_from_arrays to record the generator's inputs."""
+
+    def __init__(self, real):
+        self.real = real
+        self.calls = []
+
+    def __call__(self, node_coords, cell_node_list, boundary_faces_dict, cell_zone_map=None,
+                 ndim=2, cell_face_node_list=None):
+        self.calls.append((np.array(node_coords), [np.asarray(c) for c in cell_node_list],
+                           {k: [np.asarray(f) for f in v] for k, v in boundary_faces_dict.items()},
+                           ndim, None if cell_face_node_list is None else
+                           [[np.asarray(f) for f in fl] for fl in cell_face_node_list]))
+        return self.real(node_coords, cell_node_list, boundary_faces_dict, cell_zone_map=cell_zone_map,
+                         ndim=ndim, cell_face_node_list=cell_face_node_list)
+
+
+def _inputs_arrays(call, prefix="in_"):
+    nodes, cells, bdict, ndim, cfl = call
+    out = {prefix + "nodes": nodes}
+    lens = np.array([len(c) for c in cells], dtype=np.int64)
+    out[prefix + "cell_ptr"] = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+    out[prefix + "cell_nodes"] = np.concatenate(cells).astype(np.int64)
+    names = list(bdict.keys())
+    out[prefix + "bnames"] = np.array(names)
+    bl = [len(bdict[k]) for k in names]
+    out[prefix + "bptr"] = np.concatenate([[0], np.cumsum(bl)]).astype(np.int64)
+    bf = [f for k in names for f in bdict[k]]
+    out[prefix + "bface_len"] = np.array([len(f) for f in bf], dtype=np.int64)
+    out[prefix + "bface_nodes"] = np.concatenate(bf).astype(np.int64) if bf else np.zeros(0, np.int64)
+    if cfl is not None:
+        nf = np.array([len(fl) for fl in cfl], dtype=np.int64)
+        out[prefix + "cface_ptr"] = np.concatenate([[0], np.cumsum(nf)]).astype(np.int64)
+        flat = [f for fl in cfl for f in fl]
+        out[prefix + "face_len"] = np.array([len(f) for f in flat], dtype=np.int64)
+        out[prefix + "face_nodes"] = np.concatenate(flat).astype(np.int64)
+    return out
+
+
+def _system_arrays(system, prefix):
+    A = system.to_sparse()
+    A.sort_indices()
+    return {prefix + "indptr": A.indptr.astype(np.int64), prefix + "indices": A.indices.astype(np.int64),
+            prefix + "data": A.data.copy(), prefix + "rhs": system.rhs.copy(), prefix + "diag": system.diag.copy()}
+
+
+def make_meshes(out):
+    import mesh.mesh_generator as mg
+    import mesh.mesh_generator_3d as mg3
+    import mesh.hybrid_mesh_generator as mgh
+    rec = _Recorder(mg.build_fvmesh_from_arrays)
+    mg.build_fvmesh_from_arrays = rec
+    mg3.build_fvmesh_from_arrays = rec
+    mgh.build_fvmesh_from_arrays = rec
+    cases = {
+        "quad": lambda: mg.generate_channel_mesh(1.0, 0.6, 6, 5),
+        "cavity": lambda: mg.generate_cavity_mesh(1.0, 8),
+        "tri": lambda: mg.generate_triangle_channel_mesh(1.0, 0.5, 5, 3),
+        "hex": lambda: mg3.generate_3d_cavity_mesh(1.0, 0.9, 0.8, 4, 3, 2),
+        "hybrid": lambda: mgh.generate_hybrid_hex_tet_mesh(1.0, 0.5, 0.5, 4, 2, 2, 0.5),
+    }
+    meshes = {}
+    for name, fn in cases.items():
+        rec.calls.clear()
+        m = fn()
+        meshes[name] = m
+        d = _mesh_arrays(m)
+        d.update(_inputs_arrays(rec.calls[0]))
+        np.savez_compressed(os.path.join(out, f"mesh_{name}.npz"), **d)
+    return meshes
+
+
+def make_operators(out, meshes):
+    from core.fields import ScalarField, VectorField
+    from core.fvm_operators import (FVMSystem, diffusion_operator, convection_operator_upwind,
+                                    temporal_operator, source_term, linearized_source,
+                                    apply_boundary_conditions, under_relax)
+    from core.gradient import green_gauss_gradient
+    from core.interpolation import compute_mass_flux, muscl_deferred_correction
+    for name in ("quad", "tri", "hex", "hybrid"):
+        m = meshes[name]
+        rng = np.random.default_rng(1234)
+        n, F, ndim = m.n_cells, m.n_faces, m.ndim
+        d = {}
+        gamma = ScalarField(m, "gamma")
+        gamma.values = rng.uniform(0.1, 2.0, n)
+        phi = ScalarField(m, "phi")
+        phi.values = rng.normal(size=n)
+        for bn in phi.boundary_values:
+            phi.boundary_values[bn] = rng.normal(size=len(phi.boundary_values[bn]))
+        U = VectorField(m, "U")
+        U.values = rng.normal(size=(n, ndim))
+        for bn in U.boundary_values:
+            U.boundary_values[bn] = rng.normal(size=U.boundary_values[bn].shape)
+        mf = rng.normal(size=F)
+        phi_old = rng.normal(size=n)
+        S = rng.normal(size=n)
+        Sp = -rng.uniform(0.0, 1.0, n)
+        Su = rng.normal(size=n)
+        d["gamma"], d["phi"], d["U"], d["mf"] = gamma.values, phi.values, U.values, mf
+        d["phi_old"], d["S"], d["Sp"], d["Su"] = phi_old, S, Sp, Su
+        names = list(m.boundary_patches.keys())
+        d["phi_b"] = np.concatenate([phi.boundary_values[k] for k in names])
+        d["U_b"] = np.concatenate([U.boundary_values[k] for k in names])
+        # boundary condition mix: patch i -> dirichlet / zero_gradient / neumann cyclically
+        kinds = ["dirichlet", "zero_gradient", "neumann"]
+        bc = {}
+        for i, k in enumerate(names):
+            t = kinds[i % 3]
+            bc[k] = {"type": t, "value": 0.37 * (i + 1)} if t == "neumann" else {"type": t}
+        d["bc_kind"] = np.array([bc[k]["type"] for k in names])
+        d["bc_value"] = np.array([bc[k].get("value", 0.0) for k in names])
+        s = FVMSystem(n); diffusion_operator(m, gamma, s); d.update(_system_arrays(s, "diff_"))
+        s = FVMSystem(n); convection_operator_upwind(m, mf, s); d.update(_system_arrays(s, "conv_"))
+        s = FVMSystem(n); temporal_operator(m, 1.3, 0.01, phi_old, s); d.update(_system_arrays(s, "temp_"))
+        s = FVMSystem(n); source_term(m, S, s); d["src_rhs"] = s.rhs.copy()
+        s = FVMSystem(n); linearized_source(m, Sp, Su, s); d.update(_system_arrays(s, "lin_"))
+        s = FVMSystem(n); apply_boundary_conditions(m, phi, gamma, mf, s, bc); d.update(_system_arrays(s, "bc_"))
+        # a full transport system in the two-fluid order, then under-relaxation
+        s = FVMSystem(n)
+        diffusion_operator(m, gamma, s)
+        convection_operator_upwind(m, mf, s)
+        temporal_operator(m, 1.3, 0.01, phi_old, s)
+        apply_boundary_conditions(m, phi, gamma, mf, s, bc)
+        under_relax(s, phi, 0.7)
+        d.update(_system_arrays(s, "full_"))
+        d["gg"] = green_gauss_gradient(phi)
+        d["mflux"] = compute_mass_flux(U, 1.7, m)
+        for lim in ("minmod", "superbee", "van_albada", "van_leer"):
+            d["muscl_" + lim] = muscl_deferred_correction(m, phi, mf, d["gg"], lim)
+        np.savez_compressed(os.path.join(out, f"ops_{name}.npz"), **d)
+
+
+def make_solvers(out):
+    import scipy.sparse.linalg as spla
+    from core.gpu_solver import _cpu_bicgstab
+    from core.preconditioner import create_preconditioner
+    from verification.case16_preconditioner import _build_convdiff_system
+    from mesh.mesh_generator import generate_channel_mesh
+    d = {}
+    for nx in (20, 80):
+        m = generate_channel_mesh(1.0, 1.0, nx, nx)
+        s = _build_convdiff_system(m, gamma_val=0.01, u_conv=1.0)
+        A = s.to_sparse()
+        b = s.rhs.copy()
+        p = f"c16_{nx}_"
+        if nx == 20:
+            A.sort_indices()
+            d[p + "indptr"], d[p + "indices"], d[p + "data"], d[p + "rhs"] = A.indptr, A.indices, A.data, b
+        d[p + "direct"] = spla.spsolve(A.tocsc(), b)
+        # the reference's case 16 call: bicgstab(atol=1e-10, rtol=0) per preconditioner
+        # (verification/case16_preconditioner.py:170-173)
+        for pc in ("none", "jacobi", "ilu0"):
+            M, _ = create_preconditioner(A, pc)
+            cnt = [0]
+
+            def cb(xk):
+                cnt[0] += 1
+
+            x, info = spla.bicgstab(A, b, x0=np.zeros(len(b)), atol=1e-10, rtol=0.0, maxiter=2000, M=M,
+                                    callback=cb)
+            d[p + pc + "_iters"] = np.int64(cnt[0])
+            d[p + pc + "_info"] = np.int64(info)
+            d[p + pc + "_x"] = x
+    # the incumbent GPU path's algorithm (core/gpu_solver.py:158-199) on the 20x20 system
+    m = generate_channel_mesh(1.0, 1.0, 20, 20)
+    s = _build_convdiff_system(m, gamma_val=0.01, u_conv=1.0)
+    A = s.to_sparse()
+
+    class Counting:
+        def __init__(self, A):
+            self.A, self.n = A, 0
+
+        def __matmul__(self, x):
+            self.n += 1
+            return self.A @ x
+
+    for tol in (1e-6, 1e-10):
+        C = Counting(A)
+        x = _cpu_bicgstab(C, s.rhs.copy(), None, tol, 1000)
+        d[f"gpu_{tol:.0e}_x"] = x
+        d[f"gpu_{tol:.0e}_matvecs"] = np.int64(C.n)
+    np.savez_compressed(os.path.join(out, "solvers.npz"), **d)
+
+
+def make_simple(out):
+    from mesh.mesh_generator import generate_cavity_mesh
+    from mesh.mesh_generator_3d import generate_3d_cavity_mesh
+    from models.single_phase import SIMPLESolver
+    import contextlib
+    import io
+    d = {}
+    for tag, mk, mu, iters in (("2d", lambda: generate_cavity_mesh(1.0, 8), 0.01, 20),
+                               ("3d", lambda: generate_3d_cavity_mesh(1, 1, 1, 3, 3, 3), 0.01, 6)):
+        m = mk()
+        sv = SIMPLESolver(m, rho=1.0, mu=mu)
+        ndim = m.ndim
+        for pname in m.boundary_patches:
+            if pname == "lid":
+                sv.set_velocity_bc(pname, "dirichlet", [1.0] + [0.0] * (ndim - 1))
+            else:
+                sv.set_velocity_bc(pname, "dirichlet", [0.0] * ndim)
+            sv.set_pressure_bc(pname, "zero_gradient")
+        sv.alpha_u, sv.alpha_p, sv.max_outer_iter, sv.tol = 0.7, 0.3, iters, 0.0
+        with contextlib.redirect_stdout(io.StringIO()):
+            r = sv.solve_steady()
+        d[tag + "_U"] = sv.U.values.copy()
+        d[tag + "_p"] = sv.p.values.copy()
+        d[tag + "_res"] = np.array(r["residuals"])
+        d[tag + "_iters"] = np.int64(iters)
+    np.savez_compressed(os.path.join(out, "simple.npz"), **d)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--out", default=HERE)
+    a = ap.parse_args()
+    _install_stubs()
+    sys.path.insert(0, a.ref)
+    meshes = make_meshes(a.out)
+    make_operators(a.out, meshes)
+    make_solvers(a.out)
+    make_simple(a.out)
+    print("golden fixtures written to", a.out)
+
+
+if __name__ == "__main__":
+    main()

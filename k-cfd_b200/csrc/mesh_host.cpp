@@ -1,0 +1,519 @@
+// Host-side mesh builder of libkcfd: face discovery, geometry, boundary tagging,
+// canonical CSR pattern, face -> CSR slot map, face and cell colourings.
+//
+// Semantics follow the K-CFD reference builder (mesh/mesh_reader.py):
+//  * a face id is the rank of the face's first discovery while cells are visited in
+//    order and, per cell, edges (2D, :189-214) or the given face lists (3D, :269-290);
+//    owner = first cell, neighbour = the last later cell;
+//  * 2D geometry :66-78 and :102-113, 3D geometry :81-99 and :116-138 (node-mean
+//    centres, Newell normals, divergence-theorem volumes), with the reference's
+//    operation order so results agree to the last bit;
+//  * boundary tagging :216-231 / :298-313 (last patch assignment of a key wins).
+// Face discovery uses an open-addressing hash of the sorted node tuple (<= 4 nodes,
+// node ids < 2^32), so the whole build is one pass over the cell faces.
+#include <algorithm>
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <mutex>
+#include <vector>
+
+#include "kcfd_common.h"
+
+namespace kcfd {
+
+static thread_local std::string g_err;
+void set_error(const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_err = buf;
+}
+const std::string& last_error() { return g_err; }
+
+namespace {
+
+struct Key {
+    uint64_t hi, lo;
+    bool operator==(const Key& o) const { return hi == o.hi && lo == o.lo; }
+};
+
+inline uint64_t mix(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdULL;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ULL;
+    x ^= x >> 33;
+    return x;
+}
+
+// Sorted node tuple (k <= 4 nodes, ids < 2^32) packed in 128 bits; unused slots are
+// 0xffffffff so faces of different sizes never collide.
+inline Key make_key(const int64_t* nodes, int k) {
+    uint32_t v[4] = {0xffffffffu, 0xffffffffu, 0xffffffffu, 0xffffffffu};
+    for (int i = 0; i < k; ++i) v[i] = (uint32_t)nodes[i];
+    std::sort(v, v + k);
+    Key key;
+    key.hi = ((uint64_t)v[0] << 32) | v[1];
+    key.lo = ((uint64_t)v[2] << 32) | v[3];
+    return key;
+}
+
+class KeyTable {
+   public:
+    explicit KeyTable(size_t n_expected) {
+        size_t cap = 16;
+        while (cap < 2 * n_expected + 16) cap <<= 1;
+        mask_ = cap - 1;
+        keys_.resize(cap);
+        vals_.assign(cap, -1);
+    }
+    // Returns the slot; *found tells whether the key was present.
+    size_t find_or_insert(const Key& k, bool* found) {
+        size_t h = (size_t)(mix(k.hi ^ mix(k.lo))) & mask_;
+        while (true) {
+            if (vals_[h] < 0) {
+                keys_[h] = k;
+                *found = false;
+                return h;
+            }
+            if (keys_[h] == k) {
+                *found = true;
+                return h;
+            }
+            h = (h + 1) & mask_;
+        }
+    }
+    int64_t& val(size_t slot) { return vals_[slot]; }
+    int64_t lookup(const Key& k) const {
+        size_t h = (size_t)(mix(k.hi ^ mix(k.lo))) & mask_;
+        while (true) {
+            if (vals_[h] < 0) return -1;
+            if (keys_[h] == k) return vals_[h];
+            h = (h + 1) & mask_;
+        }
+    }
+
+   private:
+    size_t mask_;
+    std::vector<Key> keys_;
+    std::vector<int64_t> vals_;
+};
+
+}  // namespace
+}  // namespace kcfd
+
+struct kcfd_host_mesh {
+    int ndim = 2;
+    int64_t n_cells = 0, n_faces = 0, n_internal = 0, nnz = 0;
+    int max_face_nodes = 2, max_cell_faces = 0;
+    int n_int_colors = 0, n_bnd_colors = 0, n_cell_colors = 0, n_levels = 0;
+    std::vector<int64_t> owner, neighbour, face_nodes, cell_faces;
+    std::vector<double> area, normal, fcenter, ccenter, volume;
+    std::vector<int32_t> face_patch, indptr, indices, slot_on, slot_no, diag_slot;
+    std::vector<int32_t> face_color, cell_color, level_natural;
+};
+
+using kcfd::Key;
+using kcfd::make_key;
+using kcfd::KeyTable;
+
+namespace {
+
+void build_pattern(kcfd_host_mesh* m) {
+    const int64_t n = m->n_cells, F = m->n_faces;
+    std::vector<int64_t> cnt(n + 1, 0);
+    for (int64_t i = 0; i < n; ++i) cnt[i + 1] += 1;
+    for (int64_t f = 0; f < F; ++f)
+        if (m->neighbour[f] >= 0) {
+            cnt[m->owner[f] + 1] += 1;
+            cnt[m->neighbour[f] + 1] += 1;
+        }
+    for (int64_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
+    std::vector<int32_t> cols(cnt[n]);
+    std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
+    for (int64_t i = 0; i < n; ++i) cols[pos[i]++] = (int32_t)i;
+    for (int64_t f = 0; f < F; ++f)
+        if (m->neighbour[f] >= 0) {
+            int64_t o = m->owner[f], nb = m->neighbour[f];
+            cols[pos[o]++] = (int32_t)nb;
+            cols[pos[nb]++] = (int32_t)o;
+        }
+    m->indptr.assign(n + 1, 0);
+    m->indices.clear();
+    m->indices.reserve(cols.size());
+    for (int64_t i = 0; i < n; ++i) {
+        auto b = cols.begin() + cnt[i], e = cols.begin() + cnt[i + 1];
+        std::sort(b, e);
+        auto u = std::unique(b, e);
+        m->indices.insert(m->indices.end(), b, u);
+        m->indptr[i + 1] = (int32_t)m->indices.size();
+    }
+    m->nnz = (int64_t)m->indices.size();
+    auto slot = [&](int64_t r, int64_t c) -> int32_t {
+        auto b = m->indices.begin() + m->indptr[r], e = m->indices.begin() + m->indptr[r + 1];
+        auto it = std::lower_bound(b, e, (int32_t)c);
+        return (int32_t)(it - m->indices.begin());
+    };
+    m->diag_slot.resize(n);
+    for (int64_t i = 0; i < n; ++i) m->diag_slot[i] = slot(i, i);
+    m->slot_on.assign(F, -1);
+    m->slot_no.assign(F, -1);
+    for (int64_t f = 0; f < F; ++f)
+        if (m->neighbour[f] >= 0) {
+            m->slot_on[f] = slot(m->owner[f], m->neighbour[f]);
+            m->slot_no[f] = slot(m->neighbour[f], m->owner[f]);
+        }
+}
+
+// Greedy edge colouring of internal faces in face order (no two faces of a colour
+// share a cell), and per-owner counting colours for boundary faces.
+int color_faces(kcfd_host_mesh* m) {
+    const int64_t n = m->n_cells, F = m->n_faces;
+    std::vector<uint64_t> used(n, 0);
+    m->face_color.assign(F, -1);
+    int ci = 0;
+    for (int64_t f = 0; f < F; ++f) {
+        if (m->neighbour[f] < 0) continue;
+        uint64_t u = used[m->owner[f]] | used[m->neighbour[f]];
+        if (~u == 0) return -1;
+        int c = __builtin_ctzll(~u);
+        used[m->owner[f]] |= 1ULL << c;
+        used[m->neighbour[f]] |= 1ULL << c;
+        m->face_color[f] = c;
+        ci = std::max(ci, c + 1);
+    }
+    std::vector<int32_t> nb(n, 0);
+    int cb = 0;
+    for (int64_t f = 0; f < F; ++f) {
+        if (m->neighbour[f] >= 0) continue;
+        int c = nb[m->owner[f]]++;
+        m->face_color[f] = ci + c;
+        cb = std::max(cb, c + 1);
+    }
+    m->n_int_colors = ci;
+    m->n_bnd_colors = cb;
+    return 0;
+}
+
+void color_cells_and_levels(kcfd_host_mesh* m) {
+    const int64_t n = m->n_cells;
+    m->cell_color.assign(n, -1);
+    m->level_natural.assign(n, 0);
+    int nc = 0, nl = 0;
+    std::vector<char> seen;
+    for (int64_t i = 0; i < n; ++i) {
+        seen.assign(nc + 1, 0);
+        int lev = 0;
+        for (int32_t k = m->indptr[i]; k < m->indptr[i + 1]; ++k) {
+            int32_t j = m->indices[k];
+            if (j == i) continue;
+            if (m->cell_color[j] >= 0) seen[m->cell_color[j]] = 1;
+            if (j < i) lev = std::max(lev, m->level_natural[j] + 1);
+        }
+        int c = 0;
+        while (c < nc && seen[c]) ++c;
+        m->cell_color[i] = c;
+        nc = std::max(nc, c + 1);
+        m->level_natural[i] = lev;
+        nl = std::max(nl, lev + 1);
+    }
+    m->n_cell_colors = nc;
+    m->n_levels = nl;
+}
+
+}  // namespace
+
+extern "C" {
+
+int kcfd_mesh_build(int32_t ndim, int64_t n_nodes, const double* nodes, int64_t n_cells,
+                    const int64_t* cell_ptr, const int64_t* cell_nodes, const int64_t* cface_ptr,
+                    const int64_t* cface_len, const int64_t* cface_off, const int64_t* cface_nodes,
+                    int64_t n_bfaces, const int64_t* bface_len, const int64_t* bface_nodes,
+                    const int32_t* bface_patch, kcfd_host_mesh** out) {
+    KCFD_REQUIRE(out != nullptr, "kcfd_mesh_build: out is NULL");
+    *out = nullptr;
+    KCFD_REQUIRE(ndim == 2 || ndim == 3, "kcfd_mesh_build: ndim must be 2 or 3 (got %d)", ndim);
+    KCFD_REQUIRE(n_nodes > 0 && n_nodes < 0xffffffffLL, "kcfd_mesh_build: bad n_nodes %lld", (long long)n_nodes);
+    KCFD_REQUIRE(n_cells > 0 && n_cells < 0x7fffffffLL, "kcfd_mesh_build: bad n_cells %lld", (long long)n_cells);
+    KCFD_REQUIRE(nodes && cell_ptr && cell_nodes, "kcfd_mesh_build: NULL node/cell arrays");
+    const bool is3d = (ndim == 3 && cface_ptr != nullptr);
+    if (ndim == 3) KCFD_REQUIRE(cface_ptr && cface_len && cface_off && cface_nodes, "kcfd_mesh_build: 3D needs cell face lists");
+    for (int64_t k = 0; k < cell_ptr[n_cells]; ++k)
+        KCFD_REQUIRE(cell_nodes[k] >= 0 && cell_nodes[k] < n_nodes, "kcfd_mesh_build: cell node %lld out of range", (long long)cell_nodes[k]);
+
+    auto* m = new kcfd_host_mesh();
+    m->ndim = ndim;
+    m->n_cells = n_cells;
+    const int64_t n = n_cells;
+    const int D = ndim;
+    // ---- cell centres (node mean, sequential sum) and 2D areas (shoelace) ----
+    m->ccenter.assign(n * D, 0.0);
+    m->volume.assign(n, 0.0);
+    for (int64_t c = 0; c < n; ++c) {
+        int64_t b = cell_ptr[c], e = cell_ptr[c + 1];
+        int k = (int)(e - b);
+        for (int d = 0; d < D; ++d) {
+            double s = nodes[cell_nodes[b] * D + d];
+            for (int i = 1; i < k; ++i) s = s + nodes[cell_nodes[b + i] * D + d];
+            m->ccenter[c * D + d] = s / (double)k;
+        }
+        if (!is3d) {
+            double a = 0.0;
+            for (int i = 0; i < k; ++i) {
+                const double* pi = nodes + cell_nodes[b + i] * D;
+                const double* pj = nodes + cell_nodes[b + (i + 1) % k] * D;
+                double t1 = pi[0] * pj[1];
+                double t2 = pj[0] * pi[1];
+                a = a + (t1 - t2);
+            }
+            m->volume[c] = std::fabs(a) / 2.0;
+        }
+    }
+    // ---- face discovery ----
+    int64_t n_items = is3d ? cface_ptr[n] : cell_ptr[n];
+    KeyTable table((size_t)n_items);
+    std::vector<int64_t> first_item;  // per face: item index of first discovery
+    first_item.reserve(n_items / 2 + 16);
+    std::vector<int64_t> item_face(n_items);
+    int kmax_face = 2;
+    std::vector<int64_t> cells_nf(n, 0);
+    auto item_nodes = [&](int64_t it, int64_t c, int64_t* buf) -> int {
+        if (is3d) {
+            int k = (int)cface_len[it];
+            for (int i = 0; i < k; ++i) buf[i] = cface_nodes[cface_off[it] + i];
+            return k;
+        }
+        int64_t b = cell_ptr[c], e = cell_ptr[c + 1];
+        int64_t pos = it - b;
+        buf[0] = cell_nodes[it];
+        buf[1] = cell_nodes[b + (pos + 1) % (e - b)];
+        return 2;
+    };
+    int64_t buf[8];
+    for (int64_t c = 0; c < n; ++c) {
+        int64_t b = is3d ? cface_ptr[c] : cell_ptr[c];
+        int64_t e = is3d ? cface_ptr[c + 1] : cell_ptr[c + 1];
+        cells_nf[c] = e - b;
+        for (int64_t it = b; it < e; ++it) {
+            int k = item_nodes(it, c, buf);
+            if (k < 2 || k > 4) {
+                delete m;
+                kcfd::set_error("kcfd_mesh_build: faces need 2..4 nodes (got %d)", k);
+                return KCFD_BAD_INPUT;
+            }
+            for (int i = 0; i < k; ++i)
+                if (buf[i] < 0 || buf[i] >= n_nodes) {
+                    delete m;
+                    kcfd::set_error("kcfd_mesh_build: face node out of range");
+                    return KCFD_BAD_INPUT;
+                }
+            kmax_face = std::max(kmax_face, k);
+            Key key = make_key(buf, k);
+            bool found = false;
+            size_t s = table.find_or_insert(key, &found);
+            if (!found) {
+                table.val(s) = (int64_t)first_item.size();
+                first_item.push_back(it);
+                m->owner.push_back(c);
+                m->neighbour.push_back(-1);
+            } else {
+                m->neighbour[table.val(s)] = c;
+            }
+            item_face[it] = table.val(s);
+        }
+    }
+    const int64_t F = (int64_t)first_item.size();
+    m->n_faces = F;
+    m->max_face_nodes = kmax_face;
+    int kc = 0;
+    for (int64_t c = 0; c < n; ++c) kc = std::max<int64_t>(kc, cells_nf[c]);
+    m->max_cell_faces = kc;
+    m->cell_faces.assign(n * kc, -1);
+    for (int64_t c = 0; c < n; ++c) {
+        int64_t b = is3d ? cface_ptr[c] : cell_ptr[c];
+        for (int64_t j = 0; j < cells_nf[c]; ++j) m->cell_faces[c * kc + j] = item_face[b + j];
+    }
+    m->face_nodes.assign(F * kmax_face, -1);
+    std::vector<int> fsize(F);
+    for (int64_t f = 0; f < F; ++f) {
+        int64_t it = first_item[f];
+        int k = item_nodes(it, m->owner[f], buf);
+        fsize[f] = k;
+        for (int i = 0; i < k; ++i) m->face_nodes[f * kmax_face + i] = buf[i];
+    }
+    int64_t ni = 0;
+    for (int64_t f = 0; f < F; ++f) ni += (m->neighbour[f] >= 0);
+    m->n_internal = ni;
+    // ---- face geometry ----
+    m->area.assign(F, 0.0);
+    m->normal.assign(F * D, 0.0);
+    m->fcenter.assign(F * D, 0.0);
+    for (int64_t f = 0; f < F; ++f) {
+        const int64_t* fn = &m->face_nodes[f * kmax_face];
+        double* nr = &m->normal[f * D];
+        double* fc = &m->fcenter[f * D];
+        const double* cc = &m->ccenter[m->owner[f] * D];
+        if (D == 2) {
+            const double* p0 = nodes + fn[0] * 2;
+            const double* p1 = nodes + fn[1] * 2;
+            fc[0] = 0.5 * (p0[0] + p1[0]);
+            fc[1] = 0.5 * (p0[1] + p1[1]);
+            double dx = p1[0] - p0[0], dy = p1[1] - p0[1];
+            double len = std::sqrt(dx * dx + dy * dy);
+            nr[0] = dy;
+            nr[1] = -dx;
+            if (len > 1e-15) {
+                nr[0] = nr[0] / len;
+                nr[1] = nr[1] / len;
+            }
+            double t0 = fc[0] - cc[0], t1 = fc[1] - cc[1];
+            double dot = nr[0] * t0 + nr[1] * t1;
+            if (dot < 0) {
+                nr[0] = -nr[0];
+                nr[1] = -nr[1];
+            }
+            m->area[f] = len;
+        } else {
+            int k = fsize[f];
+            for (int d = 0; d < 3; ++d) {
+                double s = nodes[fn[0] * 3 + d];
+                for (int i = 1; i < k; ++i) s = s + nodes[fn[i] * 3 + d];
+                fc[d] = s / (double)k;
+            }
+            double nx = 0.0, ny = 0.0, nz = 0.0;
+            for (int i = 0; i < k; ++i) {
+                const double* pi = nodes + fn[i] * 3;
+                const double* pj = nodes + fn[(i + 1) % k] * 3;
+                nx = nx + (pi[1] - pj[1]) * (pi[2] + pj[2]);
+                ny = ny + (pi[2] - pj[2]) * (pi[0] + pj[0]);
+                nz = nz + (pi[0] - pj[0]) * (pi[1] + pj[1]);
+            }
+            double a = std::sqrt(nx * nx + ny * ny + nz * nz);
+            nr[0] = nx;
+            nr[1] = ny;
+            nr[2] = nz;
+            if (a > 1e-15) {
+                nr[0] = nr[0] / a;
+                nr[1] = nr[1] / a;
+                nr[2] = nr[2] / a;
+            }
+            m->area[f] = a * 0.5;
+            double dot = nr[0] * (fc[0] - cc[0]) + nr[1] * (fc[1] - cc[1]) + nr[2] * (fc[2] - cc[2]);
+            if (dot < 0) {
+                nr[0] = -nr[0];
+                nr[1] = -nr[1];
+                nr[2] = -nr[2];
+            }
+        }
+    }
+    if (is3d) {
+        for (int64_t c = 0; c < n; ++c) {
+            double vol = 0.0;
+            const double* cc = &m->ccenter[c * 3];
+            for (int j = 0; j < kc; ++j) {
+                int64_t f = m->cell_faces[c * kc + j];
+                if (f < 0) continue;
+                const double* fc = &m->fcenter[f * 3];
+                const double* nr = &m->normal[f * 3];
+                double sgn = 1.0;
+                double tdot = nr[0] * (fc[0] - cc[0]) + nr[1] * (fc[1] - cc[1]) + nr[2] * (fc[2] - cc[2]);
+                if (tdot < 0) sgn = -1.0;
+                double d = fc[0] * nr[0] + fc[1] * nr[1] + fc[2] * nr[2];
+                vol = vol + sgn * d * m->area[f];
+            }
+            vol = std::fabs(vol) / 3.0;
+            if (vol < 1e-30) vol = 1e-30;
+            m->volume[c] = vol;
+        }
+    }
+    // ---- boundary tagging ----
+    m->face_patch.assign(F, -1);
+    {
+        KeyTable bt((size_t)std::max<int64_t>(n_bfaces, 1));
+        int64_t off = 0;
+        for (int64_t q = 0; q < n_bfaces; ++q) {
+            int k = (int)bface_len[q];
+            if (k >= 2 && k <= 4) {
+                Key key = make_key(bface_nodes + off, k);
+                bool found;
+                size_t s = bt.find_or_insert(key, &found);
+                bt.val(s) = bface_patch[q];  // last assignment wins
+            }
+            off += k;
+        }
+        for (int64_t f = 0; f < F; ++f) {
+            if (m->neighbour[f] >= 0) continue;
+            Key key = make_key(&m->face_nodes[f * kmax_face], fsize[f]);
+            int64_t p = bt.lookup(key);
+            m->face_patch[f] = (p >= 0) ? (int32_t)p : -2;
+        }
+    }
+    build_pattern(m);
+    if (color_faces(m) != 0) {
+        delete m;
+        kcfd::set_error("kcfd_mesh_build: more than 64 face colours");
+        return KCFD_BAD_INPUT;
+    }
+    color_cells_and_levels(m);
+    *out = m;
+    return KCFD_OK;
+}
+
+int kcfd_mesh_info(const kcfd_host_mesh* m, int64_t* info) {
+    KCFD_REQUIRE(m && info, "kcfd_mesh_info: NULL argument");
+    info[0] = m->n_faces;
+    info[1] = m->n_internal;
+    info[2] = m->nnz;
+    info[3] = m->max_face_nodes;
+    info[4] = m->max_cell_faces;
+    info[5] = m->n_int_colors;
+    info[6] = m->n_bnd_colors;
+    info[7] = m->n_cell_colors;
+    info[8] = m->n_levels;
+    info[9] = m->ndim;
+    return KCFD_OK;
+}
+
+int kcfd_mesh_export(const kcfd_host_mesh* m, kcfd_mesh_export_t* o) {
+    KCFD_REQUIRE(m && o, "kcfd_mesh_export: NULL argument");
+    auto cp = [](auto* dst, const auto& v) {
+        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+    };
+    cp(o->owner, m->owner);
+    cp(o->neighbour, m->neighbour);
+    cp(o->face_nodes, m->face_nodes);
+    cp(o->cell_faces, m->cell_faces);
+    cp(o->area, m->area);
+    cp(o->normal, m->normal);
+    cp(o->fcenter, m->fcenter);
+    cp(o->ccenter, m->ccenter);
+    cp(o->volume, m->volume);
+    cp(o->face_patch, m->face_patch);
+    cp(o->indptr, m->indptr);
+    cp(o->indices, m->indices);
+    cp(o->slot_on, m->slot_on);
+    cp(o->slot_no, m->slot_no);
+    cp(o->diag_slot, m->diag_slot);
+    cp(o->face_color, m->face_color);
+    cp(o->cell_color, m->cell_color);
+    cp(o->level_natural, m->level_natural);
+    return KCFD_OK;
+}
+
+void kcfd_mesh_free(kcfd_host_mesh* m) { delete m; }
+
+int kcfd_version(void) { return 100; }
+
+int kcfd_last_error(char* buf, int32_t len) {
+    if (!buf || len <= 0) return KCFD_BAD_INPUT;
+    const std::string& e = kcfd::last_error();
+    size_t k = std::min<size_t>(e.size(), (size_t)len - 1);
+    std::memcpy(buf, e.data(), k);
+    buf[k] = 0;
+    return KCFD_OK;
+}
+
+}  // extern "C"

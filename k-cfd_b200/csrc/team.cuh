@@ -1,0 +1,147 @@
+// Teams of CTAs that run one Krylov solve together, and their deterministic
+// reductions.
+//
+//  * CtaTeam  -- one CTA owns a whole system; phases are separated by __syncthreads.
+//  * GridTeam -- every CTA of a cooperative launch owns a contiguous row range of one
+//                system; phases are separated by a software grid barrier whose wait
+//                is bounded by a clock64 budget (on expiry the kernel records
+//                KCFD_TIMEOUT and returns; nothing spins forever).
+//
+// Reductions are fixed-order: a fixed xor-shuffle tree inside each warp, a fixed
+// tree over warps, and (GridTeam) a fixed strided sum over CTA partials followed by
+// the same warp tree. Every CTA therefore computes bit-identical scalars and takes
+// the same branch, and a system gives the same result whatever runs beside it.
+#pragma once
+#include <cstdint>
+
+namespace kcfd {
+
+constexpr int kWarp = 32;
+
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Sum K values over the block; result returned to every thread. smem must hold
+// 32*K doubles. Deterministic for a fixed blockDim.
+template <int K>
+__device__ __forceinline__ void block_sum(double (&v)[K], double* smem) {
+    const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5, nw = blockDim.x >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) smem[k * 32 + wid] = v[k];
+    }
+    __syncthreads();
+    if (wid == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            double t = (lane < nw) ? smem[k * 32 + lane] : 0.0;
+            t = warp_sum(t);
+            if (lane == 0) smem[k * 32] = t;
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = smem[k * 32];
+    __syncthreads();
+}
+
+struct TeamCtl {
+    unsigned int* bar;     // [2] arrive counter, generation
+    double* partials;      // [slots * kMaxK * size]
+    int* err;              // KCFD_TIMEOUT when a barrier wait expired
+    long long budget;      // clock64 cycles a barrier may wait
+};
+
+constexpr int kMaxK = 8;   // values per reduction
+constexpr int kSlots = 8;  // reduction points per iteration
+
+struct CtaTeam {
+    int rank = 0, size = 1;
+    __device__ __forceinline__ bool sync() {
+        __syncthreads();
+        return true;
+    }
+    template <int K>
+    __device__ __forceinline__ bool allreduce(double (&v)[K], int /*slot*/, double* smem) {
+        block_sum<K>(v, smem);
+        return true;
+    }
+};
+
+struct GridTeam {
+    int rank, size;
+    TeamCtl ctl;
+    __device__ GridTeam(const TeamCtl& c) : rank(blockIdx.x), size(gridDim.x), ctl(c) {}
+
+    // Grid barrier: arrive on a counter; the last CTA resets it and bumps the
+    // generation. Waiters poll the generation with a clock64 budget.
+    __device__ bool sync() {
+        __shared__ int ok_s;
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            volatile unsigned int* vgen = ctl.bar + 1;
+            volatile int* verr = ctl.err;
+            unsigned int gen = *vgen;
+            int ok = (*verr == 0);
+            __threadfence();
+            unsigned int arrived = atomicAdd(ctl.bar, 1u);
+            if (arrived == (unsigned)size - 1) {
+                ctl.bar[0] = 0;
+                __threadfence();
+                atomicAdd(ctl.bar + 1, 1u);
+            } else {
+                long long t0 = clock64();
+                while (*vgen == gen) {
+                    if (*verr != 0) {
+                        ok = 0;
+                        break;
+                    }
+                    if (clock64() - t0 > ctl.budget) {
+                        atomicCAS(ctl.err, 0, 5 /*KCFD_TIMEOUT*/);
+                        ok = 0;
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __threadfence();
+            ok_s = ok;
+        }
+        __syncthreads();
+        return ok_s != 0;
+    }
+
+    template <int K>
+    __device__ bool allreduce(double (&v)[K], int slot, double* smem) {
+        block_sum<K>(v, smem);
+        double* base = ctl.partials + (size_t)slot * kMaxK * size;
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+            if (threadIdx.x == k) base[(size_t)k * size + rank] = v[k];
+        if (!sync()) return false;
+        const int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+        if (wid == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) {
+                const volatile double* src = base + (size_t)k * size;
+                double t = 0.0;
+                for (int j = lane; j < size; j += 32) t += src[j];
+                t = warp_sum(t);
+                if (lane == 0) smem[k * 32] = t;
+            }
+        }
+        __syncthreads();
+#pragma unroll
+        for (int k = 0; k < K; ++k) v[k] = smem[k * 32];
+        __syncthreads();
+        return true;
+    }
+};
+
+}  // namespace kcfd

@@ -1,0 +1,121 @@
+"""ctypes binding of libkcfd.so (the C ABI declared in include/kcfd.h).
+
+The library is loaded on first use. There is no CPU fallback: if the library is
+missing or no CUDA device is present, every device entry point raises.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import threading
+
+PKG_DIR = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG_DIR, "libkcfd.so")
+
+OK, MAXITER, BREAKDOWN, BAD_INPUT, CUDA_ERROR, TIMEOUT = 0, 1, 2, 3, 4, 5
+STATUS_NAMES = {0: "OK", 1: "MAXITER", 2: "BREAKDOWN", 3: "BAD_INPUT", 4: "CUDA_ERROR", 5: "TIMEOUT"}
+PREC = {"none": 0, "jacobi": 1, "ilu0": 2}
+STOP_SCIPY, STOP_GPU = 0, 1
+MODE_FP64, MODE_MIXED = 0, 1
+
+i32, i64, f64, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
+P_i32, P_i64, P_f64 = C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double)
+
+
+class KcfdError(RuntimeError):
+    def __init__(self, status, msg):
+        super().__init__(f"kcfd {STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+class MeshExport(C.Structure):
+    _fields_ = [(n, vp) for n in ("owner", "neighbour", "face_nodes", "cell_faces", "area", "normal", "fcenter",
+                                  "ccenter", "volume", "face_patch", "indptr", "indices", "slot_on", "slot_no",
+                                  "diag_slot", "face_color", "cell_color", "level_natural")]
+
+
+class Csr(C.Structure):
+    _fields_ = [("n", i32), ("nnz", i32), ("indptr", vp), ("indices", vp), ("vals64", vp), ("vals32", vp)]
+
+
+class SolverOpts(C.Structure):
+    _fields_ = [("precond", i32), ("stop", i32), ("mode", i32), ("nrhs", i32), ("maxiter", i32), ("team", i32),
+                ("lanes", i32), ("block", i32), ("rtol", f64), ("atol", f64), ("inner_rtol", f64),
+                ("max_refine", i32), ("pad", i32)]
+
+
+# name -> (restype, argtypes)
+SIGNATURES = {
+    "kcfd_version": (i32, []),
+    "kcfd_last_error": (i32, [C.c_char_p, i32]),
+    "kcfd_device_info": (i32, [P_i32, P_i32, P_i32]),
+    "kcfd_mesh_build": (i32, [i32, i64, vp, i64, vp, vp, vp, vp, vp, vp, i64, vp, vp, vp, C.POINTER(vp)]),
+    "kcfd_mesh_info": (i32, [vp, P_i64]),
+    "kcfd_mesh_export": (i32, [vp, C.POINTER(MeshExport)]),
+    "kcfd_mesh_free": (None, [vp]),
+    "kcfd_cast_f64_f32": (i32, [i64, vp, vp, vp]),
+    "kcfd_spmv_f64": (i32, [C.POINTER(Csr), vp, vp, i32, vp]),
+    "kcfd_spmv_f32": (i32, [C.POINTER(Csr), vp, vp, i32, vp]),
+    "kcfd_solver_create": (i32, [C.POINTER(Csr), C.POINTER(SolverOpts), vp, C.POINTER(vp)]),
+    "kcfd_solver_destroy": (None, [vp]),
+    "kcfd_solver_setup": (i32, [vp, C.POINTER(Csr), vp]),
+    "kcfd_solver_solve": (i32, [vp, C.POINTER(Csr), vp, vp, vp, vp, vp, vp]),
+    "kcfd_solver_error": (i32, [vp, P_i32, vp]),
+}
+
+_lib = None
+_lock = threading.Lock()
+
+
+def lib():
+    """Load libkcfd.so (building it first if the sources are newer)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    with _lock:
+        if _lib is not None:
+            return _lib
+        if not os.path.exists(LIB_PATH):
+            from . import build
+            build.build()
+        L = C.CDLL(LIB_PATH)
+        for name, (res, args) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.restype = res
+            fn.argtypes = args
+        _lib = L
+    return _lib
+
+
+def last_error():
+    buf = C.create_string_buffer(2048)
+    lib().kcfd_last_error(buf, 2048)
+    return buf.value.decode(errors="replace")
+
+
+def check(status, what=""):
+    if status != OK:
+        raise KcfdError(status, f"{what}: {last_error()}" if what else last_error())
+    return status
+
+
+def ptr(t):
+    """Device or host address of a torch tensor / numpy array (None -> NULL)."""
+    if t is None:
+        return None
+    if hasattr(t, "data_ptr"):
+        return t.data_ptr()
+    return t.ctypes.data
+
+
+def require_cuda():
+    import torch
+    if not torch.cuda.is_available():
+        raise KcfdError(CUDA_ERROR, "no CUDA device: the kcfd device path has no CPU fallback")
+    return torch
+
+
+def stream_handle(stream=None):
+    import torch
+    s = stream if stream is not None else torch.cuda.current_stream()
+    return s.cuda_stream

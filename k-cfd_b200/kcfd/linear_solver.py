@@ -1,0 +1,105 @@
+"""Drop-in for core/linear_solver.py and core/preconditioner.py of the K-CFD reference.
+
+solve_linear_system(system, x0, method, tol, maxiter, backend, preconditioner, **kw)
+keeps the reference signature (core/linear_solver.py:14-19). backend='b200' (or
+'auto') runs on libkcfd and is chosen before anything that could hide an error: a
+device failure raises instead of falling back to the CPU. Semantics kept:
+  * method='bicgstab': scipy's BiCGSTAB loop as the reference calls it
+    (core/linear_solver.py:59): atol=tol and scipy's default rtol=1e-5 unless the
+    caller passes rtol=..., so the stop is ||r|| < max(tol, rtol ||b||); x0=None
+    starts from zero; non-convergence prints and returns x (:60-61).
+  * preconditioner: 'none' | 'jacobi' (1/d where |d| > 1e-30, :43-47) | 'ilu0'
+    (structural, level-scheduled ILU(0); the reference's 'ilu0' is SuperLU spilu,
+    so agreement with it is at the solution level) | 'amg' (falls back to 'ilu0' as
+    the reference does without pyamg, :63-66).
+  * method='direct': the device has no sparse LU; BiCGSTAB + ILU(0) to a relative
+    residual of 1e-12 stands in for spsolve (documented difference).
+system may be the reference's FVMSystem (anything with .to_sparse() and .rhs), a
+kcfd FVMSystem, or a device-assembled kcfd DeviceSystem.
+"""
+from __future__ import annotations
+
+import time
+
+import numpy as np
+
+from . import _lib
+from .solver import DeviceCSR, Solver
+
+DIRECT_RTOL = 1e-12
+SCIPY_DEFAULT_RTOL = 1e-5
+
+
+def create_preconditioner(A_csr, method="none", **kwargs):
+    """Returns (M, info) like core/preconditioner.py:18-76. M is a device
+    preconditioner descriptor consumed by solve_linear_system / Solver."""
+    t0 = time.time()
+    if method == "amg":
+        print("  [Preconditioner] amg not built on the device path; using ILU(0).")
+        return create_preconditioner(A_csr, "ilu0")
+    if method == "iluk":
+        raise NotImplementedError("iluk is not on the kcfd device path (use 'ilu0')")
+    if method not in _lib.PREC:
+        raise ValueError(f"Unknown preconditioner: {method}")
+    if method == "none":
+        return None, {"method": "none", "setup_time": 0.0}
+    d = DeviceCSR.from_scipy(A_csr) if not isinstance(A_csr, DeviceCSR) else A_csr
+    s = Solver(d, precond=method, levels=kwargs.get("levels"))
+    s.setup(d)
+    _lib.require_cuda().cuda.synchronize()
+    return {"method": method, "solver": s, "csr": d}, {"method": method, "setup_time": time.time() - t0}
+
+
+def _as_device(system):
+    """(DeviceCSR, b device tensor, levels or None) from any supported system."""
+    torch = _lib.require_cuda()
+    if hasattr(system, "device_csr"):
+        return system.device_csr(), system.device_rhs(), getattr(system, "ilu_levels", None)
+    A = system.to_sparse()
+    b = torch.from_numpy(np.ascontiguousarray(system.rhs, dtype=np.float64)).cuda()
+    return DeviceCSR.from_scipy(A), b, None
+
+
+def solve_linear_system(system, x0=None, method="direct", tol=1e-8, maxiter=1000, backend="auto",
+                        preconditioner="none", **precond_kwargs):
+    if backend not in ("auto", "b200", "gpu"):
+        raise ValueError(f"kcfd runs on the device only (backend '{backend}' is the reference's CPU path)")
+    torch = _lib.require_cuda()
+    rtol = precond_kwargs.pop("rtol", SCIPY_DEFAULT_RTOL)
+    d, b, levels = _as_device(system)
+    levels = precond_kwargs.pop("levels", levels)
+    n = d.n
+    if method == "direct":
+        prec, atol, rtol_eff, its = "ilu0", 0.0, DIRECT_RTOL, max(maxiter, 20 * n)
+    elif method == "bicgstab":
+        prec, atol, rtol_eff, its = preconditioner, float(tol), float(rtol), maxiter
+        if prec == "amg":
+            prec = "ilu0"
+        if prec == "iluk":
+            raise NotImplementedError("iluk is not on the kcfd device path (use 'ilu0')")
+    elif method == "gmres":
+        raise NotImplementedError("gmres is not on the kcfd device path (use 'bicgstab')")
+    else:
+        raise ValueError(f"Unknown solver method: {method}")
+    x = torch.zeros(n, dtype=torch.float64, device=b.device) if x0 is None else \
+        torch.from_numpy(np.array(x0, dtype=np.float64)).to(b.device)
+    s = Solver(d, precond=prec, stop=_lib.STOP_SCIPY, maxiter=its, rtol=rtol_eff, atol=atol, levels=levels)
+    s.setup(d)
+    it, rr, st = s.solve(d, b, x)
+    status = int(st[0])
+    if status == _lib.MAXITER and method == "bicgstab":
+        print(f"[bicgstab] 수렴 실패: {int(it[0])} 반복 후 중단")
+    elif status not in (_lib.OK, _lib.MAXITER, _lib.BREAKDOWN):
+        raise _lib.KcfdError(status, "device solve failed")
+    err = s.barrier_error()
+    if err:
+        raise _lib.KcfdError(err, "device barrier wait expired")
+    return x.cpu().numpy()
+
+
+def solve_pressure_correction(system, method="direct", tol=1e-6, maxiter=2000, preconditioner="none",
+                              **precond_kwargs):
+    """core/linear_solver.py:73-93. The reference uses CG (atol=tol) for the iterative
+    branch; the device path uses BiCGSTAB with the same absolute threshold."""
+    m = "direct" if method == "direct" else "bicgstab"
+    return solve_linear_system(system, None, m, tol, maxiter, "b200", preconditioner, **precond_kwargs)

@@ -1,0 +1,141 @@
+"""Device CSR matrices and the BiCGSTAB solver handle (libkcfd kcfd_solver_*).
+
+Torch tensors serve only as device buffers; every computation runs in libkcfd's
+sm_100a kernels. A Solver binds one sparsity pattern and keeps its Krylov scratch
+and preconditioner resident, so repeated solves (SIMPLE outer iterations) allocate
+nothing and never synchronise with the host unless results are read.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+class DeviceCSR:
+    """CSR on the device: int32 indptr/indices, FP64 values and optional FP32 copy."""
+
+    def __init__(self, indptr, indices, vals64, vals32=None):
+        self.indptr, self.indices, self.vals64, self.vals32 = indptr, indices, vals64, vals32
+        self.n = int(indptr.numel() - 1)
+        self.nnz = int(indices.numel())
+
+    @classmethod
+    def from_scipy(cls, A, fp32=False, device="cuda"):
+        torch = _lib.require_cuda()
+        A = A.tocsr()
+        if not A.has_sorted_indices:
+            A = A.sorted_indices()
+        ip = torch.from_numpy(np.ascontiguousarray(A.indptr, dtype=np.int32)).to(device)
+        ix = torch.from_numpy(np.ascontiguousarray(A.indices, dtype=np.int32)).to(device)
+        v = torch.from_numpy(np.ascontiguousarray(A.data, dtype=np.float64)).to(device)
+        out = cls(ip, ix, v)
+        if fp32:
+            out.refresh_fp32()
+        return out
+
+    @classmethod
+    def from_pattern(cls, indptr, indices, device="cuda", fp32=False):
+        torch = _lib.require_cuda()
+        ip = torch.from_numpy(np.ascontiguousarray(indptr, dtype=np.int32)).to(device)
+        ix = torch.from_numpy(np.ascontiguousarray(indices, dtype=np.int32)).to(device)
+        v = torch.zeros(len(indices), dtype=torch.float64, device=device)
+        out = cls(ip, ix, v)
+        if fp32:
+            out.vals32 = torch.zeros(len(indices), dtype=torch.float32, device=device)
+        return out
+
+    def refresh_fp32(self, stream=None):
+        """FP32 copy of the FP64 values (kcfd_cast_f64_f32)."""
+        torch = _lib.require_cuda()
+        if self.vals32 is None:
+            self.vals32 = torch.empty(self.nnz, dtype=torch.float32, device=self.vals64.device)
+        _lib.check(_lib.lib().kcfd_cast_f64_f32(self.nnz, _lib.ptr(self.vals64), _lib.ptr(self.vals32),
+                                                _lib.stream_handle(stream)), "kcfd_cast_f64_f32")
+
+    def desc(self):
+        d = _lib.Csr()
+        d.n, d.nnz = self.n, self.nnz
+        d.indptr, d.indices = _lib.ptr(self.indptr), _lib.ptr(self.indices)
+        d.vals64 = _lib.ptr(self.vals64)
+        d.vals32 = _lib.ptr(self.vals32) if self.vals32 is not None else None
+        return d
+
+    def spmv(self, x, y=None, nrhs=1, fp32=False, stream=None):
+        torch = _lib.require_cuda()
+        if y is None:
+            y = torch.empty_like(x)
+        d = self.desc()
+        fn = _lib.lib().kcfd_spmv_f32 if fp32 else _lib.lib().kcfd_spmv_f64
+        _lib.check(fn(C.byref(d), _lib.ptr(x), _lib.ptr(y), nrhs, _lib.stream_handle(stream)), "kcfd_spmv")
+        return y
+
+
+class Solver:
+    """BiCGSTAB handle for one pattern.
+
+    precond: 'none' | 'jacobi' | 'ilu0'; stop: _lib.STOP_SCIPY | _lib.STOP_GPU;
+    mode: _lib.MODE_FP64 | _lib.MODE_MIXED; nrhs: 1 or 3; team: 0 auto, 1 one CTA,
+    2 whole grid; levels: ILU(0) level of each row (e.g. mesh.cell_color), None for
+    natural-order levels.
+    """
+
+    def __init__(self, csr, precond="jacobi", stop=_lib.STOP_SCIPY, mode=_lib.MODE_FP64, nrhs=1, maxiter=1000,
+                 rtol=1e-8, atol=0.0, team=0, lanes=0, block=0, inner_rtol=1e-4, max_refine=30, levels=None):
+        torch = _lib.require_cuda()
+        if precond not in _lib.PREC:
+            raise ValueError(f"Unknown preconditioner: {precond}")
+        o = _lib.SolverOpts()
+        o.precond, o.stop, o.mode, o.nrhs, o.maxiter = _lib.PREC[precond], stop, mode, nrhs, int(maxiter)
+        o.team, o.lanes, o.block = team, lanes, block
+        o.rtol, o.atol, o.inner_rtol, o.max_refine = float(rtol), float(atol), float(inner_rtol), int(max_refine)
+        self.opts = o
+        self.n, self.nrhs, self.mode = csr.n, nrhs, mode
+        self.precond = precond
+        lev = None
+        if levels is not None:
+            lev = np.ascontiguousarray(levels, dtype=np.int32)
+        h = C.c_void_p()
+        d = csr.desc()
+        _lib.check(_lib.lib().kcfd_solver_create(C.byref(d), C.byref(o), _lib.ptr(lev), C.byref(h)),
+                   "kcfd_solver_create")
+        self._h = h
+        dev = csr.vals64.device
+        self.iters = torch.zeros(nrhs, dtype=torch.int32, device=dev)
+        self.relres = torch.zeros(nrhs, dtype=torch.float64, device=dev)
+        self.status = torch.zeros(nrhs, dtype=torch.int32, device=dev)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().kcfd_solver_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def set_tolerances(self, rtol=None, atol=None, maxiter=None):
+        """Tolerances live in the handle; a change re-creates nothing."""
+        raise NotImplementedError("create a new Solver to change tolerances")
+
+    def setup(self, csr, stream=None):
+        d = csr.desc()
+        _lib.check(_lib.lib().kcfd_solver_setup(self._h, C.byref(d), _lib.stream_handle(stream)), "kcfd_solver_setup")
+
+    def solve(self, csr, b, x, stream=None):
+        """x (FP64, [n] or [n, nrhs]) holds x0 on entry and the solution on return.
+        Launches one kernel; returns the device arrays (iters, relres, status)."""
+        if self.mode == _lib.MODE_MIXED and csr.vals32 is None:
+            csr.refresh_fp32(stream)
+        d = csr.desc()
+        _lib.check(_lib.lib().kcfd_solver_solve(self._h, C.byref(d), _lib.ptr(b), _lib.ptr(x), _lib.ptr(self.iters),
+                                                _lib.ptr(self.relres), _lib.ptr(self.status),
+                                                _lib.stream_handle(stream)), "kcfd_solver_solve")
+        return self.iters, self.relres, self.status
+
+    def barrier_error(self, stream=None):
+        e = C.c_int32(0)
+        _lib.check(_lib.lib().kcfd_solver_error(self._h, C.byref(e), _lib.stream_handle(stream)), "kcfd_solver_error")
+        return e.value

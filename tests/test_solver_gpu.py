@@ -1,0 +1,198 @@
+"""Device BiCGSTAB (libkcfd) vs the oracle and the reference's own results.
+
+Tolerances: a converged Krylov solve is compared with (a) the reference result of
+the same algorithm (iteration count within 1, solution within 1e-8 relative L2),
+(b) the direct solution (relative L2 within 1e-6 for a 1e-10 absolute / 1e-8
+relative stop), and (c) itself across team shapes (1e-12: only the reduction
+partition differs).
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+
+from conftest import load_golden
+from case16 import channel_mesh, convdiff_system
+
+pytestmark = pytest.mark.gpu
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+@pytest.fixture(scope="module")
+def torch_cuda():
+    import torch
+    assert torch.cuda.is_available()
+    return torch
+
+
+def _hex_system(nx, seed=0):
+    """A 3D convection-diffusion system on an nx^3 hex cavity (oracle operators)."""
+    from kcfd import meshgen
+    from oracle import mesh as om, fvm
+    n, c, f, b = meshgen.hex_box_arrays(1, 1, 1, nx, nx, nx, meshgen.CAVITY_3D_NAMES)
+    m = om.build_3d(n, c, f, b)
+    rng = np.random.default_rng(seed)
+    s = fvm.System(m.n_cells)
+    fvm.diffusion_operator(m, rng.uniform(0.5, 2.0, m.n_cells), s)
+    fvm.convection_operator_upwind(m, rng.normal(size=m.n_faces) * m.area, s)
+    fvm.temporal_operator(m, 1.0, 10.0, np.zeros(m.n_cells), s)
+    A = s.to_sparse()
+    return m, A, rng.normal(size=m.n_cells)
+
+
+def test_gpu_bicgstab_matches_reference_gpu_path(torch_cuda):
+    from kcfd.gpu_solver import gpu_bicgstab
+    g = load_golden("solvers")
+    A, b = convdiff_system(channel_mesh(20, 20))
+    for tol in (1e-6, 1e-10):
+        x, info = gpu_bicgstab(A, b, None, tol, 1000, return_info=True)
+        ref = g[f"gpu_{tol:.0e}_x"]
+        assert abs(info["iterations"] - int(g[f"gpu_{tol:.0e}_matvecs"]) // 2) <= 1, info
+        assert _rel(x, ref) < 1e-8, _rel(x, ref)
+        assert np.linalg.norm(b - A @ x) / np.linalg.norm(b) < 10 * tol
+
+
+def test_gpu_bicgstab_with_x0_and_zero_rhs(torch_cuda):
+    from kcfd.gpu_solver import gpu_bicgstab
+    from oracle.linsolve import bicgstab_gpu_semantics
+    A, b = convdiff_system(channel_mesh(12, 9))
+    x0 = np.linspace(0, 1, A.shape[0])
+    x = gpu_bicgstab(A, b, x0, 1e-9, 500)
+    xr, _ = bicgstab_gpu_semantics(A, b, x0.copy(), 1e-9, 500)
+    assert _rel(x, xr) < 1e-8
+    # ||b|| < 1e-30: the reference returns x0 untouched
+    z = gpu_bicgstab(A, np.zeros(A.shape[0]), x0, 1e-9, 500)
+    np.testing.assert_array_equal(z, x0)
+
+
+@pytest.mark.parametrize("pc", ["none", "jacobi", "ilu0"])
+def test_scipy_semantics_case16(torch_cuda, pc):
+    """solve_linear_system(backend='b200') on the reference's case-16 system
+    (80x80, Pe=100) with the case's own call: atol=1e-10, rtol=0."""
+    from kcfd.linear_solver import solve_linear_system
+    from kcfd.fvm_operators import FVMSystem
+    g = load_golden("solvers")
+    A, b = convdiff_system(channel_mesh(80, 80))
+    sysm = FVMSystem.from_csr(A, b)
+    x = solve_linear_system(sysm, None, "bicgstab", 1e-10, 2000, "b200", pc, rtol=0.0)
+    xd = g["c16_80_direct"]
+    assert _rel(x, xd) < 1e-6
+    assert np.linalg.norm(b - A @ x) < 1e-9
+
+
+def test_iteration_counts_follow_scipy_loop(torch_cuda):
+    """Same loop as scipy: counts equal the oracle restatement's to within one."""
+    from kcfd.solver import DeviceCSR, Solver
+    from oracle.linsolve import bicgstab_scipy, jacobi
+    torch = torch_cuda
+    A, b = convdiff_system(channel_mesh(40, 40))
+    d = DeviceCSR.from_scipy(A)
+    for pc, M in (("none", None), ("jacobi", jacobi(A))):
+        _, info, its = bicgstab_scipy(A, b, np.zeros(len(b)), rtol=1e-8, atol=0.0, maxiter=3000, M=M)
+        s = Solver(d, precond=pc, rtol=1e-8, maxiter=3000)
+        s.setup(d)
+        x = torch.zeros(len(b), dtype=torch.float64, device="cuda")
+        it, rr, st = s.solve(d, torch.from_numpy(b).cuda(), x)
+        assert int(st[0]) == 0
+        assert abs(int(it[0]) - its) <= 1, (pc, int(it[0]), its)
+
+
+def test_grid_and_cta_teams_agree(torch_cuda):
+    from kcfd.solver import DeviceCSR, Solver
+    torch = torch_cuda
+    m, A, b = _hex_system(14)
+    d = DeviceCSR.from_scipy(A)
+    bd = torch.from_numpy(b).cuda()
+    xs = []
+    from kcfd import meshgen, mesh as km
+    n_, c_, f_, b_ = meshgen.hex_box_arrays(1, 1, 1, 14, 14, 14, meshgen.CAVITY_3D_NAMES)
+    colors = km.build_mesh(n_, c_, b_, ndim=3, cell_face_node_list=f_).cell_color
+    for team in (1, 2):
+        for pc, lev in (("jacobi", None), ("ilu0", None), ("ilu0", colors)):
+            s = Solver(d, precond=pc, rtol=1e-10, maxiter=5000, team=team, levels=lev)
+            s.setup(d)
+            x = torch.zeros_like(bd)
+            it, rr, st = s.solve(d, bd, x)
+            assert int(st[0]) == 0, (team, pc, int(st[0]))
+            assert s.barrier_error() == 0
+            xs.append(x.cpu().numpy())
+    xd = spla.spsolve(A.tocsc(), b)
+    for x in xs:
+        assert _rel(x, xd) < 1e-8
+
+
+def test_deterministic_repeat(torch_cuda):
+    from kcfd.solver import DeviceCSR, Solver
+    torch = torch_cuda
+    m, A, b = _hex_system(16, seed=3)
+    d = DeviceCSR.from_scipy(A)
+    bd = torch.from_numpy(b).cuda()
+    s = Solver(d, precond="jacobi", rtol=1e-9, maxiter=5000, team=2)
+    s.setup(d)
+    out = []
+    for _ in range(2):
+        x = torch.zeros_like(bd)
+        s.solve(d, bd, x)
+        out.append(x.cpu().numpy())
+    np.testing.assert_array_equal(out[0], out[1])
+
+
+def test_three_rhs_match_single_solves(torch_cuda):
+    from kcfd.solver import DeviceCSR, Solver
+    torch = torch_cuda
+    m, A, _ = _hex_system(12, seed=5)
+    rng = np.random.default_rng(9)
+    B = rng.normal(size=(A.shape[0], 3))
+    B[:, 2] *= 1e-3
+    d = DeviceCSR.from_scipy(A)
+    s3 = Solver(d, precond="jacobi", rtol=1e-10, maxiter=5000, nrhs=3)
+    s3.setup(d)
+    X = torch.zeros(A.shape[0], 3, dtype=torch.float64, device="cuda")
+    it3, _, st3 = s3.solve(d, torch.from_numpy(np.ascontiguousarray(B)).cuda(), X)
+    assert list(st3.cpu().numpy()) == [0, 0, 0]
+    s1 = Solver(d, precond="jacobi", rtol=1e-10, maxiter=5000)
+    s1.setup(d)
+    for c in range(3):
+        x = torch.zeros(A.shape[0], dtype=torch.float64, device="cuda")
+        it1, _, _ = s1.solve(d, torch.from_numpy(B[:, c].copy()).cuda(), x)
+        assert int(it1[0]) == int(it3[c])
+        assert _rel(X[:, c].cpu().numpy(), x.cpu().numpy()) < 1e-12
+
+
+@pytest.mark.parametrize("pc", ["jacobi", "ilu0"])
+def test_mixed_precision_matches_fp64(torch_cuda, pc):
+    """FP32 inner BiCGSTAB + FP64 refinement reaches the FP64 solution: 1e-8 relative
+    residual, and within 1e-7 relative L2 of the FP64 solve."""
+    from kcfd import _lib
+    from kcfd.solver import DeviceCSR, Solver
+    torch = torch_cuda
+    m, A, b = _hex_system(20, seed=7)
+    d = DeviceCSR.from_scipy(A, fp32=True)
+    bd = torch.from_numpy(b).cuda()
+    res = {}
+    for mode in (_lib.MODE_FP64, _lib.MODE_MIXED):
+        s = Solver(d, precond=pc, mode=mode, rtol=1e-8, maxiter=5000)
+        s.setup(d)
+        x = torch.zeros_like(bd)
+        it, rr, st = s.solve(d, bd, x)
+        assert int(st[0]) == 0, (mode, int(st[0]))
+        xn = x.cpu().numpy()
+        assert np.linalg.norm(b - A @ xn) / np.linalg.norm(b) < 1.5e-8
+        res[mode] = xn
+    assert _rel(res[_lib.MODE_MIXED], res[_lib.MODE_FP64]) < 1e-7
+
+
+def test_spmv_matches_scipy(torch_cuda):
+    from kcfd.solver import DeviceCSR
+    torch = torch_cuda
+    m, A, b = _hex_system(10, seed=1)
+    d = DeviceCSR.from_scipy(A, fp32=True)
+    x = np.random.default_rng(0).normal(size=(A.shape[0], 3))
+    y = d.spmv(torch.from_numpy(x[:, 0].copy()).cuda()).cpu().numpy()
+    np.testing.assert_allclose(y, A @ x[:, 0], rtol=1e-13, atol=1e-13)
+    y3 = d.spmv(torch.from_numpy(np.ascontiguousarray(x)).cuda(), nrhs=3).cpu().numpy()
+    np.testing.assert_allclose(y3, A @ x, rtol=1e-13, atol=1e-13)
+    y32 = d.spmv(torch.from_numpy(x[:, 0].astype(np.float32)).cuda(), fp32=True).cpu().numpy()
+    np.testing.assert_allclose(y32, A @ x[:, 0], rtol=1e-4, atol=1e-4)

@@ -131,7 +131,7 @@ typedef struct {
     int32_t precond;     /* KCFD_PREC_*                                        */
     int32_t stop;        /* KCFD_STOP_*                                        */
     int32_t mode;        /* KCFD_MODE_*                                        */
-    int32_t nrhs;        /* 1 or 3 (momentum components share one matrix)     */
+    int32_t nrhs;        /* 1, 2 or 3 (momentum components share one matrix)  */
     int32_t maxiter;     /* BiCGSTAB iterations (inner iterations in MIXED)   */
     int32_t team;        /* 0 auto, 1 one CTA per system, 2 whole grid         */
     int32_t lanes;       /* SpMV lanes per row: 0 auto, 1..32                  */
@@ -158,6 +158,113 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream);
  * non-NULL; nothing is synchronised with the host.                               */
 int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, double* x,
                       int32_t* iters, double* relres, int32_t* status, void* stream);
+
+
+/* ------------------------------------------------------- device mesh -------- */
+/* Device-resident SoA mesh. Faces are stored colour by colour: internal faces first
+ * (colours 0..n_colors_int-1), then boundary faces (n_colors_bnd colours); no two
+ * faces of one colour share a cell, so the owner/neighbour scatter of a colour is
+ * free of write conflicts (no atomics). face_ref maps a device face to its
+ * reference face id. All pointers are device pointers except color_ptr (host).   */
+typedef struct {
+    int32_t ndim, n_cells, n_faces, n_internal;
+    const int32_t* owner;      /* [F]  */
+    const int32_t* neigh;      /* [Fi] */
+    const double*  area;       /* [F]  */
+    const double*  normal;     /* [F*ndim] unit, owner-outward */
+    const double*  fcenter;    /* [F*ndim] */
+    const double*  ccenter;    /* [n*ndim] */
+    const double*  volume;     /* [n]  */
+    const double*  gc;         /* [Fi] interpolation weight dN/(dO+dN) */
+    const double*  dlen;       /* [F]  |d_PN| internal, |x_f - x_P| boundary */
+    const double*  dorth;      /* [Fi] max(|d_PN . n|, 0.1 |d_PN|) */
+    const int32_t* slot_on;    /* [Fi] CSR slot (owner, neighbour) */
+    const int32_t* slot_no;    /* [Fi] CSR slot (neighbour, owner) */
+    const int32_t* diag_slot;  /* [n]  */
+    const int32_t* indptr;     /* [n+1] CSR row pointers */
+    const int32_t* face_ref;   /* [F]  reference face id */
+    const int32_t* color_ptr;  /* HOST [n_colors_int + n_colors_bnd + 1] face ranges */
+    int32_t n_colors_int, n_colors_bnd;
+} kcfd_dmesh_t;
+
+/* Boundary conditions per boundary face (index = device face - n_internal).
+ * type: 0 zero_gradient, 1 dirichlet, 2 neumann.                                */
+typedef struct {
+    const int8_t* u_type;   /* [Fb]        velocity BC type               */
+    const double* u_val;    /* [Fb*ndim]   velocity boundary values       */
+    const int8_t* p_type;   /* [Fb]        pressure BC type               */
+    const double* p_val;    /* [Fb]        pressure boundary values       */
+    int32_t has_p_dirichlet;
+    int32_t pad;
+} kcfd_bc_t;
+
+#define KCFD_LIM_NONE       (-1)
+#define KCFD_LIM_MINMOD       0
+#define KCFD_LIM_SUPERBEE     1
+#define KCFD_LIM_VAN_ALBADA   2
+#define KCFD_LIM_VAN_LEER     3
+
+typedef struct {
+    double  rho, mu, alpha_u, dt;  /* dt > 0 adds the backward-Euler term (transient) */
+    int32_t limiter;               /* KCFD_LIM_*: MUSCL deferred correction, NONE = upwind */
+    int32_t nonorth;               /* 1: over-relaxed non-orthogonal correction           */
+} kcfd_mom_params_t;
+
+/* ------------------------------------------------ SIMPLE assembly kernels --- */
+/* Face mass flux F = rho (u_f . n) A, u_f = gc U_O + (1-gc) U_N inside, the
+ * dirichlet value (else U_O) on boundary faces. mf in device face order.
+ * SIMPLESolver._face_mass_flux (models/single_phase.py:124-144);
+ * compute_mass_flux (core/interpolation.py:163-182).                            */
+int kcfd_mass_flux(const kcfd_dmesh_t* m, const kcfd_bc_t* bc, const double* U, double rho, double* mf,
+                   void* stream);
+
+/* Momentum matrix (shared by all velocity components) and ndim right-hand sides:
+ * harmonic mu, d_orth diffusion, first-order upwind, boundary terms, face pressure
+ * source, optional MUSCL deferred correction and non-orthogonal correction (gradU:
+ * [n][ndim][ndim] Green-Gauss gradients of the components), optional time term,
+ * under-relaxation. Writes vals64 (and vals32 if non-NULL), b [n][ndim],
+ * aP_phys [n] (unrelaxed aP) and dP [n] = V / mean(aP).
+ * SIMPLESolver._momentum_eq (models/single_phase.py:147-258);
+ * muscl_deferred_correction (core/interpolation.py:227-303).                    */
+int kcfd_momentum_assemble(const kcfd_dmesh_t* m, const kcfd_bc_t* bc, const kcfd_mom_params_t* prm,
+                           const double* U, const double* U_old, const double* p, const double* mf,
+                           const double* gradU, double* aP, double* vals64, float* vals32, double* b,
+                           double* dP, void* stream);
+
+/* Pressure-correction matrix and rhs (models/single_phase.py:274-348): df =
+ * rho (dP_O+dP_N)/2 A / d_orth, rhs = -sum(+-mf), dirichlet-p boundary terms, and the
+ * row-0 reference pin when no pressure patch is dirichlet.                        */
+int kcfd_pressure_assemble(const kcfd_dmesh_t* m, const kcfd_bc_t* bc, double rho, const double* dP,
+                           const double* mf, double* aP, double* vals64, float* vals32, double* b,
+                           void* stream);
+
+/* Green-Gauss gradient of ncomp cell fields phi [n][ncomp] -> grad [n][ncomp][ndim]
+ * (core/gradient.py:12-48). Boundary face value: bval[bf*ncomp+k] where
+ * btype[bf] == 1, else the owner value.                                            */
+int kcfd_gg_gradient(const kcfd_dmesh_t* m, int32_t ncomp, const double* phi, const int8_t* btype,
+                     const double* bval, double* grad, void* stream);
+
+/* Reductions use a caller-provided scratch of KCFD_REDUCE_SCRATCH doubles.       */
+#define KCFD_REDUCE_SCRATCH 8192
+
+/* SIMPLE correction (models/single_phase.py:355-377): U -= dP grad(p'),
+ * p += alpha_p p'; norms2[0] = ||p'||^2, norms2[1] = ||p||^2 (after the update),
+ * summed in a fixed order. grad_pp: [n][ndim].                                     */
+int kcfd_simple_correct(const kcfd_dmesh_t* m, double alpha_p, const double* pp, const double* grad_pp,
+                        const double* dP, double* U, double* p, double* norms2, double* scratch, void* stream);
+
+/* norms2[2c] = ||A x_c - b_c||^2, norms2[2c+1] = ||b_c||^2 for c < nrhs
+ * (the post-solve residual of models/single_phase.py:270-271).                   */
+int kcfd_residual_norms(const kcfd_csr_t* A, const double* x, const double* b, int32_t nrhs, double* norms2,
+                        double* scratch, void* stream);
+
+/* Outer residual bookkeeping of solve_steady (models/single_phase.py:86-92) on the
+ * device: res = max(max_c ||r_c||/max(||b_c||,1e-15), ||p'||/max(||p||+1e-10,1e-10)),
+ * normalised by the first residual above 1e-30 (state[0]); state[1] = raw residual;
+ * hist[*it] = normalised residual when *it < max_hist; then *it += 1 (device counter,
+ * so a captured CUDA graph can replay the step).                                   */
+int kcfd_simple_residual(int32_t ndim, const double* mom_norms2, const double* p_norms2, double* state,
+                         double* hist, int32_t* it, int32_t max_hist, void* stream);
 
 /* Barrier error flag of the handle's last launch (KCFD_TIMEOUT when a bounded team
  * barrier wait expired, else 0). Synchronises the stream.                         */

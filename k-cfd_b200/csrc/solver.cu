@@ -680,8 +680,10 @@ void* solve_kernel_ptr(int mixed, int nrhs, int prec, bool grid) {
 #define KC_CASE(M, R, P) \
     if (mixed == M && nrhs == R && prec == P) return pick_kernel<M, R, P>(grid);
     KC_CASE(0, 1, 0) KC_CASE(0, 1, 1) KC_CASE(0, 1, 2)
+    KC_CASE(0, 2, 0) KC_CASE(0, 2, 1) KC_CASE(0, 2, 2)
     KC_CASE(0, 3, 0) KC_CASE(0, 3, 1) KC_CASE(0, 3, 2)
     KC_CASE(1, 1, 0) KC_CASE(1, 1, 1) KC_CASE(1, 1, 2)
+    KC_CASE(1, 2, 0) KC_CASE(1, 2, 1) KC_CASE(1, 2, 2)
     KC_CASE(1, 3, 0) KC_CASE(1, 3, 1) KC_CASE(1, 3, 2)
 #undef KC_CASE
     return nullptr;
@@ -763,7 +765,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     *out = nullptr;
     KCFD_REQUIRE(A->n > 0 && A->nnz >= A->n && A->indptr && A->indices, "kcfd_solver_create: bad CSR (n=%d nnz=%d)",
                  A->n, A->nnz);
-    KCFD_REQUIRE(opts->nrhs == 1 || opts->nrhs == 3, "kcfd_solver_create: nrhs must be 1 or 3");
+    KCFD_REQUIRE(opts->nrhs >= 1 && opts->nrhs <= 3, "kcfd_solver_create: nrhs must be 1, 2 or 3");
     KCFD_REQUIRE(opts->precond >= 0 && opts->precond <= 2, "kcfd_solver_create: bad precond");
     KCFD_REQUIRE(opts->mode == KCFD_MODE_FP64 || opts->mode == KCFD_MODE_MIXED, "kcfd_solver_create: bad mode");
     KCFD_REQUIRE(opts->stop == KCFD_STOP_SCIPY || opts->stop == KCFD_STOP_GPU, "kcfd_solver_create: bad stop rule");
@@ -1013,10 +1015,12 @@ int spmv_launch(const kcfd_csr_t* A, const V* vals, const V* x, V* y, int nrhs, 
     blocks = std::max(blocks, 1);
     if (nrhs == 1)
         spmv_kernel<V, V, 1><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y, L);
+    else if (nrhs == 2)
+        spmv_kernel<V, V, 2><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y, L);
     else if (nrhs == 3)
         spmv_kernel<V, V, 3><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y, L);
     else {
-        set_error("kcfd_spmv: nrhs must be 1 or 3");
+        set_error("kcfd_spmv: nrhs must be 1, 2 or 3");
         return KCFD_BAD_INPUT;
     }
     KCFD_CUDA(cudaGetLastError());

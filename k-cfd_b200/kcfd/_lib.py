@@ -61,7 +61,21 @@ SIGNATURES = {
     "kcfd_solver_setup": (i32, [vp, C.POINTER(Csr), vp]),
     "kcfd_solver_solve": (i32, [vp, C.POINTER(Csr), vp, vp, vp, vp, vp, vp]),
     "kcfd_solver_error": (i32, [vp, P_i32, vp]),
+    "kcfd_mass_flux": (i32, [vp, vp, vp, f64, vp, vp]),
+    "kcfd_momentum_assemble": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_pressure_assemble": (i32, [vp, vp, f64, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_gg_gradient": (i32, [vp, i32, vp, vp, vp, vp, vp]),
+    "kcfd_simple_correct": (i32, [vp, f64, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_residual_norms": (i32, [C.POINTER(Csr), vp, vp, i32, vp, vp, vp]),
+    "kcfd_simple_residual": (i32, [i32, vp, vp, vp, vp, vp, i32, vp]),
 }
+
+REDUCE_SCRATCH = 8192
+LIMITERS = {None: -1, "none": -1, "minmod": 0, "superbee": 1, "van_albada": 2, "van_leer": 3}
+
+
+class MomParams(C.Structure):
+    _fields_ = [("rho", f64), ("mu", f64), ("alpha_u", f64), ("dt", f64), ("limiter", i32), ("nonorth", i32)]
 
 _lib = None
 _lock = threading.Lock()

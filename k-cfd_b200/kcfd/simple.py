@@ -1,0 +1,234 @@
+"""SIMPLE solver on the device: the drop-in for models/single_phase.py SIMPLESolver.
+
+Public API as in the reference (models/single_phase.py:16-121): SIMPLESolver(mesh,
+rho, mu), set_velocity_bc, set_pressure_bc, alpha_u, alpha_p, max_outer_iter, tol,
+solve_steady() -> {'converged', 'iterations', 'residuals'}, and U / p fields whose
+.values are host numpy arrays (copied from / to the device on access).
+
+One outer iteration (models/single_phase.py:77-92) runs entirely on the device:
+  mass flux -> [Green-Gauss of U] -> momentum assembly (one matrix, ndim rhs) ->
+  one BiCGSTAB+Jacobi launch for all components -> post-solve residual norms ->
+  mass flux -> p' assembly -> ILU(0)/Jacobi set-up -> BiCGSTAB launch for p' ->
+  Green-Gauss of p' -> velocity/pressure correction -> residual bookkeeping.
+No step reads back to the host; with graph=True the iteration is captured once in a
+CUDA graph and replayed.
+
+Linear solves: the reference calls spsolve; here BiCGSTAB runs to a relative
+residual `rtol` (1e-8 by default) from the current field (momentum) or zero (p').
+precision='mixed' keeps FP64 assembly values for the outer residual and an FP32
+copy (written by the same kernels) for the inner iterations.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+from .device_mesh import BoundaryConditions, DeviceMesh
+from .mesh import Mesh, from_fvmesh
+from .solver import DeviceCSR, Solver
+
+
+class _Field:
+    """values: host numpy view of a device tensor (read copies, assignment uploads)."""
+
+    def __init__(self, owner, name):
+        self._owner, self._name = owner, name
+
+    @property
+    def values(self):
+        return getattr(self._owner, self._name).detach().cpu().numpy().copy()
+
+    @values.setter
+    def values(self, v):
+        t = getattr(self._owner, self._name)
+        torch = _lib.require_cuda()
+        t.copy_(torch.from_numpy(np.ascontiguousarray(v, dtype=np.float64).reshape(t.shape)))
+
+
+class SIMPLESolver:
+    def __init__(self, mesh, rho=1.0, mu=1e-3, precision="fp64", precond_p="jacobi", ilu_order="color",
+                 rtol=1e-8, maxiter=10000, muscl=None, nonorth=False, graph=False, team=0, lanes=0,
+                 inner_rtol=1e-4, device="cuda"):
+        torch = _lib.require_cuda()
+        if not isinstance(mesh, Mesh):
+            mesh = from_fvmesh(mesh)
+        self.mesh = mesh
+        self.dm = DeviceMesh(mesh, device)
+        self.bcs = BoundaryConditions(self.dm, device)
+        self.rho, self.mu = float(rho), float(mu)
+        self.alpha_u, self.alpha_p = 0.7, 0.3
+        self.max_outer_iter, self.tol = 500, 1e-6
+        self.residuals = []
+        self.transient, self.dt = False, 0.01
+        self.precision = precision
+        self.muscl = muscl
+        self.nonorth = bool(nonorth)
+        self.graph = graph
+        n, D, nnz = mesh.n_cells, mesh.ndim, mesh.nnz
+        self.ndim = D
+        f64 = dict(dtype=torch.float64, device=device)
+        self.U_t = torch.zeros(n, D, **f64)
+        self.U_old_t = torch.zeros(n, D, **f64)
+        self.p_t = torch.zeros(n, **f64)
+        self.pp_t = torch.zeros(n, **f64)
+        self.mf_t = torch.zeros(mesh.n_faces, **f64)
+        self.aP_t = torch.zeros(n, **f64)
+        self.dP_t = torch.zeros(n, **f64)
+        self.b_m = torch.zeros(n, D, **f64)
+        self.b_p = torch.zeros(n, **f64)
+        self.gU_t = torch.zeros(n, D, D, **f64) if (muscl or nonorth) else None
+        self.gpp_t = torch.zeros(n, D, **f64)
+        self.mom_norms = torch.zeros(2 * D, **f64)
+        self.p_norms = torch.zeros(2, **f64)
+        self.scratch = torch.zeros(_lib.REDUCE_SCRATCH, **f64)
+        self.state = torch.zeros(2, **f64)
+        self.it_dev = torch.zeros(1, dtype=torch.int32, device=device)
+        self.hist_cap = 1 << 16
+        self.hist = torch.zeros(self.hist_cap, **f64)
+        mixed = precision == "mixed"
+        self.mode = _lib.MODE_MIXED if mixed else _lib.MODE_FP64
+        ip, ix = self.dm.t["indptr"], self.dm.t["indices"]
+        self.A_m = DeviceCSR(ip, ix, torch.zeros(nnz, **f64),
+                             torch.zeros(nnz, dtype=torch.float32, device=device) if mixed else None)
+        self.A_p = DeviceCSR(ip, ix, torch.zeros(nnz, **f64),
+                             torch.zeros(nnz, dtype=torch.float32, device=device) if mixed else None)
+        self.s_m = Solver(self.A_m, precond="jacobi", mode=self.mode, nrhs=D, maxiter=maxiter, rtol=rtol,
+                          team=team, lanes=lanes, inner_rtol=inner_rtol)
+        levels = None
+        if precond_p == "ilu0":
+            levels = mesh.cell_color if ilu_order == "color" else mesh.level_natural
+        self.s_p = Solver(self.A_p, precond=precond_p, mode=self.mode, nrhs=1, maxiter=maxiter, rtol=rtol,
+                          team=team, lanes=lanes, inner_rtol=inner_rtol, levels=levels)
+        self.U = _Field(self, "U_t")
+        self.p = _Field(self, "p_t")
+        self._graph = None
+        self._params = _lib.MomParams()
+
+    # ---- boundary conditions (models/single_phase.py:55-68) ----
+    def set_velocity_bc(self, patch, bc_type, value=None):
+        self.bcs.set_velocity(patch, bc_type, value)
+        self._graph = None
+
+    def set_pressure_bc(self, patch, bc_type, value=None):
+        self.bcs.set_pressure(patch, bc_type, value)
+        self._graph = None
+
+    # ---- one outer iteration, all on the device ----
+    def _step(self):
+        L = _lib.lib()
+        chk = _lib.check
+        st = _lib.stream_handle()
+        dm = C.byref(self.dm.desc)
+        bc = C.byref(self.bcs.desc)
+        P = _lib.ptr
+        prm = self._params
+        prm.rho, prm.mu, prm.alpha_u = self.rho, self.mu, self.alpha_u
+        prm.dt = self.dt if self.transient else 0.0
+        prm.limiter = _lib.LIMITERS[self.muscl]
+        prm.nonorth = 1 if self.nonorth else 0
+        chk(L.kcfd_mass_flux(dm, bc, P(self.U_t), self.rho, P(self.mf_t), st), "mass_flux")
+        if self.gU_t is not None:
+            chk(L.kcfd_gg_gradient(dm, self.ndim, P(self.U_t), P(self.bcs.tensor("u_type")),
+                                   P(self.bcs.tensor("u_val")), P(self.gU_t), st), "gg_gradient U")
+        chk(L.kcfd_momentum_assemble(dm, bc, C.byref(prm), P(self.U_t), P(self.U_old_t), P(self.p_t), P(self.mf_t),
+                                     P(self.gU_t), P(self.aP_t), P(self.A_m.vals64), P(self.A_m.vals32),
+                                     P(self.b_m), P(self.dP_t), st), "momentum_assemble")
+        self.s_m.setup(self.A_m)
+        self.s_m.solve(self.A_m, self.b_m, self.U_t)
+        am = self.A_m.desc()
+        chk(L.kcfd_residual_norms(C.byref(am), P(self.U_t), P(self.b_m), self.ndim, P(self.mom_norms),
+                                  P(self.scratch), st), "residual_norms")
+        chk(L.kcfd_mass_flux(dm, bc, P(self.U_t), self.rho, P(self.mf_t), st), "mass_flux")
+        chk(L.kcfd_pressure_assemble(dm, bc, self.rho, P(self.dP_t), P(self.mf_t), P(self.aP_t),
+                                     P(self.A_p.vals64), P(self.A_p.vals32), P(self.b_p), st), "pressure_assemble")
+        self.s_p.setup(self.A_p)
+        self.pp_t.zero_()
+        self.s_p.solve(self.A_p, self.b_p, self.pp_t)
+        chk(L.kcfd_gg_gradient(dm, 1, P(self.pp_t), P(self.bcs.tensor("pp_type")), P(self.bcs.tensor("pp_val")),
+                               P(self.gpp_t), st), "gg_gradient p'")
+        chk(L.kcfd_simple_correct(dm, self.alpha_p, P(self.pp_t), P(self.gpp_t), P(self.dP_t), P(self.U_t),
+                                  P(self.p_t), P(self.p_norms), P(self.scratch), st), "simple_correct")
+        chk(L.kcfd_simple_residual(self.ndim, P(self.mom_norms), P(self.p_norms), P(self.state), P(self.hist),
+                                   P(self.it_dev), self.hist_cap, st), "simple_residual")
+
+    def iterate(self, n=1):
+        """Run n outer iterations (graph replay when graph=True)."""
+        torch = _lib.require_cuda()
+        self.bcs.upload()
+        if self.graph:
+            if self._graph is None:
+                s = torch.cuda.Stream()
+                s.wait_stream(torch.cuda.current_stream())
+                with torch.cuda.stream(s):
+                    self._step()      # warm-up outside capture (loads kernels, no allocations)
+                torch.cuda.current_stream().wait_stream(s)
+                g = torch.cuda.CUDAGraph()
+                with torch.cuda.graph(g):
+                    self._step()
+                self._graph = g
+                n -= 1
+            for _ in range(n):
+                self._graph.replay()
+        else:
+            for _ in range(n):
+                self._step()
+
+    def reset_history(self):
+        self.state.zero_()
+        self.it_dev.zero_()
+        self.hist.zero_()
+
+    def solve_steady(self):
+        """models/single_phase.py:70-101 semantics; the residual history is kept on the
+        device and read back once (and per iteration only when tol > 0)."""
+        torch = _lib.require_cuda()
+        self.reset_history()
+        self.residuals = []
+        done = 0
+        converged = False
+        while done < self.max_outer_iter:
+            step = 1 if self.tol > 0 else self.max_outer_iter - done
+            self.iterate(step)
+            done += step
+            if self.tol > 0:
+                r = float(self.hist[done - 1].item())
+                if r < self.tol:
+                    converged = True
+                    break
+        torch.cuda.synchronize()
+        self.residuals = self.hist[:done].cpu().numpy().tolist()
+        return {"converged": converged, "iterations": done, "residuals": self.residuals}
+
+    def solve_transient(self, t_end, dt=None):
+        """models/single_phase.py:103-121: up to 30 SIMPLE iterations per step, stopping
+        when the p' residual falls below 10 tol."""
+        torch = _lib.require_cuda()
+        if dt:
+            self.dt = dt
+        self.transient = True
+        self._graph = None
+        t, steps = 0.0, 0
+        while t < t_end - 1e-15:
+            self.U_old_t.copy_(self.U_t)
+            for _ in range(30):
+                self.iterate(1)
+                pn = self.p_norms.cpu().numpy()
+                rp = np.sqrt(pn[0]) / max(np.sqrt(pn[1]) + 1e-10, 1e-10)
+                if rp < self.tol * 10:
+                    break
+            t += self.dt
+            steps += 1
+        self.transient = False
+        self._graph = None
+        return {"time_steps": steps, "final_time": t}
+
+    def face_mass_flux(self):
+        """Current face mass flux in reference face order (host)."""
+        return self.dm.to_reference_faces(self.mf_t)
+
+    def solver_stats(self):
+        """Iterations / status of the last momentum and p' solves (host)."""
+        return {"mom_iters": self.s_m.iters.cpu().numpy().tolist(), "mom_status": self.s_m.status.cpu().numpy().tolist(),
+                "p_iters": int(self.s_p.iters[0]), "p_status": int(self.s_p.status[0])}

@@ -140,11 +140,14 @@ typedef struct {
     double  atol;        /* absolute tolerance (KCFD_STOP_SCIPY)               */
     double  inner_rtol;  /* MIXED: inner FP32 solve reduction per refinement   */
     int32_t max_refine;  /* MIXED: refinement steps                            */
-    int32_t pad;
+    int32_t inner_maxiter; /* MIXED: inner iterations per refinement step (0: 400) */
 } kcfd_solver_opts_t;
 
-/* ILU(0) ordering: perm/levels as produced by kcfd_mesh_export (cell_color or
- * level_natural). level_of_row == NULL -> natural-order levels computed here.  */
+/* ILU(0) ordering: level_of_row_host gives each row's level (e.g. the mesh's cell
+ * colouring, or natural-order dependency levels); NULL -> natural-order levels.
+ * Coupled rows must lie on different levels. With ILU(0) the handle solves the
+ * level-permuted system P A P^T (rows grouped by level), so every level is a
+ * contiguous row range that all CTAs share evenly.                               */
 int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts,
                        const int32_t* level_of_row_host, kcfd_solver** out);
 void kcfd_solver_destroy(kcfd_solver* s);

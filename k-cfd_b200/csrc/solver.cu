@@ -1,28 +1,32 @@
-// BiCGSTAB on sm_100a: one persistent launch per solve (or per batch of systems).
+// BiCGSTAB on sm_100a: one persistent launch per solve.
 //
 // Replaces the solve path of the K-CFD reference:
 //   core/gpu_solver.py:82-155   gpu_bicgstab / _gpu_bicgstab_cupy (KCFD_STOP_GPU)
 //   core/linear_solver.py:50-62 scipy bicgstab with create_preconditioner's M
 //                               (KCFD_STOP_SCIPY; Jacobi core/preconditioner.py:43-47,
-//                               ILU(0) in place of the SuperLU spilu at :49-54)
+//                               structural ILU(0) in place of the SuperLU spilu at :49-54)
 //
 // Design
-//  * A team of CTAs owns one system for the whole solve: a single CTA (small or
-//    batched systems) or the whole cooperative grid (large systems). Each CTA owns a
-//    contiguous row range; SpMV runs sub-warps of `lanes` threads per row and fuses the
-//    dot products the next scalar needs into its epilogue; vector phases are fused
-//    (p-update + preconditioner, s + preconditioner, x/r update + dots), so an
-//    iteration streams 21 vectors and two SpMVs and crosses 5 team barriers.
-//  * Dot products accumulate in FP64 with fixed-order trees (team.cuh), so every CTA
-//    derives the same alpha/beta/omega and the same stopping decision without a host
-//    round trip.
-//  * MIXED: FP32 matrix and vectors in the inner iterations, FP64 outer residual
-//    r = b - A x (FP64 matrix values), FP64 solution update, FP64 dots.
-//  * nrhs = 3 solves the momentum components together: one matrix, three vectors
-//    interleaved [n][3], per-component scalars and stopping.
-//  * ILU(0): structural, in a level order (a cell colouring, or natural-order
-//    dependency levels); factorisation and both sweeps proceed level by level with a
-//    team barrier between levels.
+//  * A team of CTAs owns one system for the whole solve: a single CTA (small systems)
+//    or the whole cooperative grid (large systems). Rows are grouped into levels
+//    (one level for Jacobi / none; the ILU(0) dependency levels otherwise) and every
+//    CTA owns an even slice of every level, so level-by-level work keeps all SMs busy.
+//  * SpMV runs sub-warps of `lanes` threads per row and fuses the dot product the
+//    next scalar needs into its epilogue; the vector phases are fused (p-update +
+//    Jacobi, s + Jacobi, x/r update + dots): an iteration streams 21 vectors and two
+//    SpMVs and crosses 5 team barriers (Jacobi) or 11 (two-level ILU(0)).
+//  * Dot products accumulate in FP64 with fixed-order trees (team.cuh); every CTA
+//    derives the same alpha/beta/omega and stopping decision with no host round trip.
+//  * MIXED: FP32 matrix and vectors in the inner iterations; FP64 outer residual
+//    r = b - A x with the FP64 values, FP64 solution update, FP64 dots. Inner runs are
+//    capped per refinement step; a step that does not lower the FP64 residual is
+//    undone and ends that right-hand side (status BREAKDOWN).
+//  * nrhs 2/3 solve the momentum components together: one matrix, vectors
+//    interleaved [n][nrhs], per-component scalars and stopping.
+//  * ILU(0) solves the level-permuted system P A P^T: levels are contiguous row
+//    ranges, the lower part of a row is exactly its columns left of the diagonal, and
+//    the forward / backward sweeps read contiguous memory. b and x are permuted on
+//    entry and exit inside the same launch.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -40,28 +44,31 @@ constexpr double kEps2 = 4.930380657631324e-32;  // float64 eps^2 (scipy rhotol/
 struct SolveArgs {
     int n;
     int lanes;
+    // matrix of the Krylov iterations (the level-permuted copy when perm != null)
     const int* indptr;
     const int* indices;
     const double* vals64;
     const float* vals32;
+    const int* perm;     // [n] permuted row -> caller row, or null
+    double* px;          // [n*nrhs] permuted FP64 solution (perm only)
+    double* pb;          // [n*nrhs] permuted FP64 rhs (perm only)
     // preconditioner
-    void* dinv;           // Jacobi inverse diagonal, V
-    const int* ilu_col;   // [nnz] columns of each row in level order
-    const int* ilu_diag;  // [n] absolute position of the diagonal in the ILU layout
-    void* lu;             // [nnz] factors, V
-    void* ludinv;         // [n] 1 / u_ii, V
-    const int* lev_ptr;
-    const int* lev_rows;
+    void* dinv;          // Jacobi inverse diagonal, V
+    const int* diag;     // [n] position of the diagonal (ILU)
+    void* lu;            // [nnz] ILU factors, V
+    void* ludinv;        // [n] 1 / u_ii, V
+    const int* lev_ptr;  // [nlev+1] level row ranges
     int nlev;
     // vectors
-    void* work;           // 9 V vectors of n*nrhs
-    double* x;            // [n*nrhs] FP64 solution (x0 on entry)
-    const double* b;      // [n*nrhs] FP64 right-hand side
-    double* r64;          // [n*nrhs] MIXED outer residual
+    void* work;          // 9 V vectors of n*nrhs
+    double* x;           // caller FP64 solution (x0 on entry)
+    const double* b;     // caller FP64 rhs
+    double* r64;         // MIXED outer residual
     // control
     int stop;
     int maxiter;
     int max_refine;
+    int inner_maxiter;
     double rtol, atol, inner_rtol;
     int* iters_out;
     double* relres_out;
@@ -86,16 +93,32 @@ struct Vecs {
     }
 };
 
+// This CTA's slice [s0, s1) of level l.
 template <class Team>
-__device__ __forceinline__ void my_range(const Team& tm, int n, int& r0, int& r1) {
-    int per = (n + tm.size - 1) / tm.size;
-    r0 = min(n, tm.rank * per);
-    r1 = min(n, r0 + per);
+__device__ __forceinline__ void level_slice(const Team& tm, const SolveArgs& a, int l, int& s0, int& s1) {
+    const int b0 = __ldg(a.lev_ptr + l), m = __ldg(a.lev_ptr + l + 1) - b0;
+    const int per = (m + tm.size - 1) / tm.size;
+    s0 = b0 + min(m, tm.rank * per);
+    s1 = b0 + min(m, tm.rank * per + per);
+}
+
+// f(s0, s1) over this CTA's slices of every level: the rows it owns.
+template <class Team, class F>
+__device__ __forceinline__ void for_my_rows(const Team& tm, const SolveArgs& a, F f) {
+    for (int l = 0; l < a.nlev; ++l) {
+        int s0, s1;
+        level_slice(tm, a, l, s0, s1);
+        if (s1 > s0) f(s0, s1);
+    }
 }
 
 // y = A x over rows [r0, r1) with sub-warps of L lanes per row. epi(row, acc) runs on
 // the first lane of the sub-warp.
-template <typename VM, typename VX, int NRHS, class Epi>
+// DIFF: difference form y_i = d_i x_i + sum_{j != i} a_ij (x_j - x_i), where the
+// diagonal slot holds the row sum d_i = sum_j a_ij. Identical in exact arithmetic; in
+// FP32 it keeps near-zero row sums (Neumann-type pressure operators) exact instead of
+// leaving them to the rounding of a large diagonal.
+template <typename VM, typename VX, int NRHS, bool DIFF = false, class Epi>
 __device__ __forceinline__ void spmv_range(const int* __restrict__ ip, const int* __restrict__ ix,
                                            const VM* __restrict__ val, const VX* __restrict__ x, int r0,
                                            int r1, int L, Epi epi) {
@@ -110,11 +133,27 @@ __device__ __forceinline__ void spmv_range(const int* __restrict__ ip, const int
         for (int c = 0; c < NRHS; ++c) acc[c] = 0.0;
         if (row < r1) {
             const int kb = __ldg(ip + row), ke = __ldg(ip + row + 1);
+            double xi[NRHS];
+            if (DIFF) {
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c) xi[c] = (double)x[(size_t)row * NRHS + c];
+            }
+#pragma unroll 4
             for (int k = kb + sl; k < ke; k += L) {
                 const int j = __ldg(ix + k);
-                const double a = (double)val[k];
+                const double av = (double)val[k];
+                if (DIFF) {
+                    if (j == row) {
 #pragma unroll
-                for (int c = 0; c < NRHS; ++c) acc[c] += a * (double)x[(size_t)j * NRHS + c];
+                        for (int c = 0; c < NRHS; ++c) acc[c] += av * xi[c];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NRHS; ++c) acc[c] += av * ((double)x[(size_t)j * NRHS + c] - xi[c]);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) acc[c] += av * (double)x[(size_t)j * NRHS + c];
+                }
             }
         }
         for (int o = L >> 1; o > 0; o >>= 1) {
@@ -125,103 +164,92 @@ __device__ __forceinline__ void spmv_range(const int* __restrict__ ip, const int
     }
 }
 
-// Preconditioner z = M^{-1} q on this team's rows (Jacobi) or over all levels (ILU).
-template <typename V, int NRHS, int PREC, class Team>
-__device__ __forceinline__ bool apply_prec(Team& tm, const SolveArgs& a, const V* __restrict__ q,
-                                           V* __restrict__ z, int r0, int r1) {
-    if (PREC == KCFD_PREC_NONE) {
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x)
+// z = (LU)^{-1} q on the level-permuted system. Level 0 of the forward sweep and the
+// last level of the backward sweep only touch rows this CTA owns, so the sweeps need
+// 2 (nlev - 1) barriers; the caller syncs before anything gathers z.
+template <typename V, int NRHS, class Team>
+__device__ __forceinline__ bool ilu_apply(Team& tm, const SolveArgs& a, const V* __restrict__ q, V* __restrict__ z) {
+    const V* lu = (const V*)a.lu;
+    const V* ldi = (const V*)a.ludinv;
+    for (int l = 0; l < a.nlev; ++l) {
+        if (l > 0 && !tm.sync()) return false;
+        int s0, s1;
+        level_slice(tm, a, l, s0, s1);
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            double acc[NRHS];
 #pragma unroll
-            for (int c = 0; c < NRHS; ++c) z[(size_t)i * NRHS + c] = q[(size_t)i * NRHS + c];
-        return true;
-    } else if (PREC == KCFD_PREC_JACOBI) {
-        const V* dinv = (const V*)a.dinv;
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-            const V d = dinv[i];
+            for (int c = 0; c < NRHS; ++c) acc[c] = (double)q[(size_t)i * NRHS + c];
+            const int kb = __ldg(a.indptr + i), kd = __ldg(a.diag + i);
+#pragma unroll 4
+            for (int k = kb; k < kd; ++k) {
+                const int j = __ldg(a.indices + k);
+                const double lv = (double)lu[k];
 #pragma unroll
-            for (int c = 0; c < NRHS; ++c) z[(size_t)i * NRHS + c] = d * q[(size_t)i * NRHS + c];
-        }
-        return true;
-    } else {
-        // the sweeps read other teams' rows: the caller's q must be complete
-        if (!tm.sync()) return false;
-        const V* lu = (const V*)a.lu;
-        const V* ldi = (const V*)a.ludinv;
-        for (int l = 0; l < a.nlev; ++l) {
-            const int b0 = a.lev_ptr[l], m = a.lev_ptr[l + 1] - b0;
-            const int per = (m + tm.size - 1) / tm.size;
-            const int s0 = min(m, tm.rank * per), s1 = min(m, s0 + per);
-            for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
-                const int i = a.lev_rows[b0 + k];
-                double acc[NRHS];
-#pragma unroll
-                for (int c = 0; c < NRHS; ++c) acc[c] = (double)q[(size_t)i * NRHS + c];
-                const int kb = a.indptr[i], kd = a.ilu_diag[i];
-                for (int kk = kb; kk < kd; ++kk) {
-                    const int j = a.ilu_col[kk];
-                    const double lv = (double)lu[kk];
-#pragma unroll
-                    for (int c = 0; c < NRHS; ++c) acc[c] -= lv * (double)z[(size_t)j * NRHS + c];
-                }
-#pragma unroll
-                for (int c = 0; c < NRHS; ++c) z[(size_t)i * NRHS + c] = (V)acc[c];
+                for (int c = 0; c < NRHS; ++c) acc[c] -= lv * (double)z[(size_t)j * NRHS + c];
             }
-            if (!tm.sync()) return false;
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) z[(size_t)i * NRHS + c] = (V)acc[c];
         }
-        for (int l = a.nlev - 1; l >= 0; --l) {
-            const int b0 = a.lev_ptr[l], m = a.lev_ptr[l + 1] - b0;
-            const int per = (m + tm.size - 1) / tm.size;
-            const int s0 = min(m, tm.rank * per), s1 = min(m, s0 + per);
-            for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
-                const int i = a.lev_rows[b0 + k];
-                double acc[NRHS];
-#pragma unroll
-                for (int c = 0; c < NRHS; ++c) acc[c] = (double)z[(size_t)i * NRHS + c];
-                const int kd = a.ilu_diag[i], ke = a.indptr[i + 1];
-                for (int kk = kd + 1; kk < ke; ++kk) {
-                    const int j = a.ilu_col[kk];
-                    const double uv = (double)lu[kk];
-#pragma unroll
-                    for (int c = 0; c < NRHS; ++c) acc[c] -= uv * (double)z[(size_t)j * NRHS + c];
-                }
-                const double di = (double)ldi[i];
-#pragma unroll
-                for (int c = 0; c < NRHS; ++c) z[(size_t)i * NRHS + c] = (V)(acc[c] * di);
-            }
-            if (!tm.sync()) return false;
-        }
-        return true;
     }
+    for (int l = a.nlev - 1; l >= 0; --l) {
+        if (l < a.nlev - 1 && !tm.sync()) return false;
+        int s0, s1;
+        level_slice(tm, a, l, s0, s1);
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            double acc[NRHS];
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) acc[c] = (double)z[(size_t)i * NRHS + c];
+            const int kd = __ldg(a.diag + i), ke = __ldg(a.indptr + i + 1);
+#pragma unroll 4
+            for (int k = kd + 1; k < ke; ++k) {
+                const int j = __ldg(a.indices + k);
+                const double uv = (double)lu[k];
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c) acc[c] -= uv * (double)z[(size_t)j * NRHS + c];
+            }
+            const double di = (double)ldi[i];
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) z[(size_t)i * NRHS + c] = (V)(acc[c] * di);
+        }
+    }
+    return true;
 }
 
-// Per-rhs state of one BiCGSTAB run (identical in every thread of the team).
+// Per-rhs scalar state of one BiCGSTAB run. It lives in shared memory: thread 0
+// writes it between block barriers, every thread reads it (identical in every CTA of
+// the team, since all CTAs derive it from the same fixed-order sums).
 template <int NRHS>
 struct KState {
-    double rho[NRHS], rho_prev[NRHS], alpha[NRHS], omega[NRHS], thr[NRHS], bnorm[NRHS], rnorm[NRHS];
-    int done[NRHS], status[NRHS], iters[NRHS];
+    double rho[NRHS], rho_prev[NRHS], alpha[NRHS], omega[NRHS], beta[NRHS], thr[NRHS], bnorm[NRHS], rnorm[NRHS];
+    int done[NRHS], status[NRHS], iters[NRHS], nonfinite[NRHS];
+    int active, any_left;
 };
 
-// BiCGSTAB over this team's rows. Solves A xv = bv from xv's initial contents.
+__device__ __forceinline__ bool finite(double v) { return isfinite(v); }
+
+// BiCGSTAB on this team's rows. Solves A xv = bv from xv (x_zero: xv == 0, r = b).
 //   stop == KCFD_STOP_SCIPY: scipy.sparse.linalg.bicgstab's loop, threshold
-//       max(atol, rtol ||b||) (rtol/atol passed in), eps^2 breakdown tests.
+//       max(atol, rtol ||b||), eps^2 breakdown tests.
 //   stop == KCFD_STOP_GPU: core/gpu_solver.py:127-153 (relative tests, 1e-30 guards).
-// Per-rhs results land in st. Returns false if a team barrier failed.
+// A non-finite scalar ends a right-hand side with KCFD_BREAKDOWN (nonfinite = 1).
+// Returns false if a team barrier failed.
 template <typename V, typename VM, int NRHS, int PREC, class Team>
 __device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict__ vals, V* __restrict__ xv,
-                              const V* __restrict__ bv, Vecs<V> w, int stop, double rtol, double atol,
-                              int maxiter, KState<NRHS>& st, double* smem) {
-    const int n = a.n;
-    int r0, r1;
-    my_range(tm, n, r0, r1);
+                              const V* __restrict__ bv, bool x_zero, const Vecs<V>& w, int stop, double rtol,
+                              double atol, int maxiter, KState<NRHS>& st, double* smem) {
     const int* __restrict__ ip = a.indptr;
     const int* __restrict__ ix = a.indices;
     const bool gpu = (stop == KCFD_STOP_GPU);
-    // r = b - A x ; rhat = r ; ||b||^2, ||r||^2 (= rhat.r)
+    const V* dinv = (const V*)a.dinv;
+    constexpr bool kDiff = sizeof(VM) == 4;  // FP32 operator: difference form
+    constexpr int kU = (NRHS == 1) ? 4 : (NRHS == 2 ? 2 : 1);  // rows per thread in flight
+    const bool t0 = threadIdx.x == 0;
+    // ---- r = b - A x ; rhat = r ; ||b||^2, ||r||^2 (= rhat.r) ----
     {
         double red[2 * NRHS];
 #pragma unroll
         for (int k = 0; k < 2 * NRHS; ++k) red[k] = 0.0;
-        spmv_range<VM, V, NRHS>(ip, ix, vals, xv, r0, r1, a.lanes, [&](int i, double* acc) {
+        auto init_row = [&](int i, const double* acc) {
 #pragma unroll
             for (int c = 0; c < NRHS; ++c) {
                 const size_t q = (size_t)i * NRHS + c;
@@ -234,204 +262,334 @@ __device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict
                 red[c] += bb * bb;
                 red[NRHS + c] += (double)rr * (double)rr;
             }
-        });
-        if (!tm.template allreduce<2 * NRHS>(red, 0, smem)) return false;
+        };
+        if (x_zero) {
+            for_my_rows(tm, a, [&](int s0, int s1) {
+                for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+                    double z[NRHS];
 #pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            st.bnorm[c] = sqrt(red[c]);
-            st.rnorm[c] = sqrt(red[NRHS + c]);
-            st.rho[c] = red[NRHS + c];  // rhat . r with rhat == r
-            st.rho_prev[c] = 1.0;
-            st.alpha[c] = 1.0;
-            st.omega[c] = 1.0;
-            st.iters[c] = 0;
-            st.status[c] = KCFD_OK;
-            if (gpu) {
-                st.thr[c] = rtol;  // relative: ||.|| / ||b|| < tol
-                st.done[c] = (st.bnorm[c] < 1e-30);
-            } else {
-                st.thr[c] = fmax(atol, rtol * st.bnorm[c]);
-                st.done[c] = (st.bnorm[c] == 0.0);
-                if (st.done[c]) {
-                    // scipy returns b (== 0) as the solution
-                    for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) xv[(size_t)i * NRHS + c] = (V)0;
+                    for (int c = 0; c < NRHS; ++c) z[c] = 0.0;
+                    init_row(i, z);
                 }
+            });
+        } else {
+            for_my_rows(tm, a, [&](int s0, int s1) {
+                spmv_range<VM, V, NRHS, kDiff>(ip, ix, vals, xv, s0, s1, a.lanes, init_row);
+            });
+        }
+        if (!tm.template allreduce<2 * NRHS>(red, 0, smem)) return false;
+        if (t0) {
+            for (int c = 0; c < NRHS; ++c) {
+                st.bnorm[c] = sqrt(red[c]);
+                st.rnorm[c] = sqrt(red[NRHS + c]);
+                st.rho[c] = red[NRHS + c];  // rhat . r with rhat == r
+                st.rho_prev[c] = 1.0;
+                st.alpha[c] = 1.0;
+                st.omega[c] = 1.0;
+                st.beta[c] = 0.0;
+                st.iters[c] = 0;
+                st.status[c] = KCFD_OK;
+                st.nonfinite[c] = !finite(red[c]) || !finite(red[NRHS + c]);
+                if (gpu) {
+                    st.thr[c] = rtol;  // relative: ||.|| / ||b|| < tol
+                    st.done[c] = (st.bnorm[c] < 1e-30);
+                } else {
+                    st.thr[c] = fmax(atol, rtol * st.bnorm[c]);
+                    st.done[c] = (st.bnorm[c] == 0.0);
+                }
+                if (st.nonfinite[c]) {
+                    st.done[c] = 1;
+                    st.status[c] = KCFD_BREAKDOWN;
+                }
+            }
+        }
+        __syncthreads();
+        if (!gpu) {
+            // scipy returns b (== 0) as the solution
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) {
+                if (!(st.bnorm[c] == 0.0)) continue;
+                for_my_rows(tm, a, [&](int s0, int s1) {
+                    for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) xv[(size_t)i * NRHS + c] = (V)0;
+                });
             }
         }
     }
     for (int it = 0; it < maxiter; ++it) {
-        // ---- top of iteration: stopping tests, beta, p update, phat = M^-1 p ----
-        int active = 0;
-        double beta[NRHS];
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            beta[c] = 0.0;
-            if (st.done[c]) continue;
-            if (!gpu) {
-                if (st.rnorm[c] < st.thr[c]) { st.done[c] = 1; st.status[c] = KCFD_OK; continue; }
-                if (fabs(st.rho[c]) < kEps2) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; continue; }
-                if (it > 0) {
-                    if (fabs(st.omega[c]) < kEps2) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; continue; }
-                    beta[c] = (st.rho[c] / st.rho_prev[c]) * (st.alpha[c] / st.omega[c]);
-                }
-            } else {
-                if (fabs(st.rho[c]) < 1e-30) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.iters[c] = it + 1; continue; }
-                beta[c] = (fabs(st.rho_prev[c] * st.omega[c]) > 1e-30)
-                              ? (st.rho[c] / st.rho_prev[c]) * (st.alpha[c] / st.omega[c]) : 0.0;
-            }
-            active = 1;
-        }
-        if (!active) return true;
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-#pragma unroll
+        // ---- top of iteration: stopping tests, beta ----
+        if (t0) {
+            int active = 0;
             for (int c = 0; c < NRHS; ++c) {
+                st.beta[c] = 0.0;
                 if (st.done[c]) continue;
-                const size_t q = (size_t)i * NRHS + c;
-                if (gpu) {
-                    w.p[q] = (V)((double)w.r[q] + beta[c] * ((double)w.p[q] - st.omega[c] * (double)w.v[q]));
-                } else if (it == 0) {
-                    w.p[q] = w.r[q];
+                if (!gpu) {
+                    if (st.rnorm[c] < st.thr[c]) { st.done[c] = 1; st.status[c] = KCFD_OK; continue; }
+                    if (fabs(st.rho[c]) < kEps2) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; continue; }
+                    if (it > 0) {
+                        if (fabs(st.omega[c]) < kEps2) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; continue; }
+                        st.beta[c] = (st.rho[c] / st.rho_prev[c]) * (st.alpha[c] / st.omega[c]);
+                    }
                 } else {
-                    w.p[q] = (V)(((double)w.p[q] - st.omega[c] * (double)w.v[q]) * beta[c] + (double)w.r[q]);
+                    if (fabs(st.rho[c]) < 1e-30) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.iters[c] = it + 1; continue; }
+                    st.beta[c] = (fabs(st.rho_prev[c] * st.omega[c]) > 1e-30)
+                                     ? (st.rho[c] / st.rho_prev[c]) * (st.alpha[c] / st.omega[c]) : 0.0;
+                }
+                if (!finite(st.beta[c])) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.nonfinite[c] = 1; continue; }
+                active = 1;
+            }
+            st.active = active;
+        }
+        __syncthreads();
+        if (!st.active) return true;
+        // ---- p update, phat = M^-1 p ----
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            for (int base = s0 + threadIdx.x; base < s1; base += kU * blockDim.x) {
+                V rr[kU][NRHS], pp[kU][NRHS], vv[kU][NRHS], dd[kU];
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int i = base + u * blockDim.x;
+                    if (i >= s1) continue;
+                    dd[u] = (PREC == KCFD_PREC_JACOBI) ? dinv[i] : (V)1;
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (st.done[c]) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        rr[u][c] = w.r[q];
+                        pp[u][c] = w.p[q];
+                        vv[u][c] = w.v[q];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int i = base + u * blockDim.x;
+                    if (i >= s1) continue;
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (st.done[c]) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        const double om = st.omega[c], be = st.beta[c];
+                        V pn;
+                        if (gpu) pn = (V)((double)rr[u][c] + be * ((double)pp[u][c] - om * (double)vv[u][c]));
+                        else if (it == 0) pn = rr[u][c];
+                        else pn = (V)(((double)pp[u][c] - om * (double)vv[u][c]) * be + (double)rr[u][c]);
+                        w.p[q] = pn;
+                        if (PREC == KCFD_PREC_JACOBI) w.ph[q] = dd[u] * pn;
+                    }
                 }
             }
-        }
-        V* ph = w.ph;
-        if (PREC == KCFD_PREC_NONE) {
-            ph = w.p;
-        } else if (!apply_prec<V, NRHS, PREC>(tm, a, w.p, w.ph, r0, r1)) {
-            return false;
-        }
+        });
+        V* ph = (PREC == KCFD_PREC_NONE) ? w.p : w.ph;
+        if (PREC == KCFD_PREC_ILU0 && !ilu_apply<V, NRHS>(tm, a, w.p, w.ph)) return false;
         if (!tm.sync()) return false;
         // ---- v = A phat ; rv = rhat . v ----
         double red1[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) red1[c] = 0.0;
-        spmv_range<VM, V, NRHS>(ip, ix, vals, ph, r0, r1, a.lanes, [&](int i, double* acc) {
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            spmv_range<VM, V, NRHS, kDiff>(ip, ix, vals, ph, s0, s1, a.lanes, [&](int i, const double* acc) {
 #pragma unroll
-            for (int c = 0; c < NRHS; ++c) {
-                const size_t q = (size_t)i * NRHS + c;
-                const V vv = (V)acc[c];
-                w.v[q] = vv;
-                red1[c] += (double)w.rh[q] * (double)vv;
-            }
+                for (int c = 0; c < NRHS; ++c) {
+                    const size_t q = (size_t)i * NRHS + c;
+                    const V vv = (V)acc[c];
+                    w.v[q] = vv;
+                    red1[c] += (double)w.rh[q] * (double)vv;
+                }
+            });
         });
         if (!tm.template allreduce<NRHS>(red1, 1, smem)) return false;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            if (st.done[c]) continue;
-            if (gpu) {
-                st.alpha[c] = (fabs(red1[c]) > 1e-30) ? st.rho[c] / red1[c] : 0.0;
-            } else {
-                if (red1[c] == 0.0) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.iters[c] = it + 1; continue; }
-                st.alpha[c] = st.rho[c] / red1[c];
+        if (t0) {
+            for (int c = 0; c < NRHS; ++c) {
+                if (st.done[c]) continue;
+                if (gpu) {
+                    st.alpha[c] = (fabs(red1[c]) > 1e-30) ? st.rho[c] / red1[c] : 0.0;
+                } else {
+                    if (red1[c] == 0.0) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.iters[c] = it + 1; continue; }
+                    st.alpha[c] = st.rho[c] / red1[c];
+                }
+                if (!finite(st.alpha[c])) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.nonfinite[c] = 1; st.iters[c] = it + 1; }
             }
         }
-        // ---- s = r - alpha v (in place in r) ; shat = M^-1 s ; ||s||^2 ----
+        __syncthreads();
+        // ---- s = r - alpha v (in place in r) ; shat = M^-1 s (Jacobi) ; ||s||^2 ----
         double red2[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) red2[c] = 0.0;
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            for (int base = s0 + threadIdx.x; base < s1; base += kU * blockDim.x) {
+                V rr[kU][NRHS], vv[kU][NRHS], dd[kU];
 #pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int i = base + u * blockDim.x;
+                    if (i >= s1) continue;
+                    dd[u] = (PREC == KCFD_PREC_JACOBI) ? dinv[i] : (V)1;
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (st.done[c]) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        rr[u][c] = w.r[q];
+                        vv[u][c] = w.v[q];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int i = base + u * blockDim.x;
+                    if (i >= s1) continue;
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (st.done[c]) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        const V sv = (V)((double)rr[u][c] - st.alpha[c] * (double)vv[u][c]);
+                        w.r[q] = sv;
+                        if (PREC == KCFD_PREC_JACOBI) w.sh[q] = dd[u] * sv;
+                        red2[c] += (double)sv * (double)sv;
+                    }
+                }
+            }
+        });
+        if (!tm.template allreduce<NRHS>(red2, 2, smem)) return false;
+        // per-rhs convergence on ||s||: x += alpha * phat, then stop
+        int conv_mask = 0;
+        if (t0) {
+            int any_left = 0;
             for (int c = 0; c < NRHS; ++c) {
                 if (st.done[c]) continue;
-                const size_t q = (size_t)i * NRHS + c;
-                const V s = (V)((double)w.r[q] - st.alpha[c] * (double)w.v[q]);
-                w.r[q] = s;
-                red2[c] += (double)s * (double)s;
-            }
-        }
-        V* sh = w.sh;
-        if (PREC == KCFD_PREC_NONE) {
-            sh = w.r;
-        } else if (PREC == KCFD_PREC_JACOBI) {
-            apply_prec<V, NRHS, PREC>(tm, a, w.r, w.sh, r0, r1);
-        }
-        if (!tm.template allreduce<NRHS>(red2, 2, smem)) return false;
-        int any_left = 0;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            if (st.done[c]) continue;
-            const double sn = sqrt(red2[c]);
-            const bool conv = gpu ? (sn / st.bnorm[c] < st.thr[c]) : (sn < st.thr[c]);
-            if (conv) {
-                // x += alpha * phat, then stop
-                for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-                    const size_t q = (size_t)i * NRHS + c;
-                    xv[q] = (V)((double)xv[q] + st.alpha[c] * (double)ph[q]);
+                const double sn = sqrt(red2[c]);
+                if (!finite(sn)) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.nonfinite[c] = 1; st.iters[c] = it + 1; continue; }
+                const bool conv = gpu ? (sn / st.bnorm[c] < st.thr[c]) : (sn < st.thr[c]);
+                if (conv) {
+                    st.done[c] = 2;  // converged here: the x update below still applies
+                    st.status[c] = KCFD_OK;
+                    st.iters[c] = it + 1;
+                    st.rnorm[c] = sn;
+                    continue;
                 }
-                st.done[c] = 1;
-                st.status[c] = KCFD_OK;
-                st.iters[c] = it + 1;
-                st.rnorm[c] = sn;
-                continue;
+                any_left = 1;
             }
-            any_left = 1;
+            st.any_left = any_left;
         }
-        if (!any_left) return tm.sync();
+        __syncthreads();
+#pragma unroll
+        for (int c = 0; c < NRHS; ++c)
+            if (st.done[c] == 2) conv_mask |= 1 << c;
+        if (conv_mask) {
+            for_my_rows(tm, a, [&](int s0, int s1) {
+                for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (!(conv_mask & (1 << c))) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        xv[q] = (V)((double)xv[q] + st.alpha[c] * (double)ph[q]);
+                    }
+                }
+            });
+            __syncthreads();
+            if (t0)
+                for (int c = 0; c < NRHS; ++c)
+                    if (st.done[c] == 2) st.done[c] = 1;
+            __syncthreads();
+        }
+        if (!st.any_left) return true;
+        V* sh = (PREC == KCFD_PREC_NONE) ? w.r : w.sh;
         if (PREC == KCFD_PREC_ILU0) {
-            if (!apply_prec<V, NRHS, PREC>(tm, a, w.r, w.sh, r0, r1)) return false;
+            if (!ilu_apply<V, NRHS>(tm, a, w.r, w.sh)) return false;
+            if (!tm.sync()) return false;
         }
-        if (!tm.sync()) return false;
         // ---- t = A shat ; t.s, t.t ----
         double red3[2 * NRHS];
 #pragma unroll
         for (int k = 0; k < 2 * NRHS; ++k) red3[k] = 0.0;
-        spmv_range<VM, V, NRHS>(ip, ix, vals, sh, r0, r1, a.lanes, [&](int i, double* acc) {
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            spmv_range<VM, V, NRHS, kDiff>(ip, ix, vals, sh, s0, s1, a.lanes, [&](int i, const double* acc) {
 #pragma unroll
-            for (int c = 0; c < NRHS; ++c) {
-                const size_t q = (size_t)i * NRHS + c;
-                const V tt = (V)acc[c];
-                w.t[q] = tt;
-                red3[c] += (double)tt * (double)w.r[q];
-                red3[NRHS + c] += (double)tt * (double)tt;
-            }
+                for (int c = 0; c < NRHS; ++c) {
+                    const size_t q = (size_t)i * NRHS + c;
+                    const V tt = (V)acc[c];
+                    w.t[q] = tt;
+                    red3[c] += (double)tt * (double)w.r[q];
+                    red3[NRHS + c] += (double)tt * (double)tt;
+                }
+            });
         });
         if (!tm.template allreduce<2 * NRHS>(red3, 3, smem)) return false;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            if (st.done[c]) continue;
-            if (gpu) st.omega[c] = (red3[NRHS + c] > 1e-30) ? red3[c] / red3[NRHS + c] : 0.0;
-            else st.omega[c] = red3[c] / red3[NRHS + c];
+        if (t0) {
+            for (int c = 0; c < NRHS; ++c) {
+                if (st.done[c]) continue;
+                if (gpu) st.omega[c] = (red3[NRHS + c] > 1e-30) ? red3[c] / red3[NRHS + c] : 0.0;
+                else st.omega[c] = red3[c] / red3[NRHS + c];
+                if (!finite(st.omega[c])) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.nonfinite[c] = 1; st.iters[c] = it + 1; }
+            }
         }
+        __syncthreads();
         // ---- x += alpha phat + omega shat ; r = s - omega t ; rhat.r, ||r||^2 ----
         double red4[2 * NRHS];
 #pragma unroll
         for (int k = 0; k < 2 * NRHS; ++k) red4[k] = 0.0;
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            for (int base = s0 + threadIdx.x; base < s1; base += kU * blockDim.x) {
+                V xx[kU][NRHS], hp[kU][NRHS], hs[kU][NRHS], rr[kU][NRHS], tt[kU][NRHS], rh[kU][NRHS];
 #pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int i = base + u * blockDim.x;
+                    if (i >= s1) continue;
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (st.done[c]) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        xx[u][c] = xv[q];
+                        hp[u][c] = ph[q];
+                        hs[u][c] = sh[q];
+                        rr[u][c] = w.r[q];
+                        tt[u][c] = w.t[q];
+                        rh[u][c] = w.rh[q];
+                    }
+                }
+#pragma unroll
+                for (int u = 0; u < kU; ++u) {
+                    const int i = base + u * blockDim.x;
+                    if (i >= s1) continue;
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) {
+                        if (st.done[c]) continue;
+                        const size_t q = (size_t)i * NRHS + c;
+                        const double al = st.alpha[c], om = st.omega[c];
+                        if (gpu) xv[q] = (V)((double)xx[u][c] + (al * (double)hp[u][c] + om * (double)hs[u][c]));
+                        else xv[q] = (V)(((double)xx[u][c] + al * (double)hp[u][c]) + om * (double)hs[u][c]);
+                        const V rn = (V)((double)rr[u][c] - om * (double)tt[u][c]);
+                        w.r[q] = rn;
+                        red4[c] += (double)rh[u][c] * (double)rn;
+                        red4[NRHS + c] += (double)rn * (double)rn;
+                    }
+                }
+            }
+        });
+        if (!tm.template allreduce<2 * NRHS>(red4, 4, smem)) return false;
+        if (t0) {
             for (int c = 0; c < NRHS; ++c) {
                 if (st.done[c]) continue;
-                const size_t q = (size_t)i * NRHS + c;
-                const double al = st.alpha[c], om = st.omega[c];
-                if (gpu) xv[q] = (V)((double)xv[q] + (al * (double)ph[q] + om * (double)sh[q]));
-                else xv[q] = (V)(((double)xv[q] + al * (double)ph[q]) + om * (double)sh[q]);
-                const V rn = (V)((double)w.r[q] - om * (double)w.t[q]);
-                w.r[q] = rn;
-                red4[c] += (double)w.rh[q] * (double)rn;
-                red4[NRHS + c] += (double)rn * (double)rn;
+                st.rho_prev[c] = st.rho[c];
+                st.rho[c] = red4[c];
+                st.rnorm[c] = sqrt(red4[NRHS + c]);
+                st.iters[c] = it + 1;
+                if (!finite(st.rnorm[c]) || !finite(st.rho[c])) {
+                    st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.nonfinite[c] = 1;
+                    continue;
+                }
+                if (gpu && st.rnorm[c] / st.bnorm[c] < st.thr[c]) {
+                    st.done[c] = 1;
+                    st.status[c] = KCFD_OK;
+                }
             }
         }
-        if (!tm.template allreduce<2 * NRHS>(red4, 4, smem)) return false;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            if (st.done[c]) continue;
-            st.rho_prev[c] = st.rho[c];
-            st.rho[c] = red4[c];
-            st.rnorm[c] = sqrt(red4[NRHS + c]);
-            st.iters[c] = it + 1;
-            if (gpu && st.rnorm[c] / st.bnorm[c] < st.thr[c]) {
-                st.done[c] = 1;
-                st.status[c] = KCFD_OK;
-            }
-        }
+        __syncthreads();
     }
-#pragma unroll
-    for (int c = 0; c < NRHS; ++c)
-        if (!st.done[c]) {
-            st.status[c] = KCFD_MAXITER;
-            st.iters[c] = maxiter;
-        }
+    if (t0) {
+        for (int c = 0; c < NRHS; ++c)
+            if (!st.done[c]) {
+                st.status[c] = KCFD_MAXITER;
+                st.iters[c] = maxiter;
+            }
+    }
+    __syncthreads();
     return true;
 }
 
@@ -446,118 +604,207 @@ __device__ void write_results(const SolveArgs& a, const KState<NRHS>& st, int te
     }
 }
 
-// FP64 solve: x in place.
+// Copy the caller's x, b into the level-permuted order (own rows), or back.
+template <int NRHS, class Team>
+__device__ void permute_in(Team& tm, const SolveArgs& a) {
+    for_my_rows(tm, a, [&](int s0, int s1) {
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            const int o = a.perm[i];
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) {
+                a.px[(size_t)i * NRHS + c] = a.x[(size_t)o * NRHS + c];
+                a.pb[(size_t)i * NRHS + c] = a.b[(size_t)o * NRHS + c];
+            }
+        }
+    });
+}
+
+template <int NRHS, class Team>
+__device__ void permute_out(Team& tm, const SolveArgs& a) {
+    for_my_rows(tm, a, [&](int s0, int s1) {
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            const int o = a.perm[i];
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) a.x[(size_t)o * NRHS + c] = a.px[(size_t)i * NRHS + c];
+        }
+    });
+}
+
+// FP64 solve.
 template <int NRHS, int PREC, class Team>
 __device__ void solve_fp64(Team& tm, const SolveArgs& a, double* smem) {
-    Vecs<double> w(a.work, (size_t)a.n * NRHS);
-    KState<NRHS> st;
-    bool ok = bicgstab_body<double, double, NRHS, PREC>(tm, a, a.vals64, a.x, a.b, w, a.stop, a.rtol, a.atol,
+    __shared__ KState<NRHS> st;
+    const Vecs<double> w(a.work, (size_t)a.n * NRHS);
+    double* x = a.perm ? a.px : a.x;
+    const double* b = a.perm ? a.pb : a.b;
+    if (a.perm) {
+        permute_in<NRHS>(tm, a);
+        if (!tm.sync()) return;
+    }
+    bool ok = bicgstab_body<double, double, NRHS, PREC>(tm, a, a.vals64, x, b, false, w, a.stop, a.rtol, a.atol,
                                                         a.maxiter, st, smem);
     if (!ok) return;
+    if (a.perm) permute_out<NRHS>(tm, a);
     write_results<NRHS>(a, st, tm.rank);
 }
 
-// MIXED solve: FP64 outer refinement around FP32 inner BiCGSTAB runs.
+// Outer (FP64) state of a MIXED solve, in shared memory like KState.
+template <int NRHS>
+struct MState {
+    double thr[NRHS], rn[NRHS], bn[NRHS], rn_prev[NRHS];
+    int done[NRHS], applied[NRHS], revert[NRHS];
+    int left, stop_now, total_it, cap;
+    double inner_atol;
+};
+
+// MIXED solve: FP64 outer refinement around capped FP32 inner BiCGSTAB runs.
 template <int NRHS, int PREC, class Team>
 __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
+    __shared__ KState<NRHS> out;
+    __shared__ KState<NRHS> st;
+    __shared__ MState<NRHS> ms;
     const int n = a.n;
-    int r0, r1;
-    my_range(tm, n, r0, r1);
-    Vecs<float> w(a.work, (size_t)n * NRHS);
-    KState<NRHS> out;
-    double thr[NRHS], rn[NRHS], bn[NRHS];
-    int done[NRHS];
-    int total_it = 0;
+    const Vecs<float> w(a.work, (size_t)n * NRHS);
+    double* x = a.perm ? a.px : a.x;
+    const double* b = a.perm ? a.pb : a.b;
+    const bool t0 = threadIdx.x == 0;
+    if (a.perm) {
+        permute_in<NRHS>(tm, a);
+        if (!tm.sync()) return;
+    }
+    if (t0) {
+        for (int c = 0; c < NRHS; ++c) {
+            ms.applied[c] = 0;
+            ms.done[c] = 0;
+            ms.rn_prev[c] = INFINITY;
+            ms.thr[c] = 0.0;
+            ms.rn[c] = 0.0;
+            out.status[c] = KCFD_OK;
+            out.iters[c] = 0;
+        }
+        ms.total_it = 0;
+    }
+    __syncthreads();
     for (int ref = 0;; ++ref) {
         // r64 = b - A64 x ; ||b||, ||r||
         double red[2 * NRHS];
 #pragma unroll
         for (int k = 0; k < 2 * NRHS; ++k) red[k] = 0.0;
-        spmv_range<double, double, NRHS>(a.indptr, a.indices, a.vals64, a.x, r0, r1, a.lanes,
-                                         [&](int i, double* acc) {
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            spmv_range<double, double, NRHS>(a.indptr, a.indices, a.vals64, x, s0, s1, a.lanes,
+                                             [&](int i, const double* acc) {
 #pragma unroll
-                                             for (int c = 0; c < NRHS; ++c) {
-                                                 const size_t q = (size_t)i * NRHS + c;
-                                                 const double bb = a.b[q];
-                                                 const double rr = bb - acc[c];
-                                                 a.r64[q] = rr;
-                                                 w.bi[q] = (float)rr;
-                                                 w.xi[q] = 0.0f;
-                                                 red[c] += bb * bb;
-                                                 red[NRHS + c] += rr * rr;
-                                             }
-                                         });
+                                                 for (int c = 0; c < NRHS; ++c) {
+                                                     const size_t q = (size_t)i * NRHS + c;
+                                                     const double bb = b[q];
+                                                     const double rr = bb - acc[c];
+                                                     a.r64[q] = rr;
+                                                     red[c] += bb * bb;
+                                                     red[NRHS + c] += rr * rr;
+                                                 }
+                                             });
+        });
         if (!tm.template allreduce<2 * NRHS>(red, 5, smem)) return;
-        int left = 0;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            bn[c] = sqrt(red[c]);
-            rn[c] = sqrt(red[NRHS + c]);
-            if (ref == 0) {
-                thr[c] = fmax(a.atol, a.rtol * bn[c]);
-                out.status[c] = KCFD_OK;
-                out.iters[c] = 0;
-            }
-            out.bnorm[c] = bn[c];
-            out.rnorm[c] = rn[c];
-            done[c] = (rn[c] < thr[c]) || (bn[c] == 0.0);
-            if (ref > 0 && !done[c] && out.status[c] == KCFD_BREAKDOWN) done[c] = 1;
-            if (done[c] && out.status[c] != KCFD_BREAKDOWN) out.status[c] = KCFD_OK;
-            left |= !done[c];
-        }
-        if (!left) break;
-        if (ref >= a.max_refine || total_it >= a.maxiter) {
-#pragma unroll
-            for (int c = 0; c < NRHS; ++c)
-                if (!done[c]) out.status[c] = KCFD_MAXITER;
-            break;
-        }
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-#pragma unroll
-            for (int c = 0; c < NRHS; ++c)
-                if (done[c]) w.bi[(size_t)i * NRHS + c] = 0.0f;
-        }
-        if (!tm.sync()) return;
-        // inner FP32 solve A32 e = r, from e = 0, to max(inner_rtol ||r||, thr/2)
-        KState<NRHS> st;
-        // reuse the scipy loop; per-rhs thresholds are absolute: pass rtol=inner, atol=thr/2
-        double inner_atol = thr[0] * 0.5;
-        for (int c = 1; c < NRHS; ++c) inner_atol = fmin(inner_atol, thr[c] * 0.5);
-        bool ok = bicgstab_body<float, float, NRHS, PREC>(tm, a, a.vals32, w.xi, w.bi, w, KCFD_STOP_SCIPY,
-                                                          a.inner_rtol, inner_atol, a.maxiter - total_it, st, smem);
-        if (!ok) return;
-        int max_it = 0;
-        int progress = 0;
-#pragma unroll
-        for (int c = 0; c < NRHS; ++c) {
-            if (done[c]) continue;
-            out.iters[c] += st.iters[c];
-            max_it = max(max_it, st.iters[c]);
-            if (st.iters[c] > 0) progress = 1;
-            else if (st.status[c] == KCFD_BREAKDOWN) out.status[c] = KCFD_BREAKDOWN;
-        }
-        total_it += max(max_it, 1);
-        // x += e for the rhs still running
-        for (int i = r0 + threadIdx.x; i < r1; i += blockDim.x) {
-#pragma unroll
+        if (t0) {
+            int left = 0;
             for (int c = 0; c < NRHS; ++c) {
-                if (done[c]) continue;
-                const size_t q = (size_t)i * NRHS + c;
-                a.x[q] = a.x[q] + (double)w.xi[q];
+                ms.revert[c] = 0;
+                ms.bn[c] = sqrt(red[c]);
+                const double r_new = sqrt(red[NRHS + c]);
+                if (ref == 0) ms.thr[c] = fmax(a.atol, a.rtol * ms.bn[c]);
+                out.bnorm[c] = ms.bn[c];
+                if (ms.done[c]) continue;
+                if (ms.applied[c] && !(r_new < ms.rn_prev[c])) {
+                    // the last refinement step did not lower the FP64 residual: undo it
+                    ms.revert[c] = 1;
+                    ms.done[c] = 1;
+                    out.status[c] = KCFD_BREAKDOWN;
+                    ms.rn[c] = ms.rn_prev[c];
+                } else if (!finite(r_new)) {
+                    ms.done[c] = 1;
+                    out.status[c] = KCFD_BREAKDOWN;
+                    ms.rn[c] = r_new;
+                } else {
+                    ms.rn[c] = r_new;
+                    if (r_new < ms.thr[c] || ms.bn[c] == 0.0) {
+                        ms.done[c] = 1;
+                        out.status[c] = KCFD_OK;
+                    }
+                }
+                ms.applied[c] = 0;
+                out.rnorm[c] = ms.rn[c];
+                left |= !ms.done[c];
             }
-        }
-        if (!progress) {
-#pragma unroll
+            ms.left = left;
+            ms.stop_now = 0;
+            if (left && (ref >= a.max_refine || ms.total_it >= a.maxiter)) {
+                for (int c = 0; c < NRHS; ++c)
+                    if (!ms.done[c]) out.status[c] = KCFD_MAXITER;
+                ms.stop_now = 1;
+            }
+            double ia = INFINITY;
             for (int c = 0; c < NRHS; ++c)
-                if (!done[c] && out.status[c] == KCFD_OK) out.status[c] = KCFD_BREAKDOWN;
+                if (!ms.done[c]) ia = fmin(ia, ms.thr[c] * 0.5);
+            ms.inner_atol = ia;
+            ms.cap = min(a.inner_maxiter, a.maxiter - ms.total_it);
         }
+        __syncthreads();
+        // own rows: undo rejected steps, load the inner rhs, zero the inner solution
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c) {
+                    const size_t q = (size_t)i * NRHS + c;
+                    if (ms.revert[c]) x[q] = x[q] - (double)w.xi[q];
+                    w.bi[q] = ms.done[c] ? 0.0f : (float)a.r64[q];
+                    w.xi[q] = 0.0f;
+                }
+            }
+        });
+        if (!ms.left || ms.stop_now) break;
+        // inner FP32 solve A32 e = r from e = 0 to max(inner_rtol ||r||, thr/2)
+        bool ok = bicgstab_body<float, float, NRHS, PREC>(tm, a, a.vals32, w.xi, w.bi, true, w, KCFD_STOP_SCIPY,
+                                                          a.inner_rtol, ms.inner_atol, ms.cap, st, smem);
+        if (!ok) return;
+        if (t0) {
+            int max_it = 0;
+            for (int c = 0; c < NRHS; ++c) {
+                if (ms.done[c]) continue;
+                out.iters[c] += st.iters[c];
+                max_it = max(max_it, st.iters[c]);
+                if (st.nonfinite[c] || st.iters[c] == 0) {
+                    ms.done[c] = 1;
+                    out.status[c] = KCFD_BREAKDOWN;
+                } else {
+                    ms.applied[c] = 1;
+                    ms.rn_prev[c] = ms.rn[c];
+                }
+            }
+            ms.total_it += max(max_it, 1);
+        }
+        __syncthreads();
+        for_my_rows(tm, a, [&](int s0, int s1) {
+            for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c) {
+                    if (!ms.applied[c]) continue;
+                    const size_t q = (size_t)i * NRHS + c;
+                    x[q] = x[q] + (double)w.xi[q];
+                }
+            }
+        });
         if (!tm.sync()) return;
     }
+    if (a.perm) permute_out<NRHS>(tm, a);
     write_results<NRHS>(a, out, tm.rank);
 }
 
+// 512 threads with up to 128 registers: the fused phases keep four rows per thread
+// in flight without spilling (1024-thread CTAs would cap registers at 64).
+constexpr int grid_block(int) { return 512; }
+
 template <int MIXED, int NRHS, int PREC>
-__global__ void __launch_bounds__(512) solve_grid_kernel(SolveArgs a) {
+__global__ void __launch_bounds__(grid_block(NRHS), 1) solve_grid_kernel(SolveArgs a) {
     __shared__ double smem[32 * kMaxK];
     GridTeam tm(a.ctl);
     if (MIXED) solve_mixed<NRHS, PREC>(tm, a, smem);
@@ -590,32 +837,59 @@ __global__ void cast_kernel(int64_t m, const double* __restrict__ s, V* __restri
         d[i] = (V)s[i];
 }
 
+// Gather the caller's values into the level-permuted CSR (FP64 and, if asked, FP32).
+__global__ void permute_vals_kernel(int64_t nnz, const int* __restrict__ src, const double* __restrict__ v,
+                                    double* __restrict__ p64, float* __restrict__ p32) {
+    for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
+        const double x = v[src[k]];
+        p64[k] = x;
+        if (p32) p32[k] = (float)x;
+    }
+}
+
+// FP32 operator of the MIXED inner iterations: off-diagonals rounded to FP32, the
+// diagonal slot replaced by the FP64 row sum rounded once (difference form, see
+// spmv_range).
+__global__ void rowsum_f32_kernel(int n, const int* __restrict__ ip, const int* __restrict__ ix,
+                                  const double* __restrict__ v64, float* __restrict__ v32) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        double sum = 0.0;
+        int dk = -1;
+        for (int k = ip[i]; k < ip[i + 1]; ++k) {
+            sum += v64[k];
+            if (ix[k] == i) dk = k;
+            else v32[k] = (float)v64[k];
+        }
+        if (dk >= 0) v32[dk] = (float)sum;
+    }
+}
+
 constexpr int kMaxIluRow = 64;
 
-// Structural ILU(0), IKJ order, level by level. One thread per row.
+// Structural ILU(0), IKJ order, on the level-permuted CSR: row i's lower entries
+// are its columns < i (all on earlier levels), processed left to right.
 template <typename V, class Team>
-__device__ void ilu0_factor_body(Team& tm, const SolveArgs& a, const int* __restrict__ src,
-                                 const double* __restrict__ vals) {
+__device__ void ilu0_factor_body(Team& tm, const SolveArgs& a) {
     V* lu = (V*)a.lu;
     V* ldi = (V*)a.ludinv;
+    const double* vals = a.vals64;
     for (int l = 0; l < a.nlev; ++l) {
-        const int b0 = a.lev_ptr[l], m = a.lev_ptr[l + 1] - b0;
-        const int per = (m + tm.size - 1) / tm.size;
-        const int s0 = min(m, tm.rank * per), s1 = min(m, s0 + per);
-        for (int k = s0 + threadIdx.x; k < s1; k += blockDim.x) {
-            const int i = a.lev_rows[b0 + k];
-            const int lo = a.indptr[i], hi = a.indptr[i + 1], dp = a.ilu_diag[i];
+        if (l > 0 && !tm.sync()) return;
+        int s0, s1;
+        level_slice(tm, a, l, s0, s1);
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) {
+            const int lo = a.indptr[i], hi = a.indptr[i + 1], dp = a.diag[i];
             double wv[kMaxIluRow];
-            for (int q = lo; q < hi; ++q) wv[q - lo] = vals[src[q]];
+            for (int q = lo; q < hi; ++q) wv[q - lo] = vals[q];
             for (int kk = lo; kk < dp; ++kk) {
-                const int kr = a.ilu_col[kk];
+                const int kr = a.indices[kk];
                 const double l_ik = wv[kk - lo] * (double)ldi[kr];
                 wv[kk - lo] = l_ik;
                 const int ke = a.indptr[kr + 1];
-                for (int jj = a.ilu_diag[kr] + 1; jj < ke; ++jj) {
-                    const int j = a.ilu_col[jj];
+                for (int jj = a.diag[kr] + 1; jj < ke; ++jj) {
+                    const int j = a.indices[jj];
                     for (int q = kk + 1; q < hi; ++q)
-                        if (a.ilu_col[q] == j) {
+                        if (a.indices[q] == j) {
                             wv[q - lo] -= l_ik * (double)lu[jj];
                             break;
                         }
@@ -625,20 +899,19 @@ __device__ void ilu0_factor_body(Team& tm, const SolveArgs& a, const int* __rest
             const double u = wv[dp - lo];
             ldi[i] = (V)((fabs(u) > 1e-300) ? 1.0 / u : 0.0);
         }
-        if (!tm.sync()) return;
     }
 }
 
 template <typename V>
-__global__ void __launch_bounds__(512) ilu0_factor_grid(SolveArgs a, const int* src, const double* vals) {
+__global__ void __launch_bounds__(1024, 1) ilu0_factor_grid(SolveArgs a) {
     GridTeam tm(a.ctl);
-    ilu0_factor_body<V>(tm, a, src, vals);
+    ilu0_factor_body<V>(tm, a);
 }
 
 template <typename V>
-__global__ void __launch_bounds__(1024) ilu0_factor_cta(SolveArgs a, const int* src, const double* vals) {
+__global__ void __launch_bounds__(1024) ilu0_factor_cta(SolveArgs a) {
     CtaTeam tm;
-    ilu0_factor_body<V>(tm, a, src, vals);
+    ilu0_factor_body<V>(tm, a);
 }
 
 }  // namespace kcfd
@@ -654,13 +927,19 @@ struct kcfd_solver {
     void* work = nullptr;
     double* r64 = nullptr;
     void* dinv = nullptr;
-    // ILU
-    int* ilu_col = nullptr;
-    int* ilu_diag = nullptr;
-    int* ilu_src = nullptr;
+    float* v32own = nullptr;  // MIXED, no permutation: FP32 difference-form operator
     int* lev_ptr = nullptr;
-    int* lev_rows = nullptr;
-    int nlev = 0;
+    int nlev = 1;
+    // ILU: level-permuted CSR owned by the handle
+    int* perm = nullptr;
+    int* p_indptr = nullptr;
+    int* p_indices = nullptr;
+    int* p_src = nullptr;
+    int* p_diag = nullptr;
+    double* p_vals64 = nullptr;
+    float* p_vals32 = nullptr;
+    double* px = nullptr;
+    double* pb = nullptr;
     void* lu = nullptr;
     void* ludinv = nullptr;
     // team control
@@ -691,8 +970,8 @@ void* solve_kernel_ptr(int mixed, int nrhs, int prec, bool grid) {
 
 int free_solver(kcfd_solver* s) {
     if (!s) return KCFD_OK;
-    void* ps[] = {s->work, s->r64, s->dinv, s->ilu_col, s->ilu_diag, s->ilu_src, s->lev_ptr,
-                  s->lev_rows, s->lu, s->ludinv, s->bar, s->partials, s->err};
+    void* ps[] = {s->work, s->r64, s->dinv, s->v32own, s->lev_ptr, s->perm, s->p_indptr, s->p_indices, s->p_src, s->p_diag,
+                  s->p_vals64, s->p_vals32, s->px, s->pb, s->lu, s->ludinv, s->bar, s->partials, s->err};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete s;
@@ -704,23 +983,32 @@ SolveArgs make_args(const kcfd_solver* s, const kcfd_csr_t* A) {
     std::memset(&a, 0, sizeof(a));
     a.n = s->n;
     a.lanes = s->lanes;
-    a.indptr = A->indptr;
-    a.indices = A->indices;
-    a.vals64 = A->vals64;
-    a.vals32 = A->vals32;
+    if (s->perm) {
+        a.indptr = s->p_indptr;
+        a.indices = s->p_indices;
+        a.vals64 = s->p_vals64;
+        a.vals32 = s->p_vals32;
+        a.perm = s->perm;
+        a.px = s->px;
+        a.pb = s->pb;
+    } else {
+        a.indptr = A->indptr;
+        a.indices = A->indices;
+        a.vals64 = A->vals64;
+        a.vals32 = s->v32own;
+    }
     a.dinv = s->dinv;
-    a.ilu_col = s->ilu_col;
-    a.ilu_diag = s->ilu_diag;
+    a.diag = s->p_diag;
     a.lu = s->lu;
     a.ludinv = s->ludinv;
     a.lev_ptr = s->lev_ptr;
-    a.lev_rows = s->lev_rows;
     a.nlev = s->nlev;
     a.work = s->work;
     a.r64 = s->r64;
     a.stop = s->o.stop;
     a.maxiter = s->o.maxiter;
     a.max_refine = s->o.max_refine;
+    a.inner_maxiter = s->o.inner_maxiter;
     a.rtol = s->o.rtol;
     a.atol = s->o.atol;
     a.inner_rtol = s->o.inner_rtol;
@@ -731,8 +1019,7 @@ SolveArgs make_args(const kcfd_solver* s, const kcfd_csr_t* A) {
     return a;
 }
 
-int launch(const kcfd_solver* s, void* kernel, SolveArgs& a, cudaStream_t st) {
-    void* args[] = {&a};
+int launch_team(const kcfd_solver* s, void* kernel, void** args, cudaStream_t st) {
     KCFD_CUDA(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), st));
     KCFD_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), st));
     if (s->team == 2) {
@@ -742,6 +1029,12 @@ int launch(const kcfd_solver* s, void* kernel, SolveArgs& a, cudaStream_t st) {
     }
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
+}
+
+template <typename T>
+bool upload(T** dst, const std::vector<T>& v) {
+    if (cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)) != cudaSuccess) return false;
+    return v.empty() || cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
 }
 
 }  // namespace
@@ -775,8 +1068,9 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     auto* s = new kcfd_solver();
     s->o = *opts;
     if (s->o.mode == KCFD_MODE_MIXED) {
-        if (s->o.inner_rtol <= 0) s->o.inner_rtol = 1e-4;
-        if (s->o.max_refine <= 0) s->o.max_refine = 30;
+        if (s->o.inner_rtol <= 0) s->o.inner_rtol = 1e-3;
+        if (s->o.max_refine <= 0) s->o.max_refine = 60;
+        if (s->o.inner_maxiter <= 0) s->o.inner_maxiter = 400;
     }
     s->n = A->n;
     s->nnz = A->nnz;
@@ -791,46 +1085,105 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     const int nrhs = opts->nrhs;
     const bool mixed = opts->mode == KCFD_MODE_MIXED;
     const size_t vsz = mixed ? sizeof(float) : sizeof(double);
-    // row structure on the host (once per pattern)
-    std::vector<int> ip(A->n + 1), ix(A->nnz);
+    const int n = A->n, nnz = A->nnz;
+    std::vector<int> ip(n + 1), ix(nnz);
     if (cudaMemcpy(ip.data(), A->indptr, ip.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess ||
         cudaMemcpy(ix.data(), A->indices, ix.size() * 4, cudaMemcpyDeviceToHost) != cudaSuccess) {
         free_solver(s);
         set_error("kcfd_solver_create: cannot read the CSR pattern (device pointers expected)");
         return KCFD_BAD_INPUT;
     }
-    if (ip[0] != 0 || ip[A->n] != A->nnz) {
+    auto fail = [&](const char* msg, int a1 = 0, int a2 = 0, int a3 = 0) {
         free_solver(s);
-        set_error("kcfd_solver_create: indptr[0] != 0 or indptr[n] != nnz");
+        set_error(msg, a1, a2, a3);
         return KCFD_BAD_INPUT;
-    }
-    for (int i = 0; i < A->n; ++i) {
-        if (ip[i + 1] < ip[i]) {
-            free_solver(s);
-            set_error("kcfd_solver_create: indptr not monotone at row %d", i);
-            return KCFD_BAD_INPUT;
-        }
-    }
-    for (int k = 0; k < A->nnz; ++k)
-        if (ix[k] < 0 || ix[k] >= A->n) {
-            free_solver(s);
-            set_error("kcfd_solver_create: column index %d out of range at %d", ix[k], k);
-            return KCFD_BAD_INPUT;
-        }
+    };
+    if (ip[0] != 0 || ip[n] != nnz) return fail("kcfd_solver_create: indptr[0] != 0 or indptr[n] != nnz");
+    for (int i = 0; i < n; ++i)
+        if (ip[i + 1] < ip[i]) return fail("kcfd_solver_create: indptr not monotone at row %d", i);
+    for (int k = 0; k < nnz; ++k)
+        if (ix[k] < 0 || ix[k] >= n) return fail("kcfd_solver_create: column index %d out of range at %d", ix[k], k);
     // team and launch shape
     int team = opts->team;
-    if (team == 0) team = ((int64_t)A->n * nrhs <= 40000) ? 1 : 2;
+    if (team == 0) team = ((int64_t)n * nrhs <= 40000) ? 1 : 2;
     s->team = team;
     int lanes = opts->lanes;
     if (lanes <= 0) {
-        double avg = (double)A->nnz / A->n;
+        // one lane streams up to ~8 entries of a row (FVM rows have 4-7): measured
+        // fastest on B200 for 7-point rows; wider rows get more lanes
+        const double avg = (double)nnz / n;
         lanes = 1;
-        while (lanes < 32 && lanes < avg) lanes <<= 1;
+        while (lanes < 32 && 8 * lanes < avg) lanes <<= 1;
     }
-    KCFD_REQUIRE((lanes & (lanes - 1)) == 0 && lanes >= 1 && lanes <= 32, "kcfd_solver_create: lanes must be 1..32 pow2");
+    if ((lanes & (lanes - 1)) != 0 || lanes < 1 || lanes > 32) return fail("kcfd_solver_create: lanes must be 1..32 pow2");
     s->lanes = lanes;
-    s->block = opts->block > 0 ? opts->block : (team == 1 ? 1024 : 512);
-    if (team == 2 && s->block > 512) s->block = 512;
+    const int max_grid_block = grid_block(nrhs);
+    s->block = opts->block > 0 ? opts->block : (team == 1 ? 1024 : max_grid_block);
+    if (team == 2 && s->block > max_grid_block) s->block = max_grid_block;
+    if (team == 1 && s->block > 1024) s->block = 1024;
+    if (s->block % 32 != 0 || s->block < 32) return fail("kcfd_solver_create: block must be a multiple of 32");
+    // levels
+    std::vector<int> lptr;
+    if (opts->precond == KCFD_PREC_ILU0) {
+        std::vector<int> lev(n, 0);
+        if (level_of_row_host) {
+            for (int i = 0; i < n; ++i) lev[i] = level_of_row_host[i];
+        } else {
+            for (int i = 0; i < n; ++i)
+                for (int k = ip[i]; k < ip[i + 1]; ++k)
+                    if (ix[k] < i) lev[i] = std::max(lev[i], lev[ix[k]] + 1);
+        }
+        int nlev = 0;
+        for (int i = 0; i < n; ++i) {
+            if (lev[i] < 0) return fail("kcfd_solver_create: negative level at row %d", i);
+            nlev = std::max(nlev, lev[i] + 1);
+        }
+        // permutation: rows grouped by level, row order kept inside a level
+        lptr.assign(nlev + 1, 0);
+        for (int i = 0; i < n; ++i) lptr[lev[i] + 1]++;
+        for (int l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];
+        std::vector<int> perm(n), inv(n), fill(lptr.begin(), lptr.end() - 1);
+        for (int i = 0; i < n; ++i) {
+            perm[fill[lev[i]]] = i;
+            inv[i] = fill[lev[i]]++;
+        }
+        std::vector<int> pip(n + 1, 0), pix(nnz), psrc(nnz), pdiag(n, -1);
+        std::vector<std::pair<int, int>> row;
+        for (int r = 0; r < n; ++r) {
+            const int o = perm[r];
+            const int len = ip[o + 1] - ip[o];
+            if (len > kMaxIluRow) return fail("kcfd_solver_create: ILU(0) row %d has %d entries (max %d)", o, len, kMaxIluRow);
+            pip[r + 1] = pip[r] + len;
+            row.clear();
+            for (int k = ip[o]; k < ip[o + 1]; ++k) row.emplace_back(inv[ix[k]], k);
+            std::sort(row.begin(), row.end());
+            for (int q = 0; q < len; ++q) {
+                const int c = row[q].first;
+                pix[pip[r] + q] = c;
+                psrc[pip[r] + q] = row[q].second;
+                if (c == r) pdiag[r] = pip[r] + q;
+                else if (lev[perm[c]] == lev[o]) return fail("kcfd_solver_create: coupled rows %d, %d share level %d", o, perm[c], lev[o]);
+            }
+            if (pdiag[r] < 0) return fail("kcfd_solver_create: row %d has no diagonal entry (ILU(0) needs it)", o);
+        }
+        s->nlev = nlev;
+        bool ok = upload(&s->perm, perm) && upload(&s->p_indptr, pip) && upload(&s->p_indices, pix) &&
+                  upload(&s->p_src, psrc) && upload(&s->p_diag, pdiag);
+        ok = ok && cudaMalloc(&s->p_vals64, (size_t)nnz * sizeof(double)) == cudaSuccess;
+        if (mixed) ok = ok && cudaMalloc(&s->p_vals32, (size_t)nnz * sizeof(float)) == cudaSuccess;
+        ok = ok && cudaMalloc(&s->px, (size_t)n * nrhs * sizeof(double)) == cudaSuccess;
+        ok = ok && cudaMalloc(&s->pb, (size_t)n * nrhs * sizeof(double)) == cudaSuccess;
+        ok = ok && cudaMalloc(&s->lu, (size_t)nnz * vsz) == cudaSuccess;
+        ok = ok && cudaMalloc(&s->ludinv, (size_t)n * vsz) == cudaSuccess;
+        if (!ok) {
+            free_solver(s);
+            set_error("kcfd_solver_create: device allocation failed (ILU)");
+            return KCFD_CUDA_ERROR;
+        }
+    } else {
+        lptr = {0, n};
+        s->nlev = 1;
+    }
     void* kern = solve_kernel_ptr(mixed, nrhs, opts->precond, team == 2);
     if (team == 2) {
         int per_sm = 0;
@@ -839,83 +1192,30 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
             set_error("kcfd_solver_create: solver kernel cannot be resident (block %d)", s->block);
             return KCFD_CUDA_ERROR;
         }
-        // a whole number of CTAs per SM, capped so rows per CTA stay meaningful
-        int g = per_sm * s->sm_count;
-        int max_useful = std::max(1, (int)((A->n + s->block - 1) / s->block));
+        int per_sm_f = per_sm;
+        if (opts->precond == KCFD_PREC_ILU0) {
+            void* fk = mixed ? (void*)ilu0_factor_grid<float> : (void*)ilu0_factor_grid<double>;
+            if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_f, fk, s->block, 0) != cudaSuccess || per_sm_f < 1) {
+                free_solver(s);
+                set_error("kcfd_solver_create: ILU factor kernel cannot be resident");
+                return KCFD_CUDA_ERROR;
+            }
+        }
+        const int g = std::min(per_sm, per_sm_f) * s->sm_count;
+        const int max_useful = std::max(1, (int)((n + s->block - 1) / s->block));
         s->grid = std::max(1, std::min(g, max_useful));
     } else {
         s->grid = 1;
     }
-    // allocations
-    const size_t len = (size_t)A->n * nrhs;
-    bool ok = cudaMalloc(&s->work, 9 * len * vsz) == cudaSuccess;
+    const size_t len = (size_t)n * nrhs;
+    bool ok = upload(&s->lev_ptr, lptr);
+    ok = ok && cudaMalloc(&s->work, 9 * len * vsz) == cudaSuccess;
     if (mixed) ok = ok && cudaMalloc(&s->r64, len * sizeof(double)) == cudaSuccess;
     ok = ok && cudaMalloc(&s->bar, 2 * sizeof(unsigned)) == cudaSuccess;
     ok = ok && cudaMalloc(&s->err, sizeof(int)) == cudaSuccess;
     ok = ok && cudaMalloc(&s->partials, (size_t)kSlots * kMaxK * std::max(s->grid, 1) * sizeof(double)) == cudaSuccess;
-    if (ok && opts->precond == KCFD_PREC_JACOBI) ok = cudaMalloc(&s->dinv, A->n * vsz) == cudaSuccess;
-    if (ok && opts->precond == KCFD_PREC_ILU0) {
-        // level of each row: caller's colouring / levels, else natural-order levels
-        std::vector<int> lev(A->n, 0);
-        if (level_of_row_host) {
-            for (int i = 0; i < A->n; ++i) lev[i] = level_of_row_host[i];
-        } else {
-            for (int i = 0; i < A->n; ++i)
-                for (int k = ip[i]; k < ip[i + 1]; ++k)
-                    if (ix[k] < i) lev[i] = std::max(lev[i], lev[ix[k]] + 1);
-        }
-        int nlev = 0;
-        for (int i = 0; i < A->n; ++i) {
-            if (lev[i] < 0) { free_solver(s); set_error("kcfd_solver_create: negative level"); return KCFD_BAD_INPUT; }
-            nlev = std::max(nlev, lev[i] + 1);
-        }
-        std::vector<int> icol(A->nnz), isrc(A->nnz), idiag(A->n);
-        std::vector<int> order;
-        for (int i = 0; i < A->n; ++i) {
-            const int lo = ip[i], hi = ip[i + 1];
-            if (hi - lo > kMaxIluRow) {
-                free_solver(s);
-                set_error("kcfd_solver_create: ILU(0) row %d has %d entries (max %d)", i, hi - lo, kMaxIluRow);
-                return KCFD_BAD_INPUT;
-            }
-            order.resize(hi - lo);
-            for (int k = lo; k < hi; ++k) order[k - lo] = k;
-            auto key = [&](int k) { return std::make_pair(lev[ix[k]], ix[k]); };
-            std::sort(order.begin(), order.end(), [&](int x, int y) { return key(x) < key(y); });
-            idiag[i] = -1;
-            for (int q = 0; q < hi - lo; ++q) {
-                const int k = order[q];
-                icol[lo + q] = ix[k];
-                isrc[lo + q] = k;
-                if (ix[k] == i) idiag[i] = lo + q;
-                else if (lev[ix[k]] == lev[i]) {
-                    free_solver(s);
-                    set_error("kcfd_solver_create: rows %d and %d are coupled but share level %d", i, ix[k], lev[i]);
-                    return KCFD_BAD_INPUT;
-                }
-            }
-            if (idiag[i] < 0) {
-                free_solver(s);
-                set_error("kcfd_solver_create: row %d has no diagonal entry (ILU(0) needs it)", i);
-                return KCFD_BAD_INPUT;
-            }
-        }
-        std::vector<int> lptr(nlev + 1, 0), lrows(A->n);
-        for (int i = 0; i < A->n; ++i) lptr[lev[i] + 1]++;
-        for (int l = 0; l < nlev; ++l) lptr[l + 1] += lptr[l];
-        std::vector<int> fill(lptr.begin(), lptr.end() - 1);
-        for (int i = 0; i < A->n; ++i) lrows[fill[lev[i]]++] = i;
-        s->nlev = nlev;
-        ok = cudaMalloc(&s->ilu_col, A->nnz * 4) == cudaSuccess && cudaMalloc(&s->ilu_src, A->nnz * 4) == cudaSuccess &&
-             cudaMalloc(&s->ilu_diag, A->n * 4) == cudaSuccess && cudaMalloc(&s->lev_ptr, (nlev + 1) * 4) == cudaSuccess &&
-             cudaMalloc(&s->lev_rows, A->n * 4) == cudaSuccess && cudaMalloc(&s->lu, A->nnz * vsz) == cudaSuccess &&
-             cudaMalloc(&s->ludinv, A->n * vsz) == cudaSuccess;
-        ok = ok && cudaMemcpy(s->ilu_col, icol.data(), A->nnz * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(s->ilu_src, isrc.data(), A->nnz * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(s->ilu_diag, idiag.data(), A->n * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(s->lev_ptr, lptr.data(), (nlev + 1) * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
-             cudaMemcpy(s->lev_rows, lrows.data(), A->n * 4, cudaMemcpyHostToDevice) == cudaSuccess;
-    }
+    if (ok && opts->precond == KCFD_PREC_JACOBI) ok = cudaMalloc(&s->dinv, n * vsz) == cudaSuccess;
+    if (ok && mixed && !s->perm) ok = cudaMalloc(&s->v32own, (size_t)nnz * sizeof(float)) == cudaSuccess;
     if (ok) ok = cudaMemset(s->bar, 0, 2 * sizeof(unsigned)) == cudaSuccess && cudaMemset(s->err, 0, sizeof(int)) == cudaSuccess;
     if (!ok) {
         free_solver(s);
@@ -935,28 +1235,28 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
     cudaStream_t st = (cudaStream_t)stream;
     const bool mixed = s->o.mode == KCFD_MODE_MIXED;
     const int threads = 256;
-    const int blocks = std::min((s->n + threads - 1) / threads, s->sm_count * 8);
+    const int rblocks = std::min((s->n + threads - 1) / threads, s->sm_count * 8);
+    if (mixed && !s->perm) {
+        rowsum_f32_kernel<<<rblocks, threads, 0, st>>>(s->n, A->indptr, A->indices, A->vals64, s->v32own);
+        KCFD_CUDA(cudaGetLastError());
+    }
     if (s->o.precond == KCFD_PREC_JACOBI) {
+        const int blocks = std::min((s->n + threads - 1) / threads, s->sm_count * 8);
         if (mixed)
             jacobi_setup_kernel<float><<<blocks, threads, 0, st>>>(s->n, A->indptr, A->indices, A->vals64, (float*)s->dinv);
         else
             jacobi_setup_kernel<double><<<blocks, threads, 0, st>>>(s->n, A->indptr, A->indices, A->vals64, (double*)s->dinv);
         KCFD_CUDA(cudaGetLastError());
     } else if (s->o.precond == KCFD_PREC_ILU0) {
-        SolveArgs a = make_args(s, A);
-        KCFD_CUDA(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), st));
-        KCFD_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), st));
-        const int* src = s->ilu_src;
-        const double* vals = A->vals64;
-        void* args[] = {&a, (void*)&src, (void*)&vals};
-        if (s->team == 2) {
-            void* k = mixed ? (void*)ilu0_factor_grid<float> : (void*)ilu0_factor_grid<double>;
-            KCFD_CUDA(cudaLaunchCooperativeKernel(k, dim3(s->grid), dim3(s->block), args, 0, st));
-        } else {
-            void* k = mixed ? (void*)ilu0_factor_cta<float> : (void*)ilu0_factor_cta<double>;
-            KCFD_CUDA(cudaLaunchKernel(k, dim3(1), dim3(s->block), args, 0, st));
-        }
+        const int blocks = (int)std::min<int64_t>(((int64_t)s->nnz + threads - 1) / threads, s->sm_count * 16);
+        permute_vals_kernel<<<blocks, threads, 0, st>>>(s->nnz, s->p_src, A->vals64, s->p_vals64, nullptr);
+        if (mixed) rowsum_f32_kernel<<<rblocks, threads, 0, st>>>(s->n, s->p_indptr, s->p_indices, s->p_vals64, s->p_vals32);
         KCFD_CUDA(cudaGetLastError());
+        SolveArgs a = make_args(s, A);
+        void* args[] = {&a};
+        void* k = s->team == 2 ? (mixed ? (void*)ilu0_factor_grid<float> : (void*)ilu0_factor_grid<double>)
+                               : (mixed ? (void*)ilu0_factor_cta<float> : (void*)ilu0_factor_cta<double>);
+        return launch_team(s, k, args, st);
     }
     return KCFD_OK;
 }
@@ -967,20 +1267,19 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
     KCFD_REQUIRE(A->n == s->n && A->nnz == s->nnz, "kcfd_solver_solve: matrix size differs from the bound pattern");
     const bool mixed = s->o.mode == KCFD_MODE_MIXED;
     KCFD_REQUIRE(A->vals64 != nullptr, "kcfd_solver_solve: FP64 values required");
-    KCFD_REQUIRE(!mixed || A->vals32 != nullptr, "kcfd_solver_solve: MIXED needs FP32 values (vals32)");
+    // MIXED: the FP32 operator is the handle's own (built by kcfd_solver_setup)
     SolveArgs a = make_args(s, A);
     a.x = x;
     a.b = b;
     a.iters_out = iters;
     a.relres_out = relres;
     a.status_out = status;
-    cudaStream_t st = (cudaStream_t)stream;
     void* kern = solve_kernel_ptr(mixed, s->o.nrhs, s->o.precond, s->team == 2);
     KCFD_REQUIRE(kern != nullptr, "kcfd_solver_solve: no kernel for this configuration");
-    return launch(s, kern, a, st);
+    void* args[] = {&a};
+    return launch_team(s, kern, args, (cudaStream_t)stream);
 }
 
-// Error flag of the last solve's team barriers (KCFD_TIMEOUT when a wait expired).
 int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream) {
     KCFD_REQUIRE(s && err, "kcfd_solver_error: NULL argument");
     KCFD_CUDA(cudaMemcpyAsync(err, s->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
@@ -998,7 +1297,7 @@ __global__ void spmv_kernel(int n, const int* __restrict__ ip, const int* __rest
     const int rows_per_cta = (blockDim.x / L);
     for (int r0 = blockIdx.x * rows_per_cta; r0 < n; r0 += gridDim.x * rows_per_cta) {
         const int r1 = min(n, r0 + rows_per_cta);
-        spmv_range<VM, VX, NRHS>(ip, ix, val, x, r0, r1, L, [&](int i, double* acc) {
+        spmv_range<VM, VX, NRHS>(ip, ix, val, x, r0, r1, L, [&](int i, const double* acc) {
 #pragma unroll
             for (int c = 0; c < NRHS; ++c) y[(size_t)i * NRHS + c] = (VX)acc[c];
         });

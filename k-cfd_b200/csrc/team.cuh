@@ -52,7 +52,7 @@ __device__ __forceinline__ void block_sum(double (&v)[K], double* smem) {
 }
 
 struct TeamCtl {
-    unsigned int* bar;     // [2] arrive counter, generation
+    unsigned int* bar;     // barrier counter (see GridTeam::sync)
     double* partials;      // [slots * kMaxK * size]
     int* err;              // KCFD_TIMEOUT when a barrier wait expired
     long long budget;      // clock64 cycles a barrier may wait
@@ -79,35 +79,32 @@ struct GridTeam {
     TeamCtl ctl;
     __device__ GridTeam(const TeamCtl& c) : rank(blockIdx.x), size(gridDim.x), ctl(c) {}
 
-    // Grid barrier: arrive on a counter; the last CTA resets it and bumps the
-    // generation. Waiters poll the generation with a clock64 budget.
+    // Grid barrier on one 32-bit counter (zeroed before the launch): CTA 0 adds
+    // 2^31 - (size - 1), every other CTA adds 1, so the top bit flips exactly when the
+    // last CTA arrives; a waiter polls until the top bit differs from the value it saw
+    // on arrival. A CTA cannot arrive at the next barrier before this one completed,
+    // so the flip cannot be undone under a waiter. Waits are bounded by a clock64
+    // budget; on expiry the CTA records KCFD_TIMEOUT and every later wait fails fast.
     __device__ bool sync() {
         __shared__ int ok_s;
         __syncthreads();
         if (threadIdx.x == 0) {
-            volatile unsigned int* vgen = ctl.bar + 1;
+            volatile unsigned int* vbar = ctl.bar;
             volatile int* verr = ctl.err;
-            unsigned int gen = *vgen;
             int ok = (*verr == 0);
+            const unsigned int add = (rank == 0) ? (0x80000000u - (unsigned)(size - 1)) : 1u;
             __threadfence();
-            unsigned int arrived = atomicAdd(ctl.bar, 1u);
-            if (arrived == (unsigned)size - 1) {
-                ctl.bar[0] = 0;
-                __threadfence();
-                atomicAdd(ctl.bar + 1, 1u);
-            } else {
-                long long t0 = clock64();
-                while (*vgen == gen) {
-                    if (*verr != 0) {
-                        ok = 0;
-                        break;
-                    }
-                    if (clock64() - t0 > ctl.budget) {
-                        atomicCAS(ctl.err, 0, 5 /*KCFD_TIMEOUT*/);
-                        ok = 0;
-                        break;
-                    }
-                    __nanosleep(64);
+            const unsigned int old = atomicAdd(ctl.bar, add);
+            long long t0 = clock64();
+            while (ok && (((old ^ *vbar) & 0x80000000u) == 0)) {
+                if (*verr != 0) {
+                    ok = 0;
+                    break;
+                }
+                if (clock64() - t0 > ctl.budget) {
+                    atomicCAS(ctl.err, 0, 5 /*KCFD_TIMEOUT*/);
+                    ok = 0;
+                    break;
                 }
             }
             __threadfence();
@@ -129,9 +126,11 @@ struct GridTeam {
         if (wid == 0) {
 #pragma unroll
             for (int k = 0; k < K; ++k) {
-                const volatile double* src = base + (size_t)k * size;
+                // after the barrier's fence: L2 loads (.cg), all issued before the sums
+                const double* src = base + (size_t)k * size;
                 double t = 0.0;
-                for (int j = lane; j < size; j += 32) t += src[j];
+#pragma unroll 8
+                for (int j = lane; j < size; j += 32) t += __ldcg(src + j);
                 t = warp_sum(t);
                 if (lane == 0) smem[k * 32] = t;
             }

@@ -50,7 +50,7 @@ class _Field:
 class SIMPLESolver:
     def __init__(self, mesh, rho=1.0, mu=1e-3, precision="fp64", precond_p="jacobi", ilu_order="color",
                  rtol=1e-8, maxiter=10000, muscl=None, nonorth=False, graph=False, team=0, lanes=0,
-                 inner_rtol=1e-4, device="cuda"):
+                 inner_rtol=1e-3, inner_maxiter=400, device="cuda"):
         torch = _lib.require_cuda()
         if not isinstance(mesh, Mesh):
             mesh = from_fvmesh(mesh)
@@ -95,12 +95,12 @@ class SIMPLESolver:
         self.A_p = DeviceCSR(ip, ix, torch.zeros(nnz, **f64),
                              torch.zeros(nnz, dtype=torch.float32, device=device) if mixed else None)
         self.s_m = Solver(self.A_m, precond="jacobi", mode=self.mode, nrhs=D, maxiter=maxiter, rtol=rtol,
-                          team=team, lanes=lanes, inner_rtol=inner_rtol)
+                          team=team, lanes=lanes, inner_rtol=inner_rtol, inner_maxiter=inner_maxiter)
         levels = None
         if precond_p == "ilu0":
             levels = mesh.cell_color if ilu_order == "color" else mesh.level_natural
         self.s_p = Solver(self.A_p, precond=precond_p, mode=self.mode, nrhs=1, maxiter=maxiter, rtol=rtol,
-                          team=team, lanes=lanes, inner_rtol=inner_rtol, levels=levels)
+                          team=team, lanes=lanes, inner_rtol=inner_rtol, inner_maxiter=inner_maxiter, levels=levels)
         self.U = _Field(self, "U_t")
         self.p = _Field(self, "p_t")
         self._graph = None

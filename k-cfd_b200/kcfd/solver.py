@@ -83,7 +83,8 @@ class Solver:
     """
 
     def __init__(self, csr, precond="jacobi", stop=_lib.STOP_SCIPY, mode=_lib.MODE_FP64, nrhs=1, maxiter=1000,
-                 rtol=1e-8, atol=0.0, team=0, lanes=0, block=0, inner_rtol=1e-4, max_refine=30, levels=None):
+                 rtol=1e-8, atol=0.0, team=0, lanes=0, block=0, inner_rtol=1e-3, max_refine=60, levels=None,
+                 inner_maxiter=400):
         torch = _lib.require_cuda()
         if precond not in _lib.PREC:
             raise ValueError(f"Unknown preconditioner: {precond}")
@@ -91,6 +92,7 @@ class Solver:
         o.precond, o.stop, o.mode, o.nrhs, o.maxiter = _lib.PREC[precond], stop, mode, nrhs, int(maxiter)
         o.team, o.lanes, o.block = team, lanes, block
         o.rtol, o.atol, o.inner_rtol, o.max_refine = float(rtol), float(atol), float(inner_rtol), int(max_refine)
+        o.inner_maxiter = int(inner_maxiter)
         self.opts = o
         self.n, self.nrhs, self.mode = csr.n, nrhs, mode
         self.precond = precond

@@ -273,6 +273,24 @@ int kcfd_simple_residual(int32_t ndim, const double* mom_norms2, const double* p
  * barrier wait expired, else 0). Synchronises the stream.                         */
 int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream);
 
+/* ------------------------------------------- allocation-free solve ---------- */
+/* No counterpart in the reference. For callers that cannot call cudaMalloc --
+ * code running during CUDA graph capture, real-time loops that must not block on
+ * the allocator, hosts confined to a pre-reserved memory budget -- this solves
+ * one system of at most kcfd_noalloc_max_rows() rows (32768) with the single-CTA
+ * FP64 BiCGSTAB (precond KCFD_PREC_NONE or KCFD_PREC_JACOBI, stop rule as in
+ * kcfd_solver_create) and allocates nothing: its Krylov vectors live in a fixed
+ * array inside libkcfd (about 2.6 MB held on every GPU that loads the library until
+ * the process exits). Larger systems are rejected with KCFD_BAD_INPUT. The first
+ * call on a device looks up the array's device address, so make that call before
+ * any stream capture. All calls share the array: calls that overlap on the GPU
+ * (on different streams) race. A, b, x (x0 on entry), iters, relres and status
+ * are caller device memory, as in kcfd_solver_solve.                              */
+int kcfd_noalloc_max_rows(void);
+int kcfd_bicgstab_noalloc(const kcfd_csr_t* A, const double* b, double* x, int32_t precond, int32_t stop,
+                          double rtol, double atol, int32_t maxiter, int32_t* iters, double* relres,
+                          int32_t* status, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

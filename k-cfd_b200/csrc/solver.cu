@@ -32,6 +32,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <mutex>
 #include <vector>
 
 #include "kcfd_common.h"
@@ -1284,6 +1285,125 @@ int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream) {
     KCFD_REQUIRE(s && err, "kcfd_solver_error: NULL argument");
     KCFD_CUDA(cudaMemcpyAsync(err, s->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     KCFD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return KCFD_OK;
+}
+
+}  // extern "C"
+
+// ------------------------------------------------ allocation-free entry point --
+// Some callers cannot allocate device memory: code running while a CUDA graph is
+// being captured (cudaMalloc is not allowed then), real-time loops that must not
+// block on the allocator, and hosts that run inside a fixed, pre-reserved memory
+// budget. kcfd_bicgstab_noalloc serves them: it solves one small system with the
+// single-CTA BiCGSTAB kernel and takes its Krylov vectors, Jacobi diagonal and level
+// table from the fixed array below instead of a solver handle's cudaMalloc'd scratch.
+//
+// The array is a file-scope __device__ variable: every GPU that loads libkcfd holds
+// it (kNoAllocBytes) until the process exits. Host code must not pass its host-side
+// symbol to a kernel; the device address is looked up once per device with
+// cudaGetSymbolAddress, on the first call made on that device (so that first call
+// should come before any stream capture). All calls share the array and it keeps the
+// last call's contents; the kernels re-initialise every vector they read, and calls
+// that overlap on the GPU (different streams) race on it.
+namespace kcfd {
+constexpr int kNoAllocMaxRows = 32768;                      // largest system accepted
+constexpr int kNoAllocVecs = 10;                            // 9 Krylov vectors + 1/diag
+constexpr size_t kNoAllocDoubles = (size_t)kNoAllocVecs * kNoAllocMaxRows + 32;  // + level table
+static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
+
+__global__ void noalloc_prep_kernel(int n, const int* __restrict__ ip, const int* __restrict__ ix,
+                                    const double* __restrict__ vals, int jacobi, double* __restrict__ dinv,
+                                    int* __restrict__ lev_ptr) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (jacobi) {
+            double d = 0.0;
+            for (int k = ip[i]; k < ip[i + 1]; ++k)
+                if (ix[k] == i) d += vals[k];
+            dinv[i] = (fabs(d) > 1e-30) ? 1.0 / d : 0.0;
+        }
+        if (i == 0) {
+            lev_ptr[0] = 0;
+            lev_ptr[1] = n;
+        }
+    }
+}
+
+// Device address of g_noalloc_scratch per device (looked up once).
+static std::mutex g_noalloc_mu;
+static double* g_noalloc_ptr[64] = {};
+
+static int noalloc_scratch(double** out) {
+    int dev = 0;
+    KCFD_CUDA(cudaGetDevice(&dev));
+    KCFD_REQUIRE(dev >= 0 && dev < 64, "kcfd_bicgstab_noalloc: device index %d out of range", dev);
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || !p) {
+            set_error("kcfd_bicgstab_noalloc: cudaGetSymbolAddress failed: %s", cudaGetErrorString(e));
+            return KCFD_CUDA_ERROR;
+        }
+        g_noalloc_ptr[dev] = (double*)p;
+    }
+    *out = g_noalloc_ptr[dev];
+    return KCFD_OK;
+}
+}  // namespace kcfd
+
+extern "C" {
+
+int kcfd_noalloc_max_rows(void) { return kcfd::kNoAllocMaxRows; }
+
+int kcfd_bicgstab_noalloc(const kcfd_csr_t* A, const double* b, double* x, int32_t precond, int32_t stop,
+                          double rtol, double atol, int32_t maxiter, int32_t* iters, double* relres,
+                          int32_t* status, void* stream) {
+    KCFD_REQUIRE(A, "kcfd_bicgstab_noalloc: NULL matrix");
+    KCFD_REQUIRE(A->n > 0 && A->n <= kcfd::kNoAllocMaxRows,
+                 "kcfd_bicgstab_noalloc: n = %d rows; this entry point takes 1..%d rows (use a solver handle above that)",
+                 A->n, kcfd::kNoAllocMaxRows);
+    KCFD_REQUIRE(A->indptr && A->indices && A->vals64 && b && x, "kcfd_bicgstab_noalloc: NULL argument");
+    KCFD_REQUIRE(precond == KCFD_PREC_NONE || precond == KCFD_PREC_JACOBI,
+                 "kcfd_bicgstab_noalloc: precond must be KCFD_PREC_NONE or KCFD_PREC_JACOBI");
+    KCFD_REQUIRE(stop == KCFD_STOP_SCIPY || stop == KCFD_STOP_GPU, "kcfd_bicgstab_noalloc: bad stop rule");
+    KCFD_REQUIRE(maxiter >= 0, "kcfd_bicgstab_noalloc: maxiter < 0");
+    double* scratch = nullptr;
+    if (int e = kcfd::noalloc_scratch(&scratch)) return e;
+    const int n = A->n;
+    double* work = scratch;                                     // 9 vectors of n
+    double* dinv = scratch + (size_t)9 * kcfd::kNoAllocMaxRows;  // n
+    int* lev_ptr = (int*)(scratch + (size_t)kcfd::kNoAllocVecs * kcfd::kNoAllocMaxRows);
+    cudaStream_t st = (cudaStream_t)stream;
+    const int threads = 256;
+    const int blocks = (n + threads - 1) / threads;
+    kcfd::noalloc_prep_kernel<<<blocks, threads, 0, st>>>(n, A->indptr, A->indices, A->vals64,
+                                                          precond == KCFD_PREC_JACOBI, dinv, lev_ptr);
+    KCFD_CUDA(cudaGetLastError());
+    kcfd::SolveArgs a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.lanes = 1;
+    a.indptr = A->indptr;
+    a.indices = A->indices;
+    a.vals64 = A->vals64;
+    a.dinv = dinv;
+    a.lev_ptr = lev_ptr;
+    a.nlev = 1;
+    a.work = work;
+    a.x = x;
+    a.b = b;
+    a.stop = stop;
+    a.maxiter = maxiter;
+    a.rtol = rtol;
+    a.atol = atol;
+    a.iters_out = iters;
+    a.relres_out = relres;
+    a.status_out = status;
+    void* args[] = {&a};
+    void* kern = precond == KCFD_PREC_JACOBI ? (void*)kcfd::solve_cta_kernel<0, 1, KCFD_PREC_JACOBI>
+                                             : (void*)kcfd::solve_cta_kernel<0, 1, KCFD_PREC_NONE>;
+    KCFD_CUDA(cudaLaunchKernel(kern, dim3(1), dim3(1024), args, 0, st));
+    KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }
 

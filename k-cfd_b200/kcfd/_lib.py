@@ -68,6 +68,8 @@ SIGNATURES = {
     "kcfd_simple_correct": (i32, [vp, f64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_residual_norms": (i32, [C.POINTER(Csr), vp, vp, i32, vp, vp, vp]),
     "kcfd_simple_residual": (i32, [i32, vp, vp, vp, vp, vp, i32, vp]),
+    "kcfd_noalloc_max_rows": (i32, []),
+    "kcfd_bicgstab_noalloc": (i32, [C.POINTER(Csr), vp, vp, i32, i32, f64, f64, i32, vp, vp, vp, vp]),
 }
 
 REDUCE_SCRATCH = 8192

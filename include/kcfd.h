@@ -163,6 +163,30 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
                       int32_t* iters, double* relres, int32_t* status, void* stream);
 
 
+/* ------------------------------------------------------ batched systems ---- */
+/* Many independent systems (e.g. the pressure-correction systems of many meshes) of
+ * uneven sizes solved in ONE persistent launch over packed CSR with per-system
+ * offsets: each CTA takes the next system from a largest-first queue and solves it
+ * alone (FP64 or MIXED BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule
+ * per system). No counterpart API in the reference, which solves one system per call
+ * (core/linear_solver.py:14-70); results per system equal that path's semantics.     */
+typedef struct kcfd_batch kcfd_batch;
+typedef struct {
+    int32_t precond, stop, mode, maxiter, lanes, max_refine, inner_maxiter, pad;
+    double  rtol, atol, inner_rtol;
+} kcfd_batch_opts_t;
+/* indptr_host: per system n[s]+1 local row pointers, concatenated; indices_host:
+ * local column indices, concatenated (host arrays, copied to the device).          */
+int  kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const int32_t* indptr_host,
+                       const int32_t* indices_host, const kcfd_batch_opts_t* opts, kcfd_batch** out);
+void kcfd_batch_destroy(kcfd_batch* b);
+/* info[0..3] = nsys, total rows, total entries, CTAs per launch */
+int  kcfd_batch_info(const kcfd_batch* b, int64_t* info);
+/* vals64, rhs, x: packed device arrays (system s at its row / entry offset); x holds
+ * x0 on entry. iters/relres/status: device arrays of nsys entries.                 */
+int  kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, double* x, int32_t* iters,
+                      double* relres, int32_t* status, void* stream);
+
 /* ------------------------------------------------------- device mesh -------- */
 /* Device-resident SoA mesh. Faces are stored colour by colour: internal faces first
  * (colours 0..n_colors_int-1), then boundary faces (n_colors_bnd colours); no two
@@ -212,6 +236,32 @@ typedef struct {
     int32_t limiter;               /* KCFD_LIM_*: MUSCL deferred correction, NONE = upwind */
     int32_t nonorth;               /* 1: over-relaxed non-orthogonal correction           */
 } kcfd_mom_params_t;
+
+
+/* ------------------------------------------------ generic FVM operators ---- */
+/* Each operator ADDS into a device system (vals64: CSR values on the mesh's
+ * pattern, diag: the tracked diagonal of FVMSystem, rhs), like the reference's COO
+ * triplets summed by to_sparse() (core/fvm_operators.py:13-56). Face operators run
+ * one launch per face colour.                                                     */
+/* diffusion_operator (core/fvm_operators.py:59-100): harmonic-mean gamma, |d_PN|. */
+int kcfd_op_diffusion(const kcfd_dmesh_t* m, const double* gamma, double* vals, double* diag, void* stream);
+/* convection_operator_upwind (core/fvm_operators.py:103-129); mf in device face order. */
+int kcfd_op_convection_upwind(const kcfd_dmesh_t* m, const double* mf, double* vals, double* diag, void* stream);
+/* apply_boundary_conditions (core/fvm_operators.py:178-225). Per boundary face:
+ * btype 0 zero_gradient / 1 dirichlet / 2 neumann, bval = phi_b, bgrad = neumann value. */
+int kcfd_op_boundary(const kcfd_dmesh_t* m, const int8_t* btype, const double* bval, const double* bgrad,
+                     const double* gamma, const double* mf, double* vals, double* diag, double* rhs, void* stream);
+/* Cell operators (core/fvm_operators.py:132-175, 228-240):
+ *   kind 0 temporal_operator   a0 = rho, a1 = dt, p0 = phi_old
+ *   kind 1 source_term         p0 = S
+ *   kind 2 linearized_source   p0 = Sp, p1 = Su
+ *   kind 3 under_relax         a0 = alpha, p0 = phi (reads the tracked diagonal)     */
+int kcfd_op_cells(const kcfd_dmesh_t* m, int32_t kind, double a0, double a1, const double* p0, const double* p1,
+                  double* vals, double* diag, double* rhs, void* stream);
+/* muscl_deferred_correction (core/interpolation.py:227-303): corr[n] (overwritten)
+ * from phi, mf (device face order) and grad [n][ndim]; limiter KCFD_LIM_*.        */
+int kcfd_muscl_correction(const kcfd_dmesh_t* m, int32_t limiter, const double* phi, const double* mf,
+                          const double* grad, double* corr, void* stream);
 
 /* ------------------------------------------------ SIMPLE assembly kernels --- */
 /* Face mass flux F = rho (u_f . n) A, u_f = gc U_O + (1-gc) U_N inside, the

@@ -34,6 +34,7 @@
 #include <cstring>
 #include <mutex>
 #include <vector>
+#include <type_traits>
 
 #include "kcfd_common.h"
 #include "team.cuh"
@@ -820,6 +821,113 @@ __global__ void __launch_bounds__(1024) solve_cta_kernel(SolveArgs a) {
     else solve_fp64<NRHS, PREC>(tm, a, smem);
 }
 
+// ------------------------------------------------------------- batched systems --
+// Many independent systems of uneven size in ONE persistent launch: each CTA takes
+// the next system from a queue (largest first), builds its Jacobi inverse diagonal and
+// FP32 difference-form operator row by row, and solves it alone (CtaTeam: block
+// barriers and block reductions only, no inter-CTA waits). A system's result does not
+// depend on which CTA ran it or on what ran beside it.
+struct BatchSys {
+    int n, nnz;
+    long long row_off;  // rows before this system in the packed vectors
+    long long ptr_off;  // offset of its (n + 1) row pointers
+    long long nnz_off;  // offset of its entries
+};
+
+struct BatchArgs {
+    int nsys, lanes, mixed, precond, stop, maxiter, max_refine, inner_maxiter;
+    double rtol, atol, inner_rtol;
+    const BatchSys* sys;
+    const int* order;
+    int* queue;
+    const int* indptr;
+    const int* indices;
+    const double* vals64;
+    float* vals32;
+    void* dinv;
+    int* lev;
+    void* work;
+    double* r64;
+    double* x;
+    const double* b;
+    int* iters;
+    double* relres;
+    int* status;
+};
+
+template <typename V>
+__device__ void batch_prep(const BatchArgs& B, const BatchSys& S, int sid, V* dinv, float* v32, bool mixed) {
+    const int* ip = B.indptr + S.ptr_off;
+    const int* ix = B.indices + S.nnz_off;
+    const double* v = B.vals64 + S.nnz_off;
+    for (int i = threadIdx.x; i < S.n; i += blockDim.x) {
+        double d = 0.0, sum = 0.0;
+        int dk = -1;
+        for (int k = ip[i]; k < ip[i + 1]; ++k) {
+            sum += v[k];
+            if (ix[k] == i) {
+                d += v[k];
+                dk = k;
+            } else if (mixed) {
+                v32[k] = (float)v[k];
+            }
+        }
+        if (mixed && dk >= 0) v32[dk] = (float)sum;
+        if (B.precond == KCFD_PREC_JACOBI) dinv[i] = (V)((fabs(d) > 1e-30) ? 1.0 / d : 0.0);
+    }
+    if (threadIdx.x == 0) {
+        B.lev[2 * sid] = 0;
+        B.lev[2 * sid + 1] = S.n;
+    }
+}
+
+template <int MIXED, int PREC>
+__global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs B) {
+    __shared__ double smem[32 * kMaxK];
+    __shared__ int s_q;
+    using V = typename std::conditional<MIXED, float, double>::type;
+    CtaTeam tm;
+    for (;;) {
+        if (threadIdx.x == 0) s_q = atomicAdd(B.queue, 1);
+        __syncthreads();
+        const int q = s_q;
+        __syncthreads();
+        if (q >= B.nsys) break;
+        const int sid = B.order[q];
+        const BatchSys S = B.sys[sid];
+        SolveArgs a;
+        memset(&a, 0, sizeof(a));
+        a.n = S.n;
+        a.lanes = B.lanes;
+        a.indptr = B.indptr + S.ptr_off;
+        a.indices = B.indices + S.nnz_off;
+        a.vals64 = B.vals64 + S.nnz_off;
+        a.vals32 = B.vals32 ? B.vals32 + S.nnz_off : nullptr;
+        a.dinv = (V*)B.dinv + S.row_off;
+        a.lev_ptr = B.lev + 2 * sid;
+        a.nlev = 1;
+        a.work = (V*)B.work + 9 * S.row_off;
+        a.x = B.x + S.row_off;
+        a.b = B.b + S.row_off;
+        a.r64 = B.r64 ? B.r64 + S.row_off : nullptr;
+        a.stop = B.stop;
+        a.maxiter = B.maxiter;
+        a.max_refine = B.max_refine;
+        a.inner_maxiter = B.inner_maxiter;
+        a.rtol = B.rtol;
+        a.atol = B.atol;
+        a.inner_rtol = B.inner_rtol;
+        a.iters_out = B.iters + sid;
+        a.relres_out = B.relres + sid;
+        a.status_out = B.status + sid;
+        batch_prep<V>(B, S, sid, (V*)a.dinv, (float*)a.vals32, MIXED);
+        __syncthreads();
+        if (MIXED) solve_mixed<1, PREC>(tm, a, smem);
+        else solve_fp64<1, PREC>(tm, a, smem);
+        __syncthreads();
+    }
+}
+
 // ---------------------------------------------------------------- set-up kernels --
 template <typename V>
 __global__ void jacobi_setup_kernel(int n, const int* __restrict__ ip, const int* __restrict__ ix,
@@ -1285,6 +1393,177 @@ int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream) {
     KCFD_REQUIRE(s && err, "kcfd_solver_error: NULL argument");
     KCFD_CUDA(cudaMemcpyAsync(err, s->err, sizeof(int), cudaMemcpyDeviceToHost, (cudaStream_t)stream));
     KCFD_CUDA(cudaStreamSynchronize((cudaStream_t)stream));
+    return KCFD_OK;
+}
+
+}  // extern "C"
+
+// ---------------------------------------------------------- batched host side --
+struct kcfd_batch {
+    kcfd_batch_opts_t o;
+    int nsys = 0;
+    long long n_total = 0, nnz_total = 0;
+    int grid = 0;
+    BatchSys* sys = nullptr;
+    int* order = nullptr;
+    int* queue = nullptr;
+    int* indptr = nullptr;
+    int* indices = nullptr;
+    float* vals32 = nullptr;
+    void* dinv = nullptr;
+    int* lev = nullptr;
+    void* work = nullptr;
+    double* r64 = nullptr;
+};
+
+namespace {
+int free_batch(kcfd_batch* b) {
+    if (!b) return KCFD_OK;
+    void* ps[] = {b->sys, b->order, b->queue, b->indptr, b->indices, b->vals32, b->dinv, b->lev, b->work, b->r64};
+    for (void* p : ps)
+        if (p) cudaFree(p);
+    delete b;
+    return KCFD_OK;
+}
+void* batch_kernel_ptr(int mixed, int precond) {
+    if (mixed) return precond == KCFD_PREC_JACOBI ? (void*)batch_kernel<1, KCFD_PREC_JACOBI> : (void*)batch_kernel<1, KCFD_PREC_NONE>;
+    return precond == KCFD_PREC_JACOBI ? (void*)batch_kernel<0, KCFD_PREC_JACOBI> : (void*)batch_kernel<0, KCFD_PREC_NONE>;
+}
+}  // namespace
+
+extern "C" {
+
+int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const int32_t* indptr_host,
+                      const int32_t* indices_host, const kcfd_batch_opts_t* opts, kcfd_batch** out) {
+    KCFD_REQUIRE(out && opts && n && nnz && indptr_host && indices_host, "kcfd_batch_create: NULL argument");
+    *out = nullptr;
+    KCFD_REQUIRE(nsys > 0, "kcfd_batch_create: nsys must be > 0");
+    KCFD_REQUIRE(opts->precond == KCFD_PREC_NONE || opts->precond == KCFD_PREC_JACOBI,
+                 "kcfd_batch_create: precond must be none or jacobi");
+    KCFD_REQUIRE(opts->mode == KCFD_MODE_FP64 || opts->mode == KCFD_MODE_MIXED, "kcfd_batch_create: bad mode");
+    KCFD_REQUIRE(opts->stop == KCFD_STOP_SCIPY || (opts->stop == KCFD_STOP_GPU && opts->mode == KCFD_MODE_FP64),
+                 "kcfd_batch_create: bad stop rule");
+    auto* b = new kcfd_batch();
+    b->o = *opts;
+    if (b->o.mode == KCFD_MODE_MIXED) {
+        if (b->o.inner_rtol <= 0) b->o.inner_rtol = 1e-3;
+        if (b->o.max_refine <= 0) b->o.max_refine = 60;
+        if (b->o.inner_maxiter <= 0) b->o.inner_maxiter = 400;
+    }
+    if (b->o.lanes <= 0) b->o.lanes = 1;
+    b->nsys = nsys;
+    std::vector<BatchSys> sys(nsys);
+    long long ro = 0, po = 0, zo = 0;
+    for (int s = 0; s < nsys; ++s) {
+        if (n[s] <= 0 || nnz[s] < n[s]) {
+            free_batch(b);
+            set_error("kcfd_batch_create: system %d has n=%d nnz=%d", s, n[s], nnz[s]);
+            return KCFD_BAD_INPUT;
+        }
+        const int32_t* ip = indptr_host + po;
+        if (ip[0] != 0 || ip[n[s]] != nnz[s]) {
+            free_batch(b);
+            set_error("kcfd_batch_create: system %d row pointers do not span its entries", s);
+            return KCFD_BAD_INPUT;
+        }
+        for (int i = 0; i < n[s]; ++i)
+            if (ip[i + 1] < ip[i]) {
+                free_batch(b);
+                set_error("kcfd_batch_create: system %d row pointers not monotone", s);
+                return KCFD_BAD_INPUT;
+            }
+        for (int k = 0; k < nnz[s]; ++k)
+            if (indices_host[zo + k] < 0 || indices_host[zo + k] >= n[s]) {
+                free_batch(b);
+                set_error("kcfd_batch_create: system %d column index out of range", s);
+                return KCFD_BAD_INPUT;
+            }
+        sys[s] = {n[s], nnz[s], ro, po, zo};
+        ro += n[s];
+        po += n[s] + 1;
+        zo += nnz[s];
+    }
+    b->n_total = ro;
+    b->nnz_total = zo;
+    // largest first (longest-processing-time order for the dynamic queue)
+    std::vector<int> order(nsys);
+    for (int s = 0; s < nsys; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nnz[x] > nnz[y]; });
+    const bool mixed = b->o.mode == KCFD_MODE_MIXED;
+    const size_t vsz = mixed ? 4 : 8;
+    int dev = 0, sms = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel_ptr(mixed, b->o.precond), 256, 0);
+    b->grid = std::max(1, std::min(nsys, std::max(1, per_sm) * sms));
+    bool ok = cudaMalloc(&b->sys, nsys * sizeof(BatchSys)) == cudaSuccess &&
+              cudaMemcpy(b->sys, sys.data(), nsys * sizeof(BatchSys), cudaMemcpyHostToDevice) == cudaSuccess &&
+              upload(&b->order, order) && cudaMalloc(&b->queue, sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&b->indptr, po * 4) == cudaSuccess &&
+              cudaMemcpy(b->indptr, indptr_host, po * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMalloc(&b->indices, zo * 4) == cudaSuccess &&
+              cudaMemcpy(b->indices, indices_host, zo * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
+              cudaMalloc(&b->dinv, ro * vsz) == cudaSuccess && cudaMalloc(&b->lev, 2 * nsys * sizeof(int)) == cudaSuccess &&
+              cudaMalloc(&b->work, 9 * ro * vsz) == cudaSuccess;
+    if (ok && mixed) ok = cudaMalloc(&b->vals32, zo * 4) == cudaSuccess && cudaMalloc(&b->r64, ro * 8) == cudaSuccess;
+    if (!ok) {
+        free_batch(b);
+        set_error("kcfd_batch_create: device allocation failed (%lld rows, %lld entries)", ro, zo);
+        return KCFD_CUDA_ERROR;
+    }
+    *out = b;
+    return KCFD_OK;
+}
+
+void kcfd_batch_destroy(kcfd_batch* b) { free_batch(b); }
+
+int kcfd_batch_info(const kcfd_batch* b, int64_t* info) {
+    KCFD_REQUIRE(b && info, "kcfd_batch_info: NULL argument");
+    info[0] = b->nsys;
+    info[1] = b->n_total;
+    info[2] = b->nnz_total;
+    info[3] = b->grid;
+    return KCFD_OK;
+}
+
+int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, double* x, int32_t* iters,
+                     double* relres, int32_t* status, void* stream) {
+    KCFD_REQUIRE(b && vals64 && rhs && x && iters && relres && status, "kcfd_batch_solve: NULL argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    BatchArgs B;
+    std::memset(&B, 0, sizeof(B));
+    B.nsys = b->nsys;
+    B.lanes = b->o.lanes;
+    B.mixed = b->o.mode == KCFD_MODE_MIXED;
+    B.precond = b->o.precond;
+    B.stop = b->o.stop;
+    B.maxiter = b->o.maxiter;
+    B.max_refine = b->o.max_refine;
+    B.inner_maxiter = b->o.inner_maxiter;
+    B.rtol = b->o.rtol;
+    B.atol = b->o.atol;
+    B.inner_rtol = b->o.inner_rtol;
+    B.sys = b->sys;
+    B.order = b->order;
+    B.queue = b->queue;
+    B.indptr = b->indptr;
+    B.indices = b->indices;
+    B.vals64 = vals64;
+    B.vals32 = b->vals32;
+    B.dinv = b->dinv;
+    B.lev = b->lev;
+    B.work = b->work;
+    B.r64 = b->r64;
+    B.x = x;
+    B.b = rhs;
+    B.iters = iters;
+    B.relres = relres;
+    B.status = status;
+    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, sizeof(int), st));
+    void* args[] = {&B};
+    KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond), dim3(b->grid), dim3(256), args, 0, st));
+    KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }
 

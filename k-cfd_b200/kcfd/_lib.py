@@ -68,6 +68,15 @@ SIGNATURES = {
     "kcfd_simple_correct": (i32, [vp, f64, vp, vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_residual_norms": (i32, [C.POINTER(Csr), vp, vp, i32, vp, vp, vp]),
     "kcfd_simple_residual": (i32, [i32, vp, vp, vp, vp, vp, i32, vp]),
+    "kcfd_op_diffusion": (i32, [vp, vp, vp, vp, vp]),
+    "kcfd_op_convection_upwind": (i32, [vp, vp, vp, vp, vp]),
+    "kcfd_op_boundary": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_op_cells": (i32, [vp, i32, f64, f64, vp, vp, vp, vp, vp, vp]),
+    "kcfd_muscl_correction": (i32, [vp, i32, vp, vp, vp, vp, vp]),
+    "kcfd_batch_create": (i32, [i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "kcfd_batch_destroy": (None, [vp]),
+    "kcfd_batch_info": (i32, [vp, P_i64]),
+    "kcfd_batch_solve": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_noalloc_max_rows": (i32, []),
     "kcfd_bicgstab_noalloc": (i32, [C.POINTER(Csr), vp, vp, i32, i32, f64, f64, i32, vp, vp, vp, vp]),
 }

@@ -1,0 +1,129 @@
+"""Batched solves: many independent systems of uneven size in one persistent launch.
+
+BatchSolver packs the systems' CSR (local row pointers and column indices per system,
+concatenated) once and then solves all of them in one launch of the batched kernel
+(libkcfd kcfd_batch_*): each CTA takes the next system from a largest-first queue and
+solves it alone, so a system's result is the same whatever runs beside it.
+
+The pressure-correction batch of the benchmark configs is built here too:
+p_prime_batch() makes Delaunay triangle meshes with cell counts log-uniform in
+[n_min, n_max], per-cell diffusivity log-uniform in [0.1, 10], one Dirichlet
+segment and a N(0, 1) right-hand side, assembled on the device with the generic
+operators (kcfd.assembly).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import _lib
+
+
+class BatchOpts(C.Structure):
+    _fields_ = [("precond", C.c_int32), ("stop", C.c_int32), ("mode", C.c_int32), ("maxiter", C.c_int32),
+                ("lanes", C.c_int32), ("max_refine", C.c_int32), ("inner_maxiter", C.c_int32), ("pad", C.c_int32),
+                ("rtol", C.c_double), ("atol", C.c_double), ("inner_rtol", C.c_double)]
+
+
+class BatchSolver:
+    """patterns: list of (indptr, indices) host arrays (one per system)."""
+
+    def __init__(self, patterns, mode="mixed", precond="jacobi", rtol=1e-8, atol=0.0, maxiter=20000, lanes=1,
+                 inner_rtol=1e-3, inner_maxiter=400, max_refine=60, stop=_lib.STOP_SCIPY, device="cuda"):
+        torch = _lib.require_cuda()
+        self.nsys = len(patterns)
+        self.n = np.array([len(ip) - 1 for ip, _ in patterns], dtype=np.int32)
+        self.nnz = np.array([len(ix) for _, ix in patterns], dtype=np.int32)
+        ip = np.ascontiguousarray(np.concatenate([np.asarray(p, dtype=np.int32) for p, _ in patterns]))
+        ix = np.ascontiguousarray(np.concatenate([np.asarray(i, dtype=np.int32) for _, i in patterns]))
+        self.row_off = np.concatenate([[0], np.cumsum(self.n.astype(np.int64))])
+        self.nnz_off = np.concatenate([[0], np.cumsum(self.nnz.astype(np.int64))])
+        o = BatchOpts()
+        o.precond = _lib.PREC[precond]
+        o.stop = stop
+        o.mode = _lib.MODE_MIXED if mode == "mixed" else _lib.MODE_FP64
+        o.maxiter, o.lanes, o.max_refine, o.inner_maxiter = int(maxiter), int(lanes), int(max_refine), int(inner_maxiter)
+        o.rtol, o.atol, o.inner_rtol = float(rtol), float(atol), float(inner_rtol)
+        h = C.c_void_p()
+        _lib.check(_lib.lib().kcfd_batch_create(self.nsys, self.n.ctypes.data, self.nnz.ctypes.data, ip.ctypes.data,
+                                                ix.ctypes.data, C.byref(o), C.byref(h)), "kcfd_batch_create")
+        self._h = h
+        info = np.zeros(4, dtype=np.int64)
+        _lib.check(_lib.lib().kcfd_batch_info(h, info.ctypes.data_as(_lib.P_i64)), "kcfd_batch_info")
+        self.n_total, self.nnz_total, self.ctas = int(info[1]), int(info[2]), int(info[3])
+        dev = device
+        self.iters = torch.zeros(self.nsys, dtype=torch.int32, device=dev)
+        self.relres = torch.zeros(self.nsys, dtype=torch.float64, device=dev)
+        self.status = torch.zeros(self.nsys, dtype=torch.int32, device=dev)
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().kcfd_batch_destroy(h)
+            except Exception:
+                pass
+            self._h = None
+
+    def solve(self, vals64, rhs, x, stream=None):
+        """Packed device arrays; x holds x0 on entry. One kernel launch."""
+        _lib.check(_lib.lib().kcfd_batch_solve(self._h, _lib.ptr(vals64), _lib.ptr(rhs), _lib.ptr(x),
+                                               _lib.ptr(self.iters), _lib.ptr(self.relres), _lib.ptr(self.status),
+                                               _lib.stream_handle(stream)), "kcfd_batch_solve")
+        return self.iters, self.relres, self.status
+
+    def pack(self, arrays, what="rows"):
+        """List of per-system host arrays -> one packed device tensor."""
+        torch = _lib.require_cuda()
+        return torch.from_numpy(np.ascontiguousarray(np.concatenate([np.asarray(a, dtype=np.float64)
+                                                                     for a in arrays]))).cuda()
+
+    def unpack(self, t):
+        v = t.detach().cpu().numpy()
+        return [v[self.row_off[s]:self.row_off[s + 1]] for s in range(self.nsys)]
+
+
+def lpt_shards(weights, nranks):
+    """Greedy longest-processing-time assignment of systems to ranks (largest first,
+    each to the currently lightest rank). Returns a list of index lists."""
+    order = np.argsort(-np.asarray(weights), kind="stable")
+    load = np.zeros(nranks)
+    out = [[] for _ in range(nranks)]
+    for i in order:
+        r = int(np.argmin(load))
+        out[r].append(int(i))
+        load[r] += weights[i]
+    return [sorted(o) for o in out]
+
+
+def p_prime_batch(count, n_min=2000, n_max=200000, seed=0, device="cuda"):
+    """Pressure-correction systems on Delaunay triangle meshes, assembled on the device.
+
+    Returns (patterns, vals_list [device], rhs_list [host], sizes). Cell counts are
+    log-uniform in [n_min, n_max]; each mesh triangulates ~n/2 uniform points plus the
+    unit square's corners; the 'dirichlet' hull segment (x = 0) has p' = 0, the other
+    hull edges are zero-gradient.
+    """
+    torch = _lib.require_cuda()
+    from .assembly import DeviceSystem, boundary_arrays
+    from .device_mesh import DeviceMesh
+    from .mesh import build_mesh
+    from .meshgen import delaunay_tri_arrays
+    rng = np.random.default_rng(seed)
+    sizes = np.round(np.exp(rng.uniform(np.log(n_min), np.log(n_max), count))).astype(np.int64)
+    patterns, vals, rhs = [], [], []
+    for k in range(count):
+        pts, cells, bd = delaunay_tri_arrays(max(int(sizes[k]) // 2, 4), rng)
+        m = build_mesh(pts, cells, bd)
+        dm = DeviceMesh(m, device)
+        gamma = torch.from_numpy(np.exp(rng.uniform(np.log(0.1), np.log(10.0), m.n_cells))).to(device)
+        s = DeviceSystem(dm)
+        s.diffusion_operator(gamma)
+        mf = torch.zeros(m.n_faces, dtype=torch.float64, device=device)
+        bt, bv, bg = boundary_arrays(dm, {"dirichlet": {"type": "dirichlet"}, "wall": {"type": "zero_gradient"}}, {})
+        s.apply_boundary_conditions(bt, bv, bg, gamma, mf)
+        patterns.append((m.indptr, m.indices))
+        vals.append(s.vals)
+        rhs.append(rng.normal(size=m.n_cells))
+    return patterns, vals, rhs, sizes

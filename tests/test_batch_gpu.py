@@ -1,0 +1,79 @@
+"""Batched persistent solves (one launch, many uneven systems) vs direct solves and
+vs each system solved alone.
+
+Per system: the true FP64 relative residual meets rtol (1e-8 scaled by 1.5 for the
+recursive-vs-true gap) and the solution is within 1e-6 relative L2 of spsolve. A
+system's result is bitwise the same alone and in the batch (its CTA computes it with
+the same fixed-order reductions whatever else runs), and the FP64 batch equals the
+single-CTA solver handle bitwise.
+"""
+import numpy as np
+import pytest
+import scipy.sparse.linalg as spla
+from scipy import sparse
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def batch():
+    from kcfd.batch import p_prime_batch
+    return p_prime_batch(12, n_min=300, n_max=6000, seed=3)
+
+
+def _csr(pat, v):
+    ip, ix = pat
+    return sparse.csr_matrix((v.cpu().numpy(), ix, ip), shape=(len(ip) - 1, len(ip) - 1))
+
+
+@pytest.mark.parametrize("mode", ["mixed", "fp64"])
+def test_batch_solutions(batch, mode):
+    import torch
+    from kcfd.batch import BatchSolver
+    pats, vals, rhs, sizes = batch
+    bs = BatchSolver(pats, mode=mode, precond="jacobi", rtol=1e-8)
+    v = torch.cat(vals)
+    b = bs.pack(rhs)
+    x = torch.zeros_like(b)
+    it, rr, st = bs.solve(v, b, x)
+    assert list(st.cpu().numpy()) == [0] * bs.nsys
+    xs = bs.unpack(x)
+    for k in range(bs.nsys):
+        A = _csr(pats[k], vals[k])
+        assert np.linalg.norm(rhs[k] - A @ xs[k]) / np.linalg.norm(rhs[k]) < 1.5e-8
+        xd = spla.spsolve(A.tocsc(), rhs[k])
+        assert np.linalg.norm(xs[k] - xd) / np.linalg.norm(xd) < 1e-6
+
+
+def test_same_result_alone_and_in_the_batch(batch):
+    import torch
+    from kcfd.batch import BatchSolver
+    pats, vals, rhs, sizes = batch
+    full = BatchSolver(pats, mode="mixed")
+    x = torch.zeros(full.n_total, dtype=torch.float64, device="cuda")
+    full.solve(torch.cat(vals), full.pack(rhs), x)
+    xs = full.unpack(x)
+    for k in (0, 5, 11):
+        one = BatchSolver([pats[k]], mode="mixed")
+        x1 = torch.zeros(one.n_total, dtype=torch.float64, device="cuda")
+        one.solve(vals[k], one.pack([rhs[k]]), x1)
+        np.testing.assert_array_equal(x1.cpu().numpy(), xs[k])
+
+
+def test_fp64_batch_equals_single_cta_handle(batch):
+    import torch
+    from kcfd.batch import BatchSolver
+    from kcfd.solver import DeviceCSR, Solver
+    pats, vals, rhs, sizes = batch
+    bs = BatchSolver(pats, mode="fp64")
+    x = torch.zeros(bs.n_total, dtype=torch.float64, device="cuda")
+    bs.solve(torch.cat(vals), bs.pack(rhs), x)
+    xs = bs.unpack(x)
+    for k in (1, 7):
+        ip, ix = pats[k]
+        d = DeviceCSR(torch.from_numpy(ip).cuda(), torch.from_numpy(ix).cuda(), vals[k])
+        s = Solver(d, precond="jacobi", rtol=1e-8, maxiter=20000, team=1, block=256, lanes=1)
+        s.setup(d)
+        xk = torch.zeros(d.n, dtype=torch.float64, device="cuda")
+        s.solve(d, torch.from_numpy(rhs[k]).cuda(), xk)
+        np.testing.assert_array_equal(xk.cpu().numpy(), xs[k])

@@ -319,6 +319,13 @@ int kcfd_residual_norms(const kcfd_csr_t* A, const double* x, const double* b, i
 int kcfd_simple_residual(int32_t ndim, const double* mom_norms2, const double* p_norms2, double* state,
                          double* hist, int32_t* it, int32_t max_hist, void* stream);
 
+/* out[c] = sum_i x[i*k + c]^2 for c < k (k <= 6), fixed-order sums; scratch as above. */
+int kcfd_vec_norms2(int32_t n, int32_t k, const double* x, double* out2, double* scratch, void* stream);
+
+/* Continuity residual history of served runs: chist[*it] = ||b_p'|| (from its
+ * squared norm); call before kcfd_simple_residual advances *it.                    */
+int kcfd_record_norm(const double* norm2, double* chist, const int32_t* it, int32_t max_hist, void* stream);
+
 /* Barrier error flag of the handle's last launch (KCFD_TIMEOUT when a bounded team
  * barrier wait expired, else 0). Synchronises the stream.                         */
 int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream);

@@ -421,6 +421,29 @@ __global__ void k_simple_residual(int ndim, const double* __restrict__ mom, cons
     *itp = it + 1;
 }
 
+template <int K>
+__global__ void k_norms2(int n, const double* __restrict__ x, double* __restrict__ scratch) {
+    double v[K];
+#pragma unroll
+    for (int c = 0; c < K; ++c) v[c] = 0.0;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+#pragma unroll
+        for (int c = 0; c < K; ++c) {
+            const double t = x[(size_t)i * K + c];
+            v[c] += t * t;
+        }
+    }
+    store_partials<K>(v, scratch);
+}
+
+__global__ void k_record_norm(const double* __restrict__ n2, double* __restrict__ h, const int* __restrict__ it,
+                              int max_hist) {
+    if (threadIdx.x == 0 && blockIdx.x == 0) {
+        const int i = *it;
+        if (i >= 0 && i < max_hist) h[i] = sqrt(n2[0]);
+    }
+}
+
 }  // namespace kcfd
 
 using namespace kcfd;
@@ -572,6 +595,30 @@ int kcfd_simple_residual(int32_t ndim, const double* mom_norms2, const double* p
                          int32_t* it, int32_t max_hist, void* stream) {
     KCFD_REQUIRE(mom_norms2 && p_norms2 && state && hist && it && max_hist >= 0, "kcfd_simple_residual: bad argument");
     k_simple_residual<<<1, 32, 0, (cudaStream_t)stream>>>(ndim, mom_norms2, p_norms2, state, hist, it, max_hist);
+    KCFD_CUDA(cudaGetLastError());
+    return KCFD_OK;
+}
+
+int kcfd_vec_norms2(int32_t n, int32_t k, const double* x, double* out2, double* scratch, void* stream) {
+    KCFD_REQUIRE(n >= 0 && k >= 1 && k <= 6 && x && out2 && scratch, "kcfd_vec_norms2: bad argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const int nb = std::min(kRedBlocks, blocks_for(std::max(n, 1)));
+    switch (k) {
+        case 1: k_norms2<1><<<nb, kThreads, 0, st>>>(n, x, scratch); break;
+        case 2: k_norms2<2><<<nb, kThreads, 0, st>>>(n, x, scratch); break;
+        case 3: k_norms2<3><<<nb, kThreads, 0, st>>>(n, x, scratch); break;
+        case 4: k_norms2<4><<<nb, kThreads, 0, st>>>(n, x, scratch); break;
+        case 5: k_norms2<5><<<nb, kThreads, 0, st>>>(n, x, scratch); break;
+        default: k_norms2<6><<<nb, kThreads, 0, st>>>(n, x, scratch); break;
+    }
+    k_finalize<<<1, 32 * 8, 0, st>>>(k, nb, scratch, out2);
+    KCFD_CUDA(cudaGetLastError());
+    return KCFD_OK;
+}
+
+int kcfd_record_norm(const double* norm2, double* chist, const int32_t* it, int32_t max_hist, void* stream) {
+    KCFD_REQUIRE(norm2 && chist && it && max_hist >= 0, "kcfd_record_norm: bad argument");
+    k_record_norm<<<1, 32, 0, (cudaStream_t)stream>>>(norm2, chist, it, max_hist);
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }

@@ -95,10 +95,12 @@ struct Vecs {
     }
 };
 
-// This CTA's slice [s0, s1) of level l.
+// This CTA's slice [s0, s1) of level l. The level table is written before the
+// launch and never inside it; a single level is the whole row range.
 template <class Team>
 __device__ __forceinline__ void level_slice(const Team& tm, const SolveArgs& a, int l, int& s0, int& s1) {
-    const int b0 = __ldg(a.lev_ptr + l), m = __ldg(a.lev_ptr + l + 1) - b0;
+    const int b0 = (a.nlev == 1) ? 0 : a.lev_ptr[l];
+    const int m = ((a.nlev == 1) ? a.n : a.lev_ptr[l + 1]) - b0;
     const int per = (m + tm.size - 1) / tm.size;
     s0 = b0 + min(m, tm.rank * per);
     s1 = b0 + min(m, tm.rank * per + per);
@@ -121,9 +123,11 @@ __device__ __forceinline__ void for_my_rows(const Team& tm, const SolveArgs& a, 
 // FP32 it keeps near-zero row sums (Neumann-type pressure operators) exact instead of
 // leaving them to the rounding of a large diagonal.
 template <typename VM, typename VX, int NRHS, bool DIFF = false, class Epi>
+// Only the matrix (ip, ix, val) is read-only for the whole launch; x is rewritten
+// between phases, so it is read through the coherent path.
 __device__ __forceinline__ void spmv_range(const int* __restrict__ ip, const int* __restrict__ ix,
-                                           const VM* __restrict__ val, const VX* __restrict__ x, int r0,
-                                           int r1, int L, Epi epi) {
+                                           const VM* __restrict__ val, const VX* x, int r0, int r1, int L,
+                                           Epi epi) {
     const int lane = threadIdx.x & 31;
     const int sub = lane / L, sl = lane % L;
     const int rows_per_warp = 32 / L;
@@ -170,7 +174,7 @@ __device__ __forceinline__ void spmv_range(const int* __restrict__ ip, const int
 // last level of the backward sweep only touch rows this CTA owns, so the sweeps need
 // 2 (nlev - 1) barriers; the caller syncs before anything gathers z.
 template <typename V, int NRHS, class Team>
-__device__ __forceinline__ bool ilu_apply(Team& tm, const SolveArgs& a, const V* __restrict__ q, V* __restrict__ z) {
+__device__ __forceinline__ bool ilu_apply(Team& tm, const SolveArgs& a, const V* q, V* z) {
     const V* lu = (const V*)a.lu;
     const V* ldi = (const V*)a.ludinv;
     for (int l = 0; l < a.nlev; ++l) {
@@ -236,8 +240,8 @@ __device__ __forceinline__ bool finite(double v) { return isfinite(v); }
 // A non-finite scalar ends a right-hand side with KCFD_BREAKDOWN (nonfinite = 1).
 // Returns false if a team barrier failed.
 template <typename V, typename VM, int NRHS, int PREC, class Team>
-__device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict__ vals, V* __restrict__ xv,
-                              const V* __restrict__ bv, bool x_zero, const Vecs<V>& w, int stop, double rtol,
+__device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict__ vals, V* xv,
+                              const V* bv, bool x_zero, const Vecs<V>& w, int stop, double rtol,
                               double atol, int maxiter, KState<NRHS>& st, double* smem) {
     const int* __restrict__ ip = a.indptr;
     const int* __restrict__ ix = a.indices;
@@ -881,6 +885,17 @@ __device__ void batch_prep(const BatchArgs& B, const BatchSys& S, int sid, V* di
     }
 }
 
+// Per-system set-up in its own launch (the solve launch reads these arrays through
+// the read-only path): Jacobi inverse diagonal, FP32 difference-form operator.
+template <int MIXED>
+__global__ void batch_prep_kernel(BatchArgs B) {
+    using V = typename std::conditional<MIXED, float, double>::type;
+    for (int sid = blockIdx.x; sid < B.nsys; sid += gridDim.x) {
+        const BatchSys S = B.sys[sid];
+        batch_prep<V>(B, S, sid, (V*)B.dinv + S.row_off, B.vals32 ? B.vals32 + S.nnz_off : nullptr, MIXED);
+    }
+}
+
 template <int MIXED, int PREC>
 __global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs B) {
     __shared__ double smem[32 * kMaxK];
@@ -920,8 +935,6 @@ __global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs B) {
         a.iters_out = B.iters + sid;
         a.relres_out = B.relres + sid;
         a.status_out = B.status + sid;
-        batch_prep<V>(B, S, sid, (V*)a.dinv, (float*)a.vals32, MIXED);
-        __syncthreads();
         if (MIXED) solve_mixed<1, PREC>(tm, a, smem);
         else solve_fp64<1, PREC>(tm, a, smem);
         __syncthreads();
@@ -1562,6 +1575,9 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
     B.status = status;
     KCFD_CUDA(cudaMemsetAsync(b->queue, 0, sizeof(int), st));
     void* args[] = {&B};
+    const int pgrid = std::max(1, std::min(b->nsys, 4 * b->grid));
+    KCFD_CUDA(cudaLaunchKernel(B.mixed ? (void*)batch_prep_kernel<1> : (void*)batch_prep_kernel<0>, dim3(pgrid),
+                               dim3(256), args, 0, st));
     KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond), dim3(b->grid), dim3(256), args, 0, st));
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;

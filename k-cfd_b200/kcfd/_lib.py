@@ -77,6 +77,8 @@ SIGNATURES = {
     "kcfd_batch_destroy": (None, [vp]),
     "kcfd_batch_info": (i32, [vp, P_i64]),
     "kcfd_batch_solve": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_vec_norms2": (i32, [i32, i32, vp, vp, vp, vp]),
+    "kcfd_record_norm": (i32, [vp, vp, vp, i32, vp]),
     "kcfd_noalloc_max_rows": (i32, []),
     "kcfd_bicgstab_noalloc": (i32, [C.POINTER(Csr), vp, vp, i32, i32, f64, f64, i32, vp, vp, vp, vp]),
 }

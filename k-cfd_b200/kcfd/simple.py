@@ -87,6 +87,8 @@ class SIMPLESolver:
         self.it_dev = torch.zeros(1, dtype=torch.int32, device=device)
         self.hist_cap = 1 << 16
         self.hist = torch.zeros(self.hist_cap, **f64)
+        self.chist = torch.zeros(self.hist_cap, **f64)   # ||b_p'|| per outer iteration
+        self.bp_norm2 = torch.zeros(1, **f64)
         mixed = precision == "mixed"
         self.mode = _lib.MODE_MIXED if mixed else _lib.MODE_FP64
         ip, ix = self.dm.t["indptr"], self.dm.t["indices"]
@@ -143,6 +145,9 @@ class SIMPLESolver:
         chk(L.kcfd_mass_flux(dm, bc, P(self.U_t), self.rho, P(self.mf_t), st), "mass_flux")
         chk(L.kcfd_pressure_assemble(dm, bc, self.rho, P(self.dP_t), P(self.mf_t), P(self.aP_t),
                                      P(self.A_p.vals64), P(self.A_p.vals32), P(self.b_p), st), "pressure_assemble")
+        chk(L.kcfd_vec_norms2(self.dm.n_cells, 1, P(self.b_p), P(self.bp_norm2), P(self.scratch), st),
+            "vec_norms2")
+        chk(L.kcfd_record_norm(P(self.bp_norm2), P(self.chist), P(self.it_dev), self.hist_cap, st), "record_norm")
         self.s_p.setup(self.A_p)
         self.pp_t.zero_()
         self.s_p.solve(self.A_p, self.b_p, self.pp_t)
@@ -179,6 +184,12 @@ class SIMPLESolver:
         self.state.zero_()
         self.it_dev.zero_()
         self.hist.zero_()
+        self.chist.zero_()
+
+    def continuity_residual(self, k):
+        """||b_p'|| of outer iteration k normalised by the first one (host read)."""
+        c = self.chist[: k + 1].cpu().numpy()
+        return float(c[k] / c[0]) if c[0] > 0 else 0.0
 
     def solve_steady(self):
         """models/single_phase.py:70-101 semantics; the residual history is kept on the

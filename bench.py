@@ -4,9 +4,9 @@ Workload (the headline config that fits one GPU): 128^3 hexahedra (2,097,152 cel
 the unit cube, interior nodes jittered by U(-0.2, 0.2) x spacing (seed 0), Re = 400
 (rho = 1, mu = 0.0025), MUSCL van Leer deferred correction, over-relaxed
 non-orthogonal correction, Green-Gauss gradients, BiCGSTAB + Jacobi for u, v, w and
-BiCGSTAB + ILU(0) for p', each to a 1e-8 relative residual; alpha_u = 0.7,
-alpha_p = 0.3; mixed precision (FP32 inner iterations, FP64 residual / refinement /
-dots); one outer iteration captured as a CUDA graph.
+BiCGSTAB + ILU(0) (red-black levels) for p', each to a 1e-8 relative residual;
+alpha_u = 0.7, alpha_p = 0.3. FP64 throughout; both solves run on the graph engine
+(phase kernels in one CUDA graph per solve with a device-side WHILE loop).
 
 A "step" is one SIMPLE outer iteration. Inputs (mesh, matrices, fields: several GB)
 are far larger than the 126 MB L2, so no flush is needed between steps.
@@ -133,8 +133,19 @@ def solver_bytes(n, nnz, iters, precond, w, nrhs=1):
     return iters * (2 * spmv + 21 * n * w * nrhs)
 
 
-def launches_per_step(s):
-    """Kernels of libkcfd launched by one outer iteration (excluding memsets)."""
+def solve_launches(solver, iters, precond, nlev):
+    """Kernels one solve launches: the persistent kernels launch once; the graph
+    engine launches init, final and the two copies plus, per loop trip, the phase
+    kernels (5, and 2 (nlev - 1) ILU sweeps for each of phat and shat)."""
+    if not solver.graph_engine:
+        return 1
+    body = 5 + (4 * (nlev - 1) if precond == "ilu0" else 0)
+    return 4 + body * int(iters)
+
+
+def launches_per_step(s, its_m, its_p):
+    """Kernels of libkcfd launched by one outer iteration (excluding memsets), with
+    the Krylov counts of that iteration."""
     nci, ncb = s.dm.desc.n_colors_int, s.dm.desc.n_colors_bnd
     per_colour_pass = nci + ncb
     gg = per_colour_pass + 1
@@ -142,18 +153,23 @@ def launches_per_step(s):
     pp = per_colour_pass + 1
     n = 2                       # mass flux x2
     n += gg if s.gU_t is not None else 0
-    n += mom + 1 + 1 + 2       # momentum, jacobi set-up, solve, residual norms (2)
-    n += pp + 1 + 1            # p' assembly, ILU factor, solve
-    n += gg + 2 + 1            # GG p', correction (2), residual bookkeeping
+    n += mom + 1 + 2            # momentum, jacobi set-up, residual norms (2)
+    n += pp + 2 + 2             # p' assembly, ILU permute + factor, norm + record
+    n += gg + 2 + 1             # GG p', correction (2), residual bookkeeping
+    nlev = s.s_p.info()["levels"]
+    n += solve_launches(s.s_m, its_m, "jacobi", 1)
+    n += solve_launches(s.s_p, its_p, "ilu0", nlev)
     return n
 
 
 def p_solve_roofline(s, peak, reps=3):
-    """Time the p' solve kernel alone with CUDA events on its stream; algorithmic
-    bytes from its iteration count."""
+    """The p' solve (the dominant work: >90% of the device time of an outer
+    iteration) timed alone with CUDA events on its stream; algorithmic bytes from
+    its Krylov count. Also the FP64 SpMV kernel alone on the same matrix."""
     import torch
     n, nnz = s.mesh.n_cells, s.mesh.nnz
     mixed = s.mode == 1
+    w = 4 if mixed else 8
     times, byts = [], []
     for _ in range(reps):
         s.s_p.setup(s.A_p)
@@ -165,7 +181,6 @@ def p_solve_roofline(s, peak, reps=3):
         e1.record()
         torch.cuda.synchronize()
         it = int(s.s_p.iters[0])
-        w = 4 if mixed else 8
         b = solver_bytes(n, nnz, it, "ilu0", w)
         if mixed:  # outer FP64 residuals (about one per 4 inner iterations) + updates
             nref = max(2, it // 40)
@@ -174,10 +189,47 @@ def p_solve_roofline(s, peak, reps=3):
         byts.append(b)
     t = float(np.mean(times))
     ach = float(np.mean(byts)) / t / 1e9
-    return {"bound": "hbm", "kernel": "solve_grid_kernel<MIXED=1,NRHS=1,ILU0> (p' BiCGSTAB)",
+    info = s.s_p.info()
+    kern = ("graph engine: g_p, g_fwd, g_bwd, g_spmv_v, g_s, g_spmv_t, g_xr per Krylov iteration "
+            "(p' BiCGSTAB + ILU(0), FP64)") if info["team"] == 3 else \
+        f"solve_grid_kernel (p' BiCGSTAB + ILU(0), {'mixed' if mixed else 'FP64'})"
+    # SpMV alone: nnz (8 + 4) + 4 (n + 1) + 8 n (x) + 8 n (y)
+    x = torch.randn(n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    for _ in range(3):
+        s.A_p.spmv(x, y)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    K = 50
+    e0.record()
+    for _ in range(K):
+        s.A_p.spmv(x, y)
+    e1.record()
+    torch.cuda.synchronize()
+    ts = e0.elapsed_time(e1) / 1e3 / K
+    sb = nnz * 12 + 4 * (n + 1) + 16 * n
+    spmv = {"kernel": "spmv_kernel<double> (kcfd_spmv_f64)", "bytes": int(sb), "launch_us": round(ts * 1e6, 2),
+            "achieved": round(sb / ts / 1e9, 1), "frac": round(sb / ts / 1e9 / peak[0], 3)}
+    return {"bound": "hbm", "kernel": kern, "unit_of_work": "one p' solve (Krylov iterations x bytes/iteration)",
             "achieved": round(ach, 1), "peak": peak[0], "unit": "GB/s", "frac": round(ach / peak[0], 3),
             "peak_source": peak[1], "traffic": None, "launch_ms": round(t * 1e3, 3),
-            "krylov_iters": int(s.s_p.iters[0])}
+            "krylov_iters": int(s.s_p.iters[0]), "bytes_per_krylov_iter": int(solver_bytes(n, nnz, 1, "ilu0", w)),
+            "spmv": spmv}
+
+
+def timed_iterations(s, steps):
+    """Run `steps` outer iterations between CUDA events; keeps each step's Krylov
+    counts (device copies, read after the timed region)."""
+    import torch
+    its = []
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(steps):
+        s.iterate(1)
+        its.append((s.s_m.iters.max().clone(), s.s_p.iters[0].clone()))
+    e1.record()
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / 1e3, [(int(a), int(b)) for a, b in its]
 
 
 def run_ours(args):
@@ -192,60 +244,41 @@ def run_ours(args):
     dev = torch.cuda.current_device()
     N = args.size
     t_setup = time.time()
-    s = make_solver(N, precision="mixed", graph=True)
+    s = make_solver(N, precision="fp64", graph=True)
     setup_s = time.time() - t_setup
+    n_faces, nnz = int(s.mesh.n_faces), int(s.mesh.nnz)
     s.reset_history()
     s.iterate(args.warmup)
     torch.cuda.synchronize()
+    # the state the timed region starts from (U, p: everything else is rebuilt from
+    # them each outer iteration); the e2e leg replays the same steps from it
+    D = 3
+    Uh = torch.empty(s.mesh.n_cells, D, dtype=torch.float64).pin_memory()
+    ph = torch.empty(s.mesh.n_cells, dtype=torch.float64).pin_memory()
+    Uh.copy_(s.U_t.cpu())
+    ph.copy_(s.p_t.cpu())
     if world > 1:
         dist.barrier()
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as cs:
-        e0.record()
-        s.iterate(args.steps)
-        e1.record()
-        torch.cuda.synchronize()
+        t, its = timed_iterations(s, args.steps)
     if world > 1:
         dist.barrier()
-    t = e0.elapsed_time(e1) / 1e3
-    if world > 1:
         tt = torch.tensor([t], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         t = float(tt.item())
     clocks = cs.summary()
     value = world * args.steps / t
     stats = s.solver_stats()
+    launches = sum(launches_per_step(s, a, b) for a, b in its)
     res_hist = s.hist[: args.warmup + args.steps].cpu().numpy()
-    # plain FP64 form on the same mesh (no graph), for the mixed/batched vs plain ratio
-    plain = None
-    if args.plain and rank == 0:
-        del s
-        torch.cuda.empty_cache()
-        sp = make_solver(N, precision="fp64", graph=False)
-        sp.iterate(max(1, args.warmup))
-        torch.cuda.synchronize()
-        a0, a1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        k = max(2, min(args.steps, 5))
-        a0.record()
-        sp.iterate(k)
-        a1.record()
-        torch.cuda.synchronize()
-        plain = {"value": round(k / (a0.elapsed_time(a1) / 1e3), 3), "unit": UNIT, "steps": k,
-                 "desc": "same workload, plain FP64 (FP64 assembly/SpMV/Krylov), eager launches, no graph"}
-        del sp
-        torch.cuda.empty_cache()
-        s = make_solver(N, precision="mixed", graph=True)
-        s.iterate(max(1, args.warmup))
-    # e2e through the reference-facing API with host buffers: fields in from pinned
-    # host memory, one outer iteration, fields out, every step
-    D = 3
-    Uh = torch.empty(s.mesh.n_cells, D, dtype=torch.float64).pin_memory()
-    ph = torch.empty(s.mesh.n_cells, dtype=torch.float64).pin_memory()
-    Uh.copy_(s.U_t.cpu())
-    ph.copy_(s.p_t.cpu())
+    # e2e through the reference-facing API with host buffers: the same steps as the
+    # timed region (from the same state), each taking U, p from pinned host memory
+    # and returning them there
     torch.cuda.synchronize()
-    ke = max(2, min(args.steps, 5))
+    ke = args.steps
+    if world > 1:
+        dist.barrier()
     t0 = time.perf_counter()
     for _ in range(ke):
         s.U_t.copy_(Uh, non_blocking=True)
@@ -255,29 +288,48 @@ def run_ours(args):
         ph.copy_(s.p_t, non_blocking=True)
         torch.cuda.synchronize()
     te = time.perf_counter() - t0
+    if world > 1:
+        tt = torch.tensor([te], device="cuda", dtype=torch.float64)
+        dist.all_reduce(tt, op=dist.ReduceOp.MAX)
+        te = float(tt.item())
     e2e = {"value": round(world * ke / te, 3), "unit": UNIT, "h2d_bytes_per_step": int(s.mesh.n_cells * (D + 1) * 8),
-           "d2h_bytes_per_step": int(s.mesh.n_cells * (D + 1) * 8)}
+           "d2h_bytes_per_step": int(s.mesh.n_cells * (D + 1) * 8), "steps": ke}
     roof = p_solve_roofline(s, measured_peak()) if rank == 0 else None
+    # the mixed-precision form (FP32 inner Krylov on the persistent kernel, FP64
+    # refinement) on the same mesh, for comparison
+    alt = None
+    if args.plain and rank == 0:
+        del s
+        torch.cuda.empty_cache()
+        sm = make_solver(N, precision="mixed", graph=True)
+        sm.iterate(max(1, args.warmup))
+        torch.cuda.synchronize()
+        k = max(2, min(args.steps, 5))
+        tm, _ = timed_iterations(sm, k)
+        alt = {"value": round(k / tm, 3), "unit": UNIT, "steps": k,
+               "desc": "same workload, mixed precision (FP32 inner Krylov on the persistent grid kernel, "
+                       "FP64 residual/refinement), outer iteration captured as a CUDA graph"}
+        del sm
+        torch.cuda.empty_cache()
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_baseline(N, its_p=roof["krylov_iters"] if roof else None)
     if world > 1:
         dist.barrier()
-        s._graph = None
         dist.destroy_process_group()
     if rank == 0:
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "fp32-inner/fp64-refine", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"3D jittered lid-driven cavity {N}^3 hex ({N**3} cells), Re 400, MUSCL van Leer, "
-                                   "over-relaxed non-orthogonal, ILU(0) p' / Jacobi u,v,w, rtol 1e-8, mixed precision, "
-                                   "CUDA graph per outer iteration",
-                       "cells": N ** 3, "faces": int(s.mesh.n_faces), "nnz": int(s.mesh.nnz),
+                                   "over-relaxed non-orthogonal, ILU(0) p' / Jacobi u,v,w, rtol 1e-8, FP64, "
+                                   "graph-engine solves",
+                       "cells": N ** 3, "faces": n_faces, "nnz": nnz,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "working set >> 126 MB L2; no flush needed", "setup_s": round(setup_s, 2)},
-            "clocks": clocks, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "plain_fp64": plain,
-            "gpu_launches": launches_per_step(s) * args.steps,
+            "clocks": clocks, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "mixed_precision_variant": alt,
+            "gpu_launches": launches, "krylov_iters_per_step": its,
             "solver_stats_last_step": stats,
             "residual_first_last": [float(res_hist[0]), float(res_hist[-1])],
         }
@@ -361,7 +413,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--size", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--plain", type=int, default=1, help="also time the plain FP64 form (rank 0)")
+    ap.add_argument("--plain", type=int, default=1, help="also time the mixed-precision form (rank 0)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

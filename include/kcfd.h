@@ -133,7 +133,15 @@ typedef struct {
     int32_t mode;        /* KCFD_MODE_*                                        */
     int32_t nrhs;        /* 1, 2 or 3 (momentum components share one matrix)  */
     int32_t maxiter;     /* BiCGSTAB iterations (inner iterations in MIXED)   */
-    int32_t team;        /* 0 auto, 1 one CTA per system, 2 whole grid         */
+    int32_t team;        /* 0 auto, 1 one CTA per system, 2 whole grid (one
+                            persistent cooperative kernel), 3 graph engine
+                            (FP64 only: phase kernels in one CUDA graph per solve
+                            with a device-side loop; inside a stream capture the
+                            solve runs on the team-2 kernel). Auto: 1 for
+                            n*nrhs <= 40000, else 3 (FP64) or 2 (MIXED).
+                            KCFD_ENGINE_EAGER=1 in the environment at creation
+                            launches the engine's kernels from a host loop
+                            instead (for profilers; same results).             */
     int32_t lanes;       /* SpMV lanes per row: 0 auto, 1..32                  */
     int32_t block;       /* threads per CTA: 0 auto                            */
     double  rtol;        /* relative tolerance                                 */
@@ -329,6 +337,11 @@ int kcfd_record_norm(const double* norm2, double* chist, const int32_t* it, int3
 /* Barrier error flag of the handle's last launch (KCFD_TIMEOUT when a bounded team
  * barrier wait expired, else 0). Synchronises the stream.                         */
 int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream);
+
+/* Launch shape the handle resolved at creation: info[0] team (1 one CTA, 2 whole
+ * grid, 3 graph engine), info[1] lanes per row, info[2] threads per CTA, info[3]
+ * ILU(0) levels (1 without ILU). No reference counterpart (diagnostics).         */
+int kcfd_solver_info(const kcfd_solver* s, int32_t* info4);
 
 /* ------------------------------------------- allocation-free solve ---------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc --

@@ -27,10 +27,15 @@
 //    ranges, the lower part of a row is exactly its columns left of the diagonal, and
 //    the forward / backward sweeps read contiguous memory. b and x are permuted on
 //    entry and exit inside the same launch.
+//  * Large FP64 systems run on the graph engine instead (team 3, graph_engine.cuh):
+//    the same iteration as lean phase kernels in one CUDA graph with a device-side
+//    WHILE loop. A solve issued while its stream is being captured falls back to the
+//    persistent grid kernel (the engine's graph is not nested into the capture).
 #include <cuda_runtime.h>
 
 #include <algorithm>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 #include <mutex>
 #include <vector>
@@ -38,6 +43,7 @@
 
 #include "kcfd_common.h"
 #include "team.cuh"
+#include "graph_engine.cuh"
 
 namespace kcfd {
 
@@ -1068,6 +1074,22 @@ struct kcfd_solver {
     unsigned int* bar = nullptr;
     double* partials = nullptr;
     int* err = nullptr;
+    // graph engine (team 3)
+    struct {
+        ge::St* st = nullptr;
+        double* part = nullptr;
+        unsigned* cnt = nullptr;
+        double *gx = nullptr, *gb = nullptr, *vec = nullptr;  // gx/gb: the handle's px/pb with ILU
+        int* res_i = nullptr;      // [2*3] iters, status
+        double* res_d = nullptr;   // [3] relres
+        cudaGraph_t graph = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        const double* vals_key = nullptr;  // caller values the graph was built for (non-permuted)
+        int gmax = 0;
+        int eager = 0;                     // host-driven loop instead of the graph
+        bool ready = false;                // args (and graph) built
+        ge::Args args;
+    } g;
 };
 
 namespace {
@@ -1092,6 +1114,16 @@ void* solve_kernel_ptr(int mixed, int nrhs, int prec, bool grid) {
 
 int free_solver(kcfd_solver* s) {
     if (!s) return KCFD_OK;
+    if (s->g.exec) cudaGraphExecDestroy(s->g.exec);
+    if (s->g.graph) cudaGraphDestroy(s->g.graph);
+    {
+        // with ILU the engine's x/b are the handle's permuted vectors (freed below)
+        void* gx = (s->g.gx == s->px) ? nullptr : s->g.gx;
+        void* gb = (s->g.gb == s->pb) ? nullptr : s->g.gb;
+        void* gp[] = {s->g.st, s->g.part, s->g.cnt, gx, gb, s->g.vec, s->g.res_i, s->g.res_d};
+        for (void* p : gp)
+            if (p) cudaFree(p);
+    }
     void* ps[] = {s->work, s->r64, s->dinv, s->v32own, s->lev_ptr, s->perm, s->p_indptr, s->p_indices, s->p_src, s->p_diag,
                   s->p_vals64, s->p_vals32, s->px, s->pb, s->lu, s->ludinv, s->bar, s->partials, s->err};
     for (void* p : ps)
@@ -1144,7 +1176,7 @@ SolveArgs make_args(const kcfd_solver* s, const kcfd_csr_t* A) {
 int launch_team(const kcfd_solver* s, void* kernel, void** args, cudaStream_t st) {
     KCFD_CUDA(cudaMemsetAsync(s->bar, 0, 2 * sizeof(unsigned), st));
     KCFD_CUDA(cudaMemsetAsync(s->err, 0, sizeof(int), st));
-    if (s->team == 2) {
+    if (s->team >= 2) {
         KCFD_CUDA(cudaLaunchCooperativeKernel(kernel, dim3(s->grid), dim3(s->block), args, 0, st));
     } else {
         KCFD_CUDA(cudaLaunchKernel(kernel, dim3(1), dim3(s->block), args, 0, st));
@@ -1157,6 +1189,261 @@ template <typename T>
 bool upload(T** dst, const std::vector<T>& v) {
     if (cudaMalloc(dst, std::max<size_t>(v.size(), 1) * sizeof(T)) != cudaSuccess) return false;
     return v.empty() || cudaMemcpy(*dst, v.data(), v.size() * sizeof(T), cudaMemcpyHostToDevice) == cudaSuccess;
+}
+
+// ------------------------------------------------------------ graph engine host --
+// Grid of each phase kernel: its own occupancy on every SM, capped by the rows it has
+// (a vector kernel takes Ilp::U rows per thread and step) and by the partial slots.
+struct GeGrid {
+    int init, p, fwd, bwd, sv, s, st, xr;
+};
+
+template <int NRHS, int PREC>
+GeGrid ge_grids(int n, int sms, int gmax) {
+    auto g = [&](const void* f, int rows_per_thread) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, ge::kBlock, 0) != cudaSuccess || occ < 1) occ = 1;
+        const int64_t per = (int64_t)ge::kBlock * rows_per_thread;
+        const int64_t need = ((int64_t)n + per - 1) / per;
+        return (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)occ * sms, need, (int64_t)gmax}));
+    };
+    constexpr int U = ge::Ilp<NRHS>::U;
+    GeGrid r;
+    r.init = g((const void*)ge::g_init<NRHS>, 1);
+    r.p = g((const void*)ge::g_p<NRHS, PREC>, U);
+    r.fwd = g((const void*)ge::g_fwd<NRHS>, 1);
+    r.bwd = g((const void*)ge::g_bwd<NRHS>, 1);
+    r.sv = g((const void*)ge::g_spmv_v<NRHS, PREC>, 1);
+    r.s = g((const void*)ge::g_s<NRHS, PREC>, U);
+    r.st = g((const void*)ge::g_spmv_t<NRHS, PREC>, 1);
+    r.xr = g((const void*)ge::g_xr<NRHS, PREC>, U);
+    return r;
+}
+
+// One loop trip: the phase kernels of one BiCGSTAB iteration.
+template <int NRHS, int PREC>
+void ge_body(const ge::Args& a, const GeGrid& G, cudaStream_t cs) {
+    ge::g_p<NRHS, PREC><<<G.p, ge::kBlock, 0, cs>>>(a);
+    auto sweeps = [&](int which) {
+        if (PREC != KCFD_PREC_ILU0) return;
+        if (a.nlev == 1) {
+            ge::g_bwd<NRHS><<<G.bwd, ge::kBlock, 0, cs>>>(a, 0, which);
+            return;
+        }
+        for (int l = 1; l < a.nlev; ++l) ge::g_fwd<NRHS><<<G.fwd, ge::kBlock, 0, cs>>>(a, l, which);
+        for (int l = a.nlev - 2; l >= 0; --l) ge::g_bwd<NRHS><<<G.bwd, ge::kBlock, 0, cs>>>(a, l, which);
+    };
+    sweeps(0);
+    ge::g_spmv_v<NRHS, PREC><<<G.sv, ge::kBlock, 0, cs>>>(a);
+    ge::g_s<NRHS, PREC><<<G.s, ge::kBlock, 0, cs>>>(a);
+    sweeps(1);
+    ge::g_spmv_t<NRHS, PREC><<<G.st, ge::kBlock, 0, cs>>>(a);
+    ge::g_xr<NRHS, PREC><<<G.xr, ge::kBlock, 0, cs>>>(a);
+}
+
+// Eager form: init, body trips in chunks with a host read of the active flag, final.
+template <int NRHS, int PREC>
+int ge_eager(kcfd_solver* s, cudaStream_t st) {
+    const ge::Args& a = s->g.args;
+    const GeGrid G = ge_grids<NRHS, PREC>(s->n, s->sm_count, s->g.gmax);
+    ge::g_init<NRHS><<<G.init, ge::kBlock, 0, st>>>(a);
+    KCFD_CUDA(cudaGetLastError());
+    constexpr int kChunk = 8;
+    for (int trips = 0; trips <= a.maxiter + 2; trips += kChunk) {
+        int active = 0;
+        KCFD_CUDA(cudaMemcpyAsync(&active, &a.st->active, sizeof(int), cudaMemcpyDeviceToHost, st));
+        KCFD_CUDA(cudaStreamSynchronize(st));
+        if (!active) break;
+        for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC>(a, G, st);
+        KCFD_CUDA(cudaGetLastError());
+    }
+    ge::g_final<NRHS><<<1, 256, 0, st>>>(a);
+    KCFD_CUDA(cudaGetLastError());
+    return KCFD_OK;
+}
+
+template <int NRHS, int PREC>
+int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
+    auto& g = s->g;
+    const int n = s->n;
+    ge::Args a;
+    std::memset(&a, 0, sizeof(a));
+    a.n = n;
+    a.nlev = s->nlev;
+    a.stop = s->o.stop;
+    a.maxiter = s->o.maxiter;
+    a.gmax = g.gmax;
+    a.rtol = s->o.rtol;
+    a.atol = s->o.atol;
+    a.lev = s->lev_ptr;
+    if (s->perm) {
+        a.ip = s->p_indptr;
+        a.ix = s->p_indices;
+        a.vals = s->p_vals64;
+    } else {
+        a.ip = A->indptr;
+        a.ix = A->indices;
+        a.vals = A->vals64;
+    }
+    a.diag = s->p_diag;
+    a.dinv = (const double*)s->dinv;
+    a.lu = (const double*)s->lu;
+    a.ldi = (const double*)s->ludinv;
+    const size_t len = (size_t)n * NRHS;
+    a.x = g.gx;
+    a.b = g.gb;
+    double* v = g.vec;
+    a.r = v; a.rh = v + len; a.p = v + 2 * len; a.v = v + 3 * len; a.t = v + 4 * len; a.ph = v + 5 * len;
+    a.sh = v + 6 * len;
+    a.st = g.st;
+    a.part = g.part;
+    a.cnt = g.cnt;
+    a.out_iters = g.res_i;
+    a.out_status = g.res_i + 3;
+    a.out_relres = g.res_d;
+    a.eager = g.eager;
+    if (g.exec) cudaGraphExecDestroy(g.exec);
+    if (g.graph) cudaGraphDestroy(g.graph);
+    g.exec = nullptr;
+    g.graph = nullptr;
+    g.ready = false;
+    if (g.eager) {
+        // no graph: the host loop launches the same kernels (ge_eager)
+        g.args = a;
+        g.vals_key = A->vals64;
+        g.ready = true;
+        return KCFD_OK;
+    }
+    KCFD_CUDA(cudaGraphCreate(&g.graph, 0));
+    cudaGraphConditionalHandle cond;
+    KCFD_CUDA(cudaGraphConditionalHandleCreate(&cond, g.graph, 1, cudaGraphCondAssignDefault));
+    a.cond = cond;
+    g.args = a;
+    const GeGrid G = ge_grids<NRHS, PREC>(n, s->sm_count, g.gmax);
+    void* args[] = {&a};
+    cudaKernelNodeParams kp;
+    std::memset(&kp, 0, sizeof(kp));
+    kp.func = (void*)ge::g_init<NRHS>;
+    kp.gridDim = dim3(G.init);
+    kp.blockDim = dim3(ge::kBlock);
+    kp.kernelParams = args;
+    cudaGraphNode_t n_init, n_cond, n_fin;
+    KCFD_CUDA(cudaGraphAddKernelNode(&n_init, g.graph, nullptr, 0, &kp));
+    // zero-initialised storage (the struct's default constructor is deleted)
+    alignas(cudaGraphNodeParams) unsigned char cp_buf[sizeof(cudaGraphNodeParams)] = {};
+    cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_buf);
+    cp.type = cudaGraphNodeTypeConditional;
+    cp.conditional.handle = cond;
+    cp.conditional.type = cudaGraphCondTypeWhile;
+    cp.conditional.size = 1;
+    KCFD_CUDA(cudaGraphAddNode(&n_cond, g.graph, &n_init, 1, &cp));
+    cudaGraph_t body = cp.conditional.phGraph_out[0];
+    cudaStream_t cs;
+    KCFD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
+    cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        ge_body<NRHS, PREC>(a, G, cs);
+        cudaGraph_t outg = nullptr;
+        const cudaError_t e2 = cudaStreamEndCapture(cs, &outg);
+        if (e == cudaSuccess) e = e2;
+    }
+    const cudaError_t e3 = cudaStreamDestroy(cs);
+    KCFD_CUDA(e);
+    KCFD_CUDA(e3);
+    kp.func = (void*)ge::g_final<NRHS>;
+    kp.gridDim = dim3(1);
+    kp.blockDim = dim3(256);
+    KCFD_CUDA(cudaGraphAddKernelNode(&n_fin, g.graph, &n_cond, 1, &kp));
+    KCFD_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    g.vals_key = A->vals64;
+    g.ready = true;
+    return KCFD_OK;
+}
+
+// Run-time (nrhs, precond) -> template instance.
+template <template <int, int> class F, typename... Ts>
+int ge_dispatch(const kcfd_solver* s, Ts... args) {
+    const int r = s->o.nrhs, p = s->o.precond;
+#define GE_CASE(R, P) \
+    if (r == R && p == P) return F<R, P>::run(args...);
+    GE_CASE(1, 0) GE_CASE(1, 1) GE_CASE(1, 2) GE_CASE(2, 0) GE_CASE(2, 1) GE_CASE(2, 2)
+    GE_CASE(3, 0) GE_CASE(3, 1) GE_CASE(3, 2)
+#undef GE_CASE
+    set_error("graph engine: unsupported configuration (nrhs %d, precond %d)", r, p);
+    return KCFD_BAD_INPUT;
+}
+
+template <int R, int P>
+struct GeBuild {
+    static int run(kcfd_solver* s, const kcfd_csr_t* A) { return ge_build<R, P>(s, A); }
+};
+template <int R, int P>
+struct GeEager {
+    static int run(kcfd_solver* s, cudaStream_t st) { return ge_eager<R, P>(s, st); }
+};
+
+int ge_alloc(kcfd_solver* s) {
+    auto& g = s->g;
+    const size_t len = (size_t)s->n * s->o.nrhs;
+    g.gmax = s->sm_count * 8;  // 256-thread blocks: at most 8 resident per SM
+    bool ok = cudaMalloc(&g.st, sizeof(ge::St)) == cudaSuccess &&
+              cudaMalloc(&g.part, (size_t)ge::kSlotsG * 8 * g.gmax * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&g.cnt, ge::kSlotsG * sizeof(unsigned)) == cudaSuccess &&
+              cudaMalloc(&g.vec, 7 * len * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&g.res_i, 6 * sizeof(int)) == cudaSuccess && cudaMalloc(&g.res_d, 3 * sizeof(double)) == cudaSuccess;
+    if (ok) {
+        if (s->perm) {
+            g.gx = s->px;
+            g.gb = s->pb;
+        } else {
+            ok = cudaMalloc(&g.gx, len * sizeof(double)) == cudaSuccess &&
+                 cudaMalloc(&g.gb, len * sizeof(double)) == cudaSuccess;
+        }
+    }
+    ok = ok && cudaMemset(g.cnt, 0, ge::kSlotsG * sizeof(unsigned)) == cudaSuccess &&
+         cudaMemset(g.st, 0, sizeof(ge::St)) == cudaSuccess;
+    if (!ok) {
+        set_error("graph engine: device allocation failed");
+        return KCFD_CUDA_ERROR;
+    }
+    return KCFD_OK;
+}
+
+template <int NRHS>
+void ge_copies(const kcfd_solver* s, bool in, const double* b, double* x, int32_t* iters, double* relres,
+               int32_t* status, cudaStream_t st) {
+    const int n = s->n;
+    const int blocks = std::max(1, std::min((n + 255) / 256, s->sm_count * 8));
+    if (in)
+        ge::g_copy_in<NRHS><<<blocks, 256, 0, st>>>(n, s->perm, x, b, s->g.gx, s->g.gb);
+    else
+        ge::g_copy_out<NRHS><<<blocks, 256, 0, st>>>(n, s->perm, s->g.gx, x, s->g.res_i, s->g.res_d, s->g.res_i + 3,
+                                                     iters, relres, status);
+}
+
+int ge_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, double* x, int32_t* iters, double* relres,
+             int32_t* status, cudaStream_t st) {
+    auto& g = s->g;
+    // the graph holds the matrix pointers: rebuilt when the caller's values move
+    // (with ILU the engine reads the handle's own permuted copy)
+    if (!g.ready || (!s->perm && g.vals_key != A->vals64)) {
+        if (int e = ge_dispatch<GeBuild>(s, s, A)) return e;
+    }
+    auto copies = [&](bool in) {
+        if (s->o.nrhs == 1) ge_copies<1>(s, in, b, x, iters, relres, status, st);
+        else if (s->o.nrhs == 2) ge_copies<2>(s, in, b, x, iters, relres, status, st);
+        else ge_copies<3>(s, in, b, x, iters, relres, status, st);
+    };
+    copies(true);
+    KCFD_CUDA(cudaGetLastError());
+    if (g.eager) {
+        if (int e = ge_dispatch<GeEager>(s, s, st)) return e;
+    } else {
+        KCFD_CUDA(cudaGraphLaunch(g.exec, st));
+    }
+    copies(false);
+    KCFD_CUDA(cudaGetLastError());
+    return KCFD_OK;
 }
 
 }  // namespace
@@ -1226,9 +1513,17 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     for (int k = 0; k < nnz; ++k)
         if (ix[k] < 0 || ix[k] >= n) return fail("kcfd_solver_create: column index %d out of range at %d", ix[k], k);
     // team and launch shape
+    // auto: one CTA for small systems; large FP64 systems on the graph engine, large
+    // mixed ones on the persistent grid kernel
     int team = opts->team;
-    if (team == 0) team = ((int64_t)n * nrhs <= 40000) ? 1 : 2;
+    if (team == 0) team = ((int64_t)n * nrhs <= 40000) ? 1 : (mixed ? 2 : 3);
+    if (team < 1 || team > 3) return fail("kcfd_solver_create: team must be 0..3");
+    if (team == 3 && mixed) return fail("kcfd_solver_create: the graph engine (team 3) runs FP64 only");
     s->team = team;
+    if (team == 3) {
+        const char* ev = std::getenv("KCFD_ENGINE_EAGER");
+        s->g.eager = (ev && ev[0] == '1') ? 1 : 0;
+    }
     int lanes = opts->lanes;
     if (lanes <= 0) {
         // one lane streams up to ~8 entries of a row (FVM rows have 4-7): measured
@@ -1241,7 +1536,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     s->lanes = lanes;
     const int max_grid_block = grid_block(nrhs);
     s->block = opts->block > 0 ? opts->block : (team == 1 ? 1024 : max_grid_block);
-    if (team == 2 && s->block > max_grid_block) s->block = max_grid_block;
+    if (team >= 2 && s->block > max_grid_block) s->block = max_grid_block;
     if (team == 1 && s->block > 1024) s->block = 1024;
     if (s->block % 32 != 0 || s->block < 32) return fail("kcfd_solver_create: block must be a multiple of 32");
     // levels
@@ -1306,8 +1601,10 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         lptr = {0, n};
         s->nlev = 1;
     }
-    void* kern = solve_kernel_ptr(mixed, nrhs, opts->precond, team == 2);
-    if (team == 2) {
+    // team 3 keeps the grid kernel's launch shape too: it factors ILU(0) with the
+    // grid factor kernel and solves on the grid kernel inside stream captures
+    void* kern = solve_kernel_ptr(mixed, nrhs, opts->precond, team >= 2);
+    if (team >= 2) {
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, s->block, 0) != cudaSuccess || per_sm < 1) {
             free_solver(s);
@@ -1344,14 +1641,30 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         set_error("kcfd_solver_create: device allocation failed");
         return KCFD_CUDA_ERROR;
     }
+    if (team == 3) {
+        if (int e = ge_alloc(s)) {
+            free_solver(s);
+            return e;
+        }
+    }
     *out = s;
     return KCFD_OK;
 }
 
-void kcfd_solver_destroy(kcfd_solver* s) { free_solver(s); }
+void kcfd_solver_destroy(kcfd_solver* s) {
+    free_solver(s);
+    (void)cudaGetLastError();  // a destructor reports nothing; it leaves no error behind
+}
 
 int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
     KCFD_REQUIRE(s && A, "kcfd_solver_setup: NULL argument");
+    {
+        const cudaError_t pend = cudaGetLastError();
+        if (pend != cudaSuccess) {
+            set_error("kcfd_solver_setup: error left by an earlier CUDA call: %s", cudaGetErrorString(pend));
+            return KCFD_CUDA_ERROR;
+        }
+    }
     KCFD_REQUIRE(A->n == s->n && A->nnz == s->nnz, "kcfd_solver_setup: matrix size differs from the bound pattern");
     KCFD_REQUIRE(A->vals64, "kcfd_solver_setup: FP64 values required");
     cudaStream_t st = (cudaStream_t)stream;
@@ -1376,7 +1689,7 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
         KCFD_CUDA(cudaGetLastError());
         SolveArgs a = make_args(s, A);
         void* args[] = {&a};
-        void* k = s->team == 2 ? (mixed ? (void*)ilu0_factor_grid<float> : (void*)ilu0_factor_grid<double>)
+        void* k = s->team >= 2 ? (mixed ? (void*)ilu0_factor_grid<float> : (void*)ilu0_factor_grid<double>)
                                : (mixed ? (void*)ilu0_factor_cta<float> : (void*)ilu0_factor_cta<double>);
         return launch_team(s, k, args, st);
     }
@@ -1396,10 +1709,25 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
     a.iters_out = iters;
     a.relres_out = relres;
     a.status_out = status;
-    void* kern = solve_kernel_ptr(mixed, s->o.nrhs, s->o.precond, s->team == 2);
+    if (s->team == 3) {
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        KCFD_CUDA(cudaStreamIsCapturing((cudaStream_t)stream, &cap));
+        if (cap == cudaStreamCaptureStatusNone)
+            return ge_solve(s, A, b, x, iters, relres, status, (cudaStream_t)stream);
+    }
+    void* kern = solve_kernel_ptr(mixed, s->o.nrhs, s->o.precond, s->team >= 2);
     KCFD_REQUIRE(kern != nullptr, "kcfd_solver_solve: no kernel for this configuration");
     void* args[] = {&a};
     return launch_team(s, kern, args, (cudaStream_t)stream);
+}
+
+int kcfd_solver_info(const kcfd_solver* s, int32_t* info4) {
+    KCFD_REQUIRE(s && info4, "kcfd_solver_info: NULL argument");
+    info4[0] = s->team;
+    info4[1] = s->lanes;
+    info4[2] = s->block;
+    info4[3] = s->nlev > 0 ? s->nlev : 1;
+    return KCFD_OK;
 }
 
 int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream) {
@@ -1721,9 +2049,10 @@ __global__ void spmv_kernel(int n, const int* __restrict__ ip, const int* __rest
 
 template <typename V>
 int spmv_launch(const kcfd_csr_t* A, const V* vals, const V* x, V* y, int nrhs, cudaStream_t st) {
-    double avg = (double)A->nnz / std::max(A->n, 1);
+    // one lane streams up to ~8 entries of a row, as in the solver kernels
+    const double avg = (double)A->nnz / std::max(A->n, 1);
     int L = 1;
-    while (L < 32 && L < avg) L <<= 1;
+    while (L < 32 && 8 * L < avg) L <<= 1;
     const int threads = 256;
     int blocks = (int)std::min<int64_t>(((int64_t)A->n * L + threads - 1) / threads, 148 * 16);
     blocks = std::max(blocks, 1);

@@ -61,6 +61,7 @@ SIGNATURES = {
     "kcfd_solver_setup": (i32, [vp, C.POINTER(Csr), vp]),
     "kcfd_solver_solve": (i32, [vp, C.POINTER(Csr), vp, vp, vp, vp, vp, vp]),
     "kcfd_solver_error": (i32, [vp, P_i32, vp]),
+    "kcfd_solver_info": (i32, [vp, P_i32]),
     "kcfd_mass_flux": (i32, [vp, vp, vp, f64, vp, vp]),
     "kcfd_momentum_assemble": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_pressure_assemble": (i32, [vp, vp, f64, vp, vp, vp, vp, vp, vp, vp]),

@@ -159,10 +159,13 @@ class SIMPLESolver:
                                    P(self.it_dev), self.hist_cap, st), "simple_residual")
 
     def iterate(self, n=1):
-        """Run n outer iterations (graph replay when graph=True)."""
+        """Run n outer iterations (graph replay when graph=True). Solvers that run as
+        their own graph (large FP64 systems) are not captured: for those the outer
+        iteration is launched directly, its few kernel launches cost little beside
+        the solves."""
         torch = _lib.require_cuda()
         self.bcs.upload()
-        if self.graph:
+        if self.graph and not (self.s_m.graph_engine or self.s_p.graph_engine):
             if self._graph is None:
                 s = torch.cuda.Stream()
                 s.wait_stream(torch.cuda.current_stream())

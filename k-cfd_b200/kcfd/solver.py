@@ -78,7 +78,8 @@ class Solver:
 
     precond: 'none' | 'jacobi' | 'ilu0'; stop: _lib.STOP_SCIPY | _lib.STOP_GPU;
     mode: _lib.MODE_FP64 | _lib.MODE_MIXED; nrhs: 1 or 3; team: 0 auto, 1 one CTA,
-    2 whole grid; levels: ILU(0) level of each row (e.g. mesh.cell_color), None for
+    2 whole grid (persistent cooperative kernel), 3 graph engine (phase kernels in a
+    CUDA graph with a device-side WHILE loop; FP64 only); levels: ILU(0) level of each row (e.g. mesh.cell_color), None for
     natural-order levels.
     """
 
@@ -136,6 +137,19 @@ class Solver:
                                                 _lib.ptr(self.relres), _lib.ptr(self.status),
                                                 _lib.stream_handle(stream)), "kcfd_solver_solve")
         return self.iters, self.relres, self.status
+
+    def info(self):
+        """Resolved launch shape: dict(team, lanes, block, levels)."""
+        v = np.zeros(4, dtype=np.int32)
+        _lib.check(_lib.lib().kcfd_solver_info(self._h, v.ctypes.data_as(_lib.P_i32)), "kcfd_solver_info")
+        return {"team": int(v[0]), "lanes": int(v[1]), "block": int(v[2]), "levels": int(v[3])}
+
+    @property
+    def graph_engine(self):
+        """True when solves run as the handle's own CUDA graph (team 3). Such a solve
+        is not nested into an enclosing stream capture (there it runs on the
+        persistent grid kernel), so callers keep it outside their captures."""
+        return self.info()["team"] == 3
 
     def barrier_error(self, stream=None):
         e = C.c_int32(0)

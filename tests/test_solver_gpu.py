@@ -111,7 +111,7 @@ def test_grid_and_cta_teams_agree(torch_cuda):
     from kcfd import meshgen, mesh as km
     n_, c_, f_, b_ = meshgen.hex_box_arrays(1, 1, 1, 14, 14, 14, meshgen.CAVITY_3D_NAMES)
     colors = km.build_mesh(n_, c_, b_, ndim=3, cell_face_node_list=f_).cell_color
-    for team in (1, 2):
+    for team in (1, 2, 3):
         for pc, lev in (("jacobi", None), ("ilu0", None), ("ilu0", colors)):
             s = Solver(d, precond=pc, rtol=1e-10, maxiter=5000, team=team, levels=lev)
             s.setup(d)
@@ -123,6 +123,121 @@ def test_grid_and_cta_teams_agree(torch_cuda):
     xd = spla.spsolve(A.tocsc(), b)
     for x in xs:
         assert _rel(x, xd) < 1e-8
+
+
+def test_graph_engine_matches_persistent_kernel(torch_cuda):
+    """Team 3 (lean phase kernels in a CUDA graph with a WHILE node) runs the same
+    algorithm as the persistent grid kernel; only the partition of the fixed-order
+    reductions differs. So: after 12 iterations (stopped by maxiter) the iterates agree
+    to rounding (1e-9 relative), and run to rtol 1e-10 both converge to the direct
+    solution. The iteration counts of full runs are not compared exactly: BiCGSTAB on
+    this nonsymmetric convection system is sensitive to rounding near its plateau.
+    1 and 3 right-hand sides, both stopping rules, Jacobi and two-level ILU(0)."""
+    from kcfd import _lib
+    from kcfd.solver import DeviceCSR, Solver
+    from kcfd import meshgen, mesh as km
+    torch = torch_cuda
+    m, A, b = _hex_system(24, seed=11)
+    d = DeviceCSR.from_scipy(A)
+    n_, c_, f_, b_ = meshgen.hex_box_arrays(1, 1, 1, 24, 24, 24, meshgen.CAVITY_3D_NAMES)
+    colors = km.build_mesh(n_, c_, b_, ndim=3, cell_face_node_list=f_).cell_color
+    rng = np.random.default_rng(2)
+    B = rng.normal(size=(A.shape[0], 3))
+    X = spla.splu(A.tocsc()).solve(B)
+    for nrhs in (1, 3):
+        bb = torch.from_numpy(np.ascontiguousarray(B[:, 0] if nrhs == 1 else B)).cuda()
+        xd = X[:, 0] if nrhs == 1 else X
+        for stop in (_lib.STOP_SCIPY, _lib.STOP_GPU):
+            for pc, lev in (("jacobi", None), ("ilu0", colors)):
+                short, full = {}, {}
+                for team in (2, 3):
+                    for maxiter, out in ((12, short), (5000, full)):
+                        s = Solver(d, precond=pc, stop=stop, rtol=1e-10, maxiter=maxiter, team=team, nrhs=nrhs,
+                                   levels=lev)
+                        assert s.info()["team"] == team
+                        s.setup(d)
+                        x = torch.zeros_like(bb)
+                        it, rr, st = s.solve(d, bb, x)
+                        want = 1 if maxiter == 12 else 0
+                        assert list(st.cpu().numpy()) == [want] * nrhs, (team, pc, stop, maxiter)
+                        out[team] = x.cpu().numpy()
+                assert _rel(short[3], short[2]) < 1e-9, (pc, stop, nrhs, _rel(short[3], short[2]))
+                for team in (2, 3):
+                    assert _rel(full[team], xd) < 1e-7, (team, pc, stop, nrhs)
+
+
+def test_graph_engine_repeat_and_maxiter(torch_cuda):
+    """Deterministic across launches; an iteration cap ends the loop with MAXITER."""
+    from kcfd.solver import DeviceCSR, Solver
+    torch = torch_cuda
+    m, A, b = _hex_system(20, seed=13)
+    d = DeviceCSR.from_scipy(A)
+    bd = torch.from_numpy(b).cuda()
+    s = Solver(d, precond="jacobi", rtol=1e-12, maxiter=5000, team=3)
+    s.setup(d)
+    xs = []
+    for _ in range(2):
+        x = torch.zeros_like(bd)
+        s.solve(d, bd, x)
+        xs.append(x.cpu().numpy())
+    np.testing.assert_array_equal(xs[0], xs[1])
+    s2 = Solver(d, precond="jacobi", rtol=1e-14, maxiter=3, team=3)
+    s2.setup(d)
+    x = torch.zeros_like(bd)
+    it, rr, st = s2.solve(d, bd, x)
+    assert int(st[0]) == 1 and int(it[0]) == 3
+
+
+def test_graph_engine_eager_form_is_bitwise_equal(torch_cuda, monkeypatch):
+    """KCFD_ENGINE_EAGER=1 launches the same phase kernels with the same grids from a
+    host loop (for profilers), so the results are bitwise the same."""
+    from kcfd.solver import DeviceCSR, Solver
+    from kcfd import meshgen, mesh as km
+    torch = torch_cuda
+    m, A, b = _hex_system(20, seed=17)
+    d = DeviceCSR.from_scipy(A)
+    bd = torch.from_numpy(b).cuda()
+    n_, c_, f_, b_ = meshgen.hex_box_arrays(1, 1, 1, 20, 20, 20, meshgen.CAVITY_3D_NAMES)
+    colors = km.build_mesh(n_, c_, b_, ndim=3, cell_face_node_list=f_).cell_color
+    for pc, lev in (("jacobi", None), ("ilu0", colors)):
+        out = []
+        for eager in ("0", "1"):
+            monkeypatch.setenv("KCFD_ENGINE_EAGER", eager)
+            s = Solver(d, precond=pc, rtol=1e-10, maxiter=5000, team=3, levels=lev)
+            s.setup(d)
+            x = torch.zeros_like(bd)
+            it, rr, st = s.solve(d, bd, x)
+            out.append((x.cpu().numpy(), int(it[0]), int(st[0])))
+        assert out[0][1] == out[1][1] and out[0][2] == out[1][2] == 0
+        np.testing.assert_array_equal(out[0][0], out[1][0])
+
+
+def test_graph_engine_inside_stream_capture(torch_cuda):
+    """A team-3 solve issued while its stream is captured runs on the grid kernel
+    (captured like any launch); the replayed graph solves the system."""
+    from kcfd.solver import DeviceCSR, Solver
+    torch = torch_cuda
+    m, A, b = _hex_system(16, seed=19)
+    d = DeviceCSR.from_scipy(A)
+    bd = torch.from_numpy(b).cuda()
+    s = Solver(d, precond="jacobi", rtol=1e-10, maxiter=5000, team=3)
+    s.setup(d)
+    x = torch.zeros_like(bd)
+    st = torch.cuda.Stream()
+    st.wait_stream(torch.cuda.current_stream())
+    with torch.cuda.stream(st):
+        s.solve(d, bd, x)   # warm-up outside the capture
+    torch.cuda.current_stream().wait_stream(st)
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.graph(g):
+        x.zero_()
+        s.solve(d, bd, x)
+    x.fill_(1.0)
+    g.replay()
+    torch.cuda.synchronize()
+    assert int(s.status[0]) == 0
+    xd = spla.spsolve(A.tocsc(), b)
+    assert _rel(x.cpu().numpy(), xd) < 1e-7
 
 
 def test_deterministic_repeat(torch_cuda):

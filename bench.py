@@ -135,12 +135,13 @@ def solver_bytes(n, nnz, iters, precond, w, nrhs=1):
 
 def solve_launches(solver, iters, precond, nlev):
     """Kernels one solve launches: the persistent kernels launch once; the graph
-    engine launches init, final and the two copies plus, per loop trip, the phase
-    kernels (5, and 2 (nlev - 1) ILU sweeps for each of phat and shat)."""
+    engine launches the value fill, init, final and the two copies plus, per loop
+    trip, the phase kernels (5, and 2 (nlev - 1) ILU sweeps for each of phat and
+    shat)."""
     if not solver.graph_engine:
         return 1
     body = 5 + (4 * (nlev - 1) if precond == "ilu0" else 0)
-    return 4 + body * int(iters)
+    return 5 + body * int(iters)
 
 
 def launches_per_step(s, its_m, its_p):

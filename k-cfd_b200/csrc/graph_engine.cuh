@@ -18,6 +18,14 @@
 // Scalar formulas and stopping tests are those of bicgstab_body (scipy and GPU-path
 // semantics), FP64 throughout.
 //
+// Matrix layout: sliced ELL with slices of 32 rows (SELL-32). Slice s holds rows
+// 32s..32s+31; entry k of row i sits at off[s] + 32 k + (i mod 32), padded to the
+// slice's longest row with column -1. A warp owns one slice, so each of its matrix
+// loads reads 32 consecutive values (fully coalesced) where a row-per-thread CSR
+// read touches a cache line per row. Entries keep their CSR order within a row, so
+// sums are the same as over the CSR. A holds whole rows (SpMV); L and U the strictly
+// lower and upper parts of the level-permuted ILU(0) factors.
+//
 // No kernel reads through the non-coherent path anything that the same launch
 // writes: x, r, p, z are read with plain loads; only the pattern, the matrix and
 // preconditioner values (constant during a solve) use __ldg.
@@ -39,16 +47,18 @@ struct St {
     int it, active, trips, pad;
 };
 
+struct Sell {
+    int* off;      // [slices + 1] first slot of each slice
+    int* col;      // [slots] column, -1 for padding
+    double* val;   // [slots]
+};
+
 struct Args {
     int n, nlev, stop, maxiter, gmax;
     double rtol, atol;
     const int* lev;
-    const int* ip;
-    const int* ix;
-    const int* diag;
-    const double* vals;
+    Sell A, L, U;
     const double* dinv;
-    const double* lu;
     const double* ldi;
     double *x, *b, *r, *rh, *p, *v, *t, *ph, *sh;
     St* st;
@@ -140,20 +150,28 @@ __device__ __forceinline__ void level_range(const Args& a, int l, int& r0, int& 
     r1 = (a.nlev == 1) ? a.n : a.lev[l + 1];
 }
 
-// acc += sum_k vals[k] x[ix[k]] (SUB: acc -= ...) over k in [kb, ke), in k order;
-// indices and values are loaded in batches of B before the gathers of x.
+// Slot of entry 0 of row i and the width of its slice.
+__device__ __forceinline__ void sell_row(const Sell& m, int i, int& base, int& w) {
+    const int sl = i >> 5;
+    const int o0 = __ldg(m.off + sl), o1 = __ldg(m.off + sl + 1);
+    base = o0 + (i & 31);
+    w = (o1 - o0) >> 5;
+}
+
+// acc += sum_k val x[col] over the row's entries (SUB: acc -= ...), in row order;
+// columns and values are loaded in batches of B before the gathers of x.
 template <int NRHS, bool SUB = false>
-__device__ __forceinline__ void row_gather(const int* __restrict__ ix, const double* __restrict__ vals,
-                                           const double* x, int kb, int ke, double (&acc)[NRHS]) {
+__device__ __forceinline__ void sell_gather(const Sell& m, int base, int w, const double* x, double (&acc)[NRHS]) {
     constexpr int B = NRHS == 1 ? 8 : 4;
-    for (int k0 = kb; k0 < ke; k0 += B) {
+    for (int k0 = 0; k0 < w; k0 += B) {
         int jj[B];
         double vv[B];
 #pragma unroll
         for (int u = 0; u < B; ++u) {
-            const bool in = k0 + u < ke;
-            jj[u] = in ? __ldg(ix + k0 + u) : -1;
-            vv[u] = in ? __ldg(vals + k0 + u) : 0.0;
+            const bool in = k0 + u < w;
+            const int slot = base + (k0 + u) * 32;
+            jj[u] = in ? __ldg(m.col + slot) : -1;
+            vv[u] = in ? __ldg(m.val + slot) : 0.0;
         }
         double xv[B][NRHS];
 #pragma unroll
@@ -172,6 +190,14 @@ __device__ __forceinline__ void row_gather(const int* __restrict__ ix, const dou
     }
 }
 
+// SELL values from a source array: out[k] = in[src[k]], 0 for padding.
+__global__ void g_fill(int64_t m, const int* __restrict__ src, const double* __restrict__ in, double* __restrict__ out) {
+    for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
+        const int j = src[k];
+        out[k] = j >= 0 ? in[j] : 0.0;
+    }
+}
+
 template <int NRHS>
 __global__ void __launch_bounds__(kBlock) g_init(Args a) {
     St& S = *a.st;
@@ -182,7 +208,9 @@ __global__ void __launch_bounds__(kBlock) g_init(Args a) {
         double acc[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) acc[c] = 0.0;
-        row_gather<NRHS>(a.ix, a.vals, a.x, __ldg(a.ip + i), __ldg(a.ip + i + 1), acc);
+        int base, w;
+        sell_row(a.A, i, base, w);
+        sell_gather<NRHS>(a.A, base, w, a.x, acc);
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) {
             const size_t q = (size_t)i * NRHS + c;
@@ -297,13 +325,16 @@ __global__ void __launch_bounds__(kBlock) g_fwd(Args a, int l, int which) {
     int r0, r1;
     level_range(a, l, r0, r1);
     const bool last = (l == a.nlev - 1);
-    for (int i = r0 + blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += gridDim.x * blockDim.x) {
-        const int kb = __ldg(a.ip + i), kd = __ldg(a.diag + i);
+    // rows from r0 rounded down to a slice boundary, so that warps and slices align
+    for (int i = (r0 & ~31) + blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += gridDim.x * blockDim.x) {
+        if (i < r0) continue;
         const double di = last ? __ldg(a.ldi + i) : 1.0;
         double acc[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) acc[c] = q[(size_t)i * NRHS + c];
-        row_gather<NRHS, true>(a.ix, a.lu, z, kb, kd, acc);
+        int base, w;
+        sell_row(a.L, i, base, w);
+        sell_gather<NRHS, true>(a.L, base, w, z, acc);
 #pragma unroll
         for (int c = 0; c < NRHS; ++c)
             if (!dn[c]) z[(size_t)i * NRHS + c] = acc[c] * di;
@@ -322,13 +353,15 @@ __global__ void __launch_bounds__(kBlock) g_bwd(Args a, int l, int which) {
     for (int c = 0; c < NRHS; ++c) dn[c] = which ? (S.done[c] || S.sconv[c]) : S.done[c];
     int r0, r1;
     level_range(a, l, r0, r1);
-    for (int i = r0 + blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += gridDim.x * blockDim.x) {
-        const int kd = __ldg(a.diag + i), ke = __ldg(a.ip + i + 1);
+    for (int i = (r0 & ~31) + blockIdx.x * blockDim.x + threadIdx.x; i < r1; i += gridDim.x * blockDim.x) {
+        if (i < r0) continue;
         const double di = __ldg(a.ldi + i);
         double acc[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) acc[c] = z[(size_t)i * NRHS + c];
-        row_gather<NRHS, true>(a.ix, a.lu, z, kd + 1, ke, acc);
+        int base, w;
+        sell_row(a.U, i, base, w);
+        sell_gather<NRHS, true>(a.U, base, w, z, acc);
 #pragma unroll
         for (int c = 0; c < NRHS; ++c)
             if (!dn[c]) z[(size_t)i * NRHS + c] = acc[c] * di;
@@ -344,14 +377,15 @@ __global__ void __launch_bounds__(kBlock) g_spmv_v(Args a) {
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) red[c] = 0.0;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        const int kb = __ldg(a.ip + i), ke = __ldg(a.ip + i + 1);
+        int base, w;
+        sell_row(a.A, i, base, w);
         double rhv[NRHS], acc[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) {
             rhv[c] = a.rh[(size_t)i * NRHS + c];
             acc[c] = 0.0;
         }
-        row_gather<NRHS>(a.ix, a.vals, ph, kb, ke, acc);
+        sell_gather<NRHS>(a.A, base, w, ph, acc);
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) {
             a.v[(size_t)i * NRHS + c] = acc[c];
@@ -477,14 +511,15 @@ __global__ void __launch_bounds__(kBlock) g_spmv_t(Args a) {
                 if (sc[c]) a.x[(size_t)i * NRHS + c] += al[c] * ph[(size_t)i * NRHS + c];
         }
         if (!active) continue;
-        const int kb = __ldg(a.ip + i), ke = __ldg(a.ip + i + 1);
+        int base, w;
+        sell_row(a.A, i, base, w);
         double sv[NRHS], acc[NRHS];
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) {
             sv[c] = a.r[(size_t)i * NRHS + c];
             acc[c] = 0.0;
         }
-        row_gather<NRHS>(a.ix, a.vals, sh, kb, ke, acc);
+        sell_gather<NRHS>(a.A, base, w, sh, acc);
 #pragma unroll
         for (int c = 0; c < NRHS; ++c) {
             if (dn[c]) continue;

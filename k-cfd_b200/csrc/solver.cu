@@ -34,7 +34,9 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <climits>
 #include <cmath>
+#include <cstdint>
 #include <cstdlib>
 #include <cstring>
 #include <mutex>
@@ -1089,6 +1091,11 @@ struct kcfd_solver {
         int eager = 0;                     // host-driven loop instead of the graph
         bool ready = false;                // args (and graph) built
         ge::Args args;
+        ge::Sell A, L, U;                  // sliced-ELL copies (L, U: ILU only)
+        int* srcA = nullptr;               // per slot: index into the caller's values, -1 padding
+        int* srcL = nullptr;               // per slot: index into the permuted CSR (lu), -1 padding
+        int* srcU = nullptr;
+        int64_t slotsA = 0, slotsL = 0, slotsU = 0;
     } g;
 };
 
@@ -1120,7 +1127,10 @@ int free_solver(kcfd_solver* s) {
         // with ILU the engine's x/b are the handle's permuted vectors (freed below)
         void* gx = (s->g.gx == s->px) ? nullptr : s->g.gx;
         void* gb = (s->g.gb == s->pb) ? nullptr : s->g.gb;
-        void* gp[] = {s->g.st, s->g.part, s->g.cnt, gx, gb, s->g.vec, s->g.res_i, s->g.res_d};
+        void* gp[] = {s->g.st, s->g.part, s->g.cnt, gx, gb, s->g.vec, s->g.res_i, s->g.res_d,
+                      (void*)s->g.A.off, (void*)s->g.A.col, (void*)s->g.A.val, (void*)s->g.L.off, (void*)s->g.L.col,
+                      (void*)s->g.L.val, (void*)s->g.U.off, (void*)s->g.U.col, (void*)s->g.U.val,
+                      s->g.srcA, s->g.srcL, s->g.srcU};
         for (void* p : gp)
             if (p) cudaFree(p);
     }
@@ -1192,6 +1202,10 @@ bool upload(T** dst, const std::vector<T>& v) {
 }
 
 // ------------------------------------------------------------ graph engine host --
+int ge_fill_grid(const kcfd_solver* s, int64_t m) {
+    return (int)std::max<int64_t>(1, std::min<int64_t>((m + 255) / 256, (int64_t)s->sm_count * 16));
+}
+
 // Grid of each phase kernel: its own occupancy on every SM, capped by the rows it has
 // (a vector kernel takes Ilp::U rows per thread and step) and by the partial slots.
 struct GeGrid {
@@ -1246,6 +1260,7 @@ template <int NRHS, int PREC>
 int ge_eager(kcfd_solver* s, cudaStream_t st) {
     const ge::Args& a = s->g.args;
     const GeGrid G = ge_grids<NRHS, PREC>(s->n, s->sm_count, s->g.gmax);
+    ge::g_fill<<<ge_fill_grid(s, s->g.slotsA), 256, 0, st>>>(s->g.slotsA, s->g.srcA, s->g.vals_key, s->g.A.val);
     ge::g_init<NRHS><<<G.init, ge::kBlock, 0, st>>>(a);
     KCFD_CUDA(cudaGetLastError());
     constexpr int kChunk = 8;
@@ -1276,18 +1291,10 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     a.rtol = s->o.rtol;
     a.atol = s->o.atol;
     a.lev = s->lev_ptr;
-    if (s->perm) {
-        a.ip = s->p_indptr;
-        a.ix = s->p_indices;
-        a.vals = s->p_vals64;
-    } else {
-        a.ip = A->indptr;
-        a.ix = A->indices;
-        a.vals = A->vals64;
-    }
-    a.diag = s->p_diag;
+    a.A = g.A;
+    a.L = g.L;
+    a.U = g.U;
     a.dinv = (const double*)s->dinv;
-    a.lu = (const double*)s->lu;
     a.ldi = (const double*)s->ludinv;
     const size_t len = (size_t)n * NRHS;
     a.x = g.gx;
@@ -1311,6 +1318,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
         // no graph: the host loop launches the same kernels (ge_eager)
         g.args = a;
         g.vals_key = A->vals64;
+        g.vals_key = A->vals64;
         g.ready = true;
         return KCFD_OK;
     }
@@ -1320,6 +1328,20 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     a.cond = cond;
     g.args = a;
     const GeGrid G = ge_grids<NRHS, PREC>(n, s->sm_count, g.gmax);
+    // node 1: the caller's values into the SELL copy (the graph holds their pointer)
+    int64_t f_m = g.slotsA;
+    const int* f_src = g.srcA;
+    const double* f_in = A->vals64;
+    double* f_out = g.A.val;
+    void* fargs[] = {&f_m, &f_src, &f_in, &f_out};
+    cudaKernelNodeParams kf;
+    std::memset(&kf, 0, sizeof(kf));
+    kf.func = (void*)ge::g_fill;
+    kf.gridDim = dim3(ge_fill_grid(s, g.slotsA));
+    kf.blockDim = dim3(256);
+    kf.kernelParams = fargs;
+    cudaGraphNode_t n_fill, n_init, n_cond, n_fin;
+    KCFD_CUDA(cudaGraphAddKernelNode(&n_fill, g.graph, nullptr, 0, &kf));
     void* args[] = {&a};
     cudaKernelNodeParams kp;
     std::memset(&kp, 0, sizeof(kp));
@@ -1327,8 +1349,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     kp.gridDim = dim3(G.init);
     kp.blockDim = dim3(ge::kBlock);
     kp.kernelParams = args;
-    cudaGraphNode_t n_init, n_cond, n_fin;
-    KCFD_CUDA(cudaGraphAddKernelNode(&n_init, g.graph, nullptr, 0, &kp));
+    KCFD_CUDA(cudaGraphAddKernelNode(&n_init, g.graph, &n_fill, 1, &kp));
     // zero-initialised storage (the struct's default constructor is deleted)
     alignas(cudaGraphNodeParams) unsigned char cp_buf[sizeof(cudaGraphNodeParams)] = {};
     cudaGraphNodeParams& cp = *reinterpret_cast<cudaGraphNodeParams*>(cp_buf);
@@ -1382,6 +1403,68 @@ struct GeEager {
     static int run(kcfd_solver* s, cudaStream_t st) { return ge_eager<R, P>(s, st); }
 };
 
+// Host SELL-32 of rows [0, n): row i's entries are [rb(i), re(i)) of a CSR with
+// columns col; src (empty: the CSR position itself) gives each entry's value source.
+struct SellHost {
+    std::vector<int> off, col, src;
+};
+
+template <class RB, class RE>
+bool make_sell(int n, RB rb, RE re, const std::vector<int>& col, const std::vector<int>& src, SellHost& h) {
+    const int ns = (n + 31) / 32;
+    h.off.assign(ns + 1, 0);
+    int64_t tot = 0;
+    for (int sl = 0; sl < ns; ++sl) {
+        int w = 0;
+        for (int i = 32 * sl; i < std::min(n, 32 * sl + 32); ++i) w = std::max(w, re(i) - rb(i));
+        h.off[sl] = (int)tot;
+        tot += 32LL * w;
+        if (tot > INT32_MAX) return false;
+    }
+    h.off[ns] = (int)tot;
+    h.col.assign(tot, -1);
+    h.src.assign(tot, -1);
+    for (int i = 0; i < n; ++i) {
+        const int b = rb(i), len = re(i) - b;
+        for (int k = 0; k < len; ++k) {
+            const int64_t slot = h.off[i >> 5] + 32LL * k + (i & 31);
+            h.col[slot] = col[b + k];
+            h.src[slot] = src.empty() ? b + k : src[b + k];
+        }
+    }
+    return true;
+}
+
+bool upload_sell(const SellHost& h, ge::Sell& d, int** src, int64_t& slots) {
+    slots = (int64_t)h.col.size();
+    return upload(&d.off, h.off) && upload(&d.col, h.col) && upload(src, h.src) &&
+           cudaMalloc(&d.val, std::max<int64_t>(slots, 1) * sizeof(double)) == cudaSuccess;
+}
+
+// The engine's SELL copies: A from the rows (rowptr, cols; src maps an entry to the
+// caller's value index, empty for the identity); with ILU (diag given) also the
+// strict lower / upper parts, whose values come from the factor in CSR position.
+int ge_build_sell(kcfd_solver* s, const std::vector<int>& rowptr, const std::vector<int>& cols,
+                  const std::vector<int>& src, const std::vector<int>& diag) {
+    auto& g = s->g;
+    const int n = s->n;
+    SellHost h;
+    bool ok = make_sell(n, [&](int i) { return rowptr[i]; }, [&](int i) { return rowptr[i + 1]; }, cols, src, h) &&
+              upload_sell(h, g.A, &g.srcA, g.slotsA);
+    if (ok && !diag.empty()) {
+        const std::vector<int> none;
+        ok = make_sell(n, [&](int i) { return rowptr[i]; }, [&](int i) { return diag[i]; }, cols, none, h) &&
+             upload_sell(h, g.L, &g.srcL, g.slotsL);
+        ok = ok && make_sell(n, [&](int i) { return diag[i] + 1; }, [&](int i) { return rowptr[i + 1]; }, cols, none, h) &&
+             upload_sell(h, g.U, &g.srcU, g.slotsU);
+    }
+    if (!ok) {
+        set_error("graph engine: sliced-ELL copy too large or device allocation failed");
+        return KCFD_CUDA_ERROR;
+    }
+    return KCFD_OK;
+}
+
 int ge_alloc(kcfd_solver* s) {
     auto& g = s->g;
     const size_t len = (size_t)s->n * s->o.nrhs;
@@ -1424,9 +1507,8 @@ void ge_copies(const kcfd_solver* s, bool in, const double* b, double* x, int32_
 int ge_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, double* x, int32_t* iters, double* relres,
              int32_t* status, cudaStream_t st) {
     auto& g = s->g;
-    // the graph holds the matrix pointers: rebuilt when the caller's values move
-    // (with ILU the engine reads the handle's own permuted copy)
-    if (!g.ready || (!s->perm && g.vals_key != A->vals64)) {
+    // the graph holds the caller's value pointer: rebuilt when it moves
+    if (!g.ready || g.vals_key != A->vals64) {
         if (int e = ge_dispatch<GeBuild>(s, s, A)) return e;
     }
     auto copies = [&](bool in) {
@@ -1541,6 +1623,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     if (s->block % 32 != 0 || s->block < 32) return fail("kcfd_solver_create: block must be a multiple of 32");
     // levels
     std::vector<int> lptr;
+    std::vector<int> pip, pix, psrc, pdiag;  // ILU: the level-permuted CSR (host copy)
     if (opts->precond == KCFD_PREC_ILU0) {
         std::vector<int> lev(n, 0);
         if (level_of_row_host) {
@@ -1564,7 +1647,10 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
             perm[fill[lev[i]]] = i;
             inv[i] = fill[lev[i]]++;
         }
-        std::vector<int> pip(n + 1, 0), pix(nnz), psrc(nnz), pdiag(n, -1);
+        pip.assign(n + 1, 0);
+        pix.assign(nnz, 0);
+        psrc.assign(nnz, 0);
+        pdiag.assign(n, -1);
         std::vector<std::pair<int, int>> row;
         for (int r = 0; r < n; ++r) {
             const int o = perm[r];
@@ -1642,7 +1728,9 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         return KCFD_CUDA_ERROR;
     }
     if (team == 3) {
-        if (int e = ge_alloc(s)) {
+        int e = ge_alloc(s);
+        if (!e) e = s->perm ? ge_build_sell(s, pip, pix, psrc, pdiag) : ge_build_sell(s, ip, ix, {}, {});
+        if (e) {
             free_solver(s);
             return e;
         }
@@ -1691,7 +1779,15 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
         void* args[] = {&a};
         void* k = s->team >= 2 ? (mixed ? (void*)ilu0_factor_grid<float> : (void*)ilu0_factor_grid<double>)
                                : (mixed ? (void*)ilu0_factor_cta<float> : (void*)ilu0_factor_cta<double>);
-        return launch_team(s, k, args, st);
+        if (int e = launch_team(s, k, args, st)) return e;
+        if (s->team == 3) {
+            // the factor's strict lower / upper parts into the engine's SELL copies
+            const double* lu = (const double*)s->lu;
+            ge::g_fill<<<ge_fill_grid(s, s->g.slotsL), 256, 0, st>>>(s->g.slotsL, s->g.srcL, lu, s->g.L.val);
+            ge::g_fill<<<ge_fill_grid(s, s->g.slotsU), 256, 0, st>>>(s->g.slotsU, s->g.srcU, lu, s->g.U.val);
+            KCFD_CUDA(cudaGetLastError());
+        }
+        return KCFD_OK;
     }
     return KCFD_OK;
 }

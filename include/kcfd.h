@@ -173,14 +173,18 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
 
 /* ------------------------------------------------------ batched systems ---- */
 /* Many independent systems (e.g. the pressure-correction systems of many meshes) of
- * uneven sizes solved in ONE persistent launch over packed CSR with per-system
- * offsets: each CTA takes the next system from a largest-first queue and solves it
- * alone (FP64 or MIXED BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule
- * per system). No counterpart API in the reference, which solves one system per call
+ * uneven sizes solved together over packed CSR with per-system offsets: each CTA takes
+ * the next system from a largest-first queue and solves it alone (FP64 or MIXED
+ * BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule per system). Two
+ * tiers run concurrently: systems of at least big_rows rows on 512-thread CTAs (one
+ * per SM), the rest on 256-thread CTAs; one persistent launch per tier. A system's
+ * tier depends only on its own size, so its result is the same alone and in any mix.
+ * No counterpart API in the reference, which solves one system per call
  * (core/linear_solver.py:14-70); results per system equal that path's semantics.     */
 typedef struct kcfd_batch kcfd_batch;
 typedef struct {
-    int32_t precond, stop, mode, maxiter, lanes, max_refine, inner_maxiter, pad;
+    int32_t precond, stop, mode, maxiter, lanes, max_refine, inner_maxiter;
+    int32_t big_rows;  /* tier threshold in rows: 0 default (16384), < 0 one tier */
     double  rtol, atol, inner_rtol;
 } kcfd_batch_opts_t;
 /* indptr_host: per system n[s]+1 local row pointers, concatenated; indices_host:

@@ -667,9 +667,13 @@ template <int NRHS>
 struct MState {
     double thr[NRHS], rn[NRHS], bn[NRHS], rn_prev[NRHS];
     int done[NRHS], applied[NRHS], revert[NRHS];
-    int left, stop_now, total_it, cap;
+    int left, stop_now, total_it, cap, grow, retry;
     double inner_atol;
 };
+
+// A refinement step that does not lower the FP64 residual is undone and retried from
+// the same iterate with twice the inner iteration cap, up to this many doublings.
+constexpr int kMaxGrow = 5;
 
 // MIXED solve: FP64 outer refinement around capped FP32 inner BiCGSTAB runs.
 template <int NRHS, int PREC, class Team>
@@ -697,6 +701,7 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
             out.iters[c] = 0;
         }
         ms.total_it = 0;
+        ms.grow = 0;
     }
     __syncthreads();
     for (int ref = 0;; ++ref) {
@@ -721,6 +726,7 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
         if (!tm.template allreduce<2 * NRHS>(red, 5, smem)) return;
         if (t0) {
             int left = 0;
+            ms.retry = 0;
             for (int c = 0; c < NRHS; ++c) {
                 ms.revert[c] = 0;
                 ms.bn[c] = sqrt(red[c]);
@@ -729,11 +735,16 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
                 out.bnorm[c] = ms.bn[c];
                 if (ms.done[c]) continue;
                 if (ms.applied[c] && !(r_new < ms.rn_prev[c])) {
-                    // the last refinement step did not lower the FP64 residual: undo it
+                    // the last refinement step did not lower the FP64 residual: undo it,
+                    // then retry with a larger inner cap, or give up
                     ms.revert[c] = 1;
-                    ms.done[c] = 1;
-                    out.status[c] = KCFD_BREAKDOWN;
                     ms.rn[c] = ms.rn_prev[c];
+                    if (ms.grow < kMaxGrow && ms.total_it < a.maxiter) {
+                        ms.retry = 1;
+                    } else {
+                        ms.done[c] = 1;
+                        out.status[c] = KCFD_BREAKDOWN;
+                    }
                 } else if (!finite(r_new)) {
                     ms.done[c] = 1;
                     out.status[c] = KCFD_BREAKDOWN;
@@ -760,7 +771,8 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
             for (int c = 0; c < NRHS; ++c)
                 if (!ms.done[c]) ia = fmin(ia, ms.thr[c] * 0.5);
             ms.inner_atol = ia;
-            ms.cap = min(a.inner_maxiter, a.maxiter - ms.total_it);
+            if (ms.retry) ms.grow += 1;
+            ms.cap = (int)min((long long)a.inner_maxiter << ms.grow, (long long)(a.maxiter - ms.total_it));
         }
         __syncthreads();
         // own rows: undo rejected steps, load the inner rhs, zero the inner solution
@@ -776,6 +788,11 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
             }
         });
         if (!ms.left || ms.stop_now) break;
+        if (ms.retry) {
+            // the residual of the restored iterate is recomputed at the top
+            if (!tm.sync()) return;
+            continue;
+        }
         // inner FP32 solve A32 e = r from e = 0 to max(inner_rtol ||r||, thr/2)
         bool ok = bicgstab_body<float, float, NRHS, PREC>(tm, a, a.vals32, w.xi, w.bi, true, w, KCFD_STOP_SCIPY,
                                                           a.inner_rtol, ms.inner_atol, ms.cap, st, smem);
@@ -848,6 +865,7 @@ struct BatchSys {
 
 struct BatchArgs {
     int nsys, lanes, mixed, precond, stop, maxiter, max_refine, inner_maxiter;
+    int nq;  // systems in this launch's queue (order[0..nq))
     double rtol, atol, inner_rtol;
     const BatchSys* sys;
     const int* order;
@@ -904,8 +922,8 @@ __global__ void batch_prep_kernel(BatchArgs B) {
     }
 }
 
-template <int MIXED, int PREC>
-__global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs B) {
+template <int MIXED, int PREC, int BLOCK>
+__global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 2 : 1) batch_kernel(BatchArgs B) {
     __shared__ double smem[32 * kMaxK];
     __shared__ int s_q;
     using V = typename std::conditional<MIXED, float, double>::type;
@@ -915,7 +933,7 @@ __global__ void __launch_bounds__(256, 2) batch_kernel(BatchArgs B) {
         __syncthreads();
         const int q = s_q;
         __syncthreads();
-        if (q >= B.nsys) break;
+        if (q >= B.nq) break;
         const int sid = B.order[q];
         const BatchSys S = B.sys[sid];
         SolveArgs a;
@@ -1851,20 +1869,34 @@ struct kcfd_batch {
     int* lev = nullptr;
     void* work = nullptr;
     double* r64 = nullptr;
+    // tiers: order[0..nbig) big systems (512-thread CTAs), then the rest
+    int nbig = 0, grid_big = 0;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace {
 int free_batch(kcfd_batch* b) {
     if (!b) return KCFD_OK;
+    if (b->side) cudaStreamDestroy(b->side);
+    if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+    if (b->ev_join) cudaEventDestroy(b->ev_join);
     void* ps[] = {b->sys, b->order, b->queue, b->indptr, b->indices, b->vals32, b->dinv, b->lev, b->work, b->r64};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete b;
     return KCFD_OK;
 }
-void* batch_kernel_ptr(int mixed, int precond) {
-    if (mixed) return precond == KCFD_PREC_JACOBI ? (void*)batch_kernel<1, KCFD_PREC_JACOBI> : (void*)batch_kernel<1, KCFD_PREC_NONE>;
-    return precond == KCFD_PREC_JACOBI ? (void*)batch_kernel<0, KCFD_PREC_JACOBI> : (void*)batch_kernel<0, KCFD_PREC_NONE>;
+template <int BLOCK>
+void* batch_kernel_ptr_t(int mixed, int precond) {
+    if (mixed)
+        return precond == KCFD_PREC_JACOBI ? (void*)batch_kernel<1, KCFD_PREC_JACOBI, BLOCK>
+                                           : (void*)batch_kernel<1, KCFD_PREC_NONE, BLOCK>;
+    return precond == KCFD_PREC_JACOBI ? (void*)batch_kernel<0, KCFD_PREC_JACOBI, BLOCK>
+                                       : (void*)batch_kernel<0, KCFD_PREC_NONE, BLOCK>;
+}
+void* batch_kernel_ptr(int mixed, int precond, bool big) {
+    return big ? batch_kernel_ptr_t<512>(mixed, precond) : batch_kernel_ptr_t<256>(mixed, precond);
 }
 }  // namespace
 
@@ -1922,21 +1954,32 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
     }
     b->n_total = ro;
     b->nnz_total = zo;
-    // largest first (longest-processing-time order for the dynamic queue)
+    // largest first (longest-processing-time order for the dynamic queues); the
+    // systems of at least big_rows rows form the first tier
     std::vector<int> order(nsys);
     for (int s = 0; s < nsys; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nnz[x] > nnz[y]; });
+    const int big_rows = b->o.big_rows == 0 ? 16384 : b->o.big_rows;
+    std::stable_partition(order.begin(), order.end(), [&](int x) { return big_rows > 0 && n[x] >= big_rows; });
+    b->nbig = 0;
+    for (int s = 0; s < nsys; ++s) b->nbig += (big_rows > 0 && n[s] >= big_rows) ? 1 : 0;
     const bool mixed = b->o.mode == KCFD_MODE_MIXED;
     const size_t vsz = mixed ? 4 : 8;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel_ptr(mixed, b->o.precond), 256, 0);
-    b->grid = std::max(1, std::min(nsys, std::max(1, per_sm) * sms));
+    int per_sm = 0, per_sm_big = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel_ptr(mixed, b->o.precond, false), 256, 0);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_big, batch_kernel_ptr(mixed, b->o.precond, true), 512, 0);
+    const int nsmall = nsys - b->nbig;
+    b->grid = std::max(1, std::min(std::max(nsmall, 1), std::max(1, per_sm) * sms));
+    b->grid_big = std::max(1, std::min(std::max(b->nbig, 1), std::max(1, per_sm_big) * sms));
     bool ok = cudaMalloc(&b->sys, nsys * sizeof(BatchSys)) == cudaSuccess &&
               cudaMemcpy(b->sys, sys.data(), nsys * sizeof(BatchSys), cudaMemcpyHostToDevice) == cudaSuccess &&
-              upload(&b->order, order) && cudaMalloc(&b->queue, sizeof(int)) == cudaSuccess &&
+              upload(&b->order, order) && cudaMalloc(&b->queue, 2 * sizeof(int)) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess &&
               cudaMalloc(&b->indptr, po * 4) == cudaSuccess &&
               cudaMemcpy(b->indptr, indptr_host, po * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMalloc(&b->indices, zo * 4) == cudaSuccess &&
@@ -1997,12 +2040,32 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
     B.iters = iters;
     B.relres = relres;
     B.status = status;
-    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, sizeof(int), st));
+    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, 2 * sizeof(int), st));
+    B.nq = b->nsys;
     void* args[] = {&B};
     const int pgrid = std::max(1, std::min(b->nsys, 4 * b->grid));
     KCFD_CUDA(cudaLaunchKernel(B.mixed ? (void*)batch_prep_kernel<1> : (void*)batch_prep_kernel<0>, dim3(pgrid),
                                dim3(256), args, 0, st));
-    KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond), dim3(b->grid), dim3(256), args, 0, st));
+    // big tier on the side stream, forked from and joined back into the caller's
+    BatchArgs Bb = B, Bs = B;
+    Bb.nq = b->nbig;
+    Bs.order = b->order + b->nbig;
+    Bs.queue = b->queue + 1;
+    Bs.nq = b->nsys - b->nbig;
+    void* args_b[] = {&Bb};
+    void* args_s[] = {&Bs};
+    if (b->nbig > 0) {
+        KCFD_CUDA(cudaEventRecord(b->ev_fork, st));
+        KCFD_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+        KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond, true), dim3(b->grid_big), dim3(512), args_b, 0,
+                                   b->side));
+    }
+    if (Bs.nq > 0)
+        KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond, false), dim3(b->grid), dim3(256), args_s, 0, st));
+    if (b->nbig > 0) {
+        KCFD_CUDA(cudaEventRecord(b->ev_join, b->side));
+        KCFD_CUDA(cudaStreamWaitEvent(st, b->ev_join, 0));
+    }
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }

@@ -22,7 +22,7 @@ from . import _lib
 
 class BatchOpts(C.Structure):
     _fields_ = [("precond", C.c_int32), ("stop", C.c_int32), ("mode", C.c_int32), ("maxiter", C.c_int32),
-                ("lanes", C.c_int32), ("max_refine", C.c_int32), ("inner_maxiter", C.c_int32), ("pad", C.c_int32),
+                ("lanes", C.c_int32), ("max_refine", C.c_int32), ("inner_maxiter", C.c_int32), ("big_rows", C.c_int32),
                 ("rtol", C.c_double), ("atol", C.c_double), ("inner_rtol", C.c_double)]
 
 
@@ -30,7 +30,8 @@ class BatchSolver:
     """patterns: list of (indptr, indices) host arrays (one per system)."""
 
     def __init__(self, patterns, mode="mixed", precond="jacobi", rtol=1e-8, atol=0.0, maxiter=20000, lanes=1,
-                 inner_rtol=1e-3, inner_maxiter=400, max_refine=60, stop=_lib.STOP_SCIPY, device="cuda"):
+                 inner_rtol=1e-3, inner_maxiter=400, max_refine=60, stop=_lib.STOP_SCIPY, big_rows=0,
+                 device="cuda"):
         torch = _lib.require_cuda()
         self.nsys = len(patterns)
         self.n = np.array([len(ip) - 1 for ip, _ in patterns], dtype=np.int32)
@@ -45,6 +46,7 @@ class BatchSolver:
         o.mode = _lib.MODE_MIXED if mode == "mixed" else _lib.MODE_FP64
         o.maxiter, o.lanes, o.max_refine, o.inner_maxiter = int(maxiter), int(lanes), int(max_refine), int(inner_maxiter)
         o.rtol, o.atol, o.inner_rtol = float(rtol), float(atol), float(inner_rtol)
+        o.big_rows = int(big_rows)
         h = C.c_void_p()
         _lib.check(_lib.lib().kcfd_batch_create(self.nsys, self.n.ctypes.data, self.nnz.ctypes.data, ip.ctypes.data,
                                                 ix.ctypes.data, C.byref(o), C.byref(h)), "kcfd_batch_create")
@@ -97,27 +99,62 @@ def lpt_shards(weights, nranks):
     return [sorted(o) for o in out]
 
 
-def p_prime_batch(count, n_min=2000, n_max=200000, seed=0, device="cuda"):
+def _p_prime_host(k, n_k, seed):
+    """Host part of system k: Delaunay triangles of ~n_k/2 points, per-cell
+    diffusivity and right-hand side, all from its own generator (seed, k), so the
+    systems do not depend on how many processes make them. Each side of the square
+    carries sqrt(n_k/2) equally spaced points, so the Dirichlet side (x = 0) is a
+    chain of faces of the local mesh size rather than one edge under a sliver."""
+    from .meshgen import delaunay_tri_arrays
+    rng = np.random.default_rng((seed, k))
+    npts = max(int(n_k) // 2, 4)
+    pts, cells, bd = delaunay_tri_arrays(npts, rng, side_points=int(np.ceil(np.sqrt(npts))))
+    n_cells = len(cells)
+    gamma = np.exp(rng.uniform(np.log(0.1), np.log(10.0), n_cells))
+    rhs = rng.normal(size=n_cells)
+    return pts, cells, bd, gamma, rhs
+
+
+def p_prime_sizes(count, n_min=2000, n_max=200000, seed=0):
+    """Requested cell counts, log-uniform in [n_min, n_max]."""
+    rng = np.random.default_rng(seed)
+    return np.round(np.exp(rng.uniform(np.log(n_min), np.log(n_max), count))).astype(np.int64)
+
+
+def p_prime_host(count, n_min=2000, n_max=200000, seed=0, workers=0):
+    """Host inputs of the batch (list of (pts, cells, bd, gamma, rhs)); workers > 0
+    makes them in a pool of spawned processes (Delaunay dominates: ~16 us a point)."""
+    sizes = p_prime_sizes(count, n_min, n_max, seed)
+    if workers and workers > 1 and count > 1:
+        import multiprocessing as mp
+        from concurrent.futures import ProcessPoolExecutor
+        with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
+            return list(ex.map(_p_prime_host, range(count), sizes, [seed] * count, chunksize=4)), sizes
+    return [_p_prime_host(k, sizes[k], seed) for k in range(count)], sizes
+
+
+def p_prime_batch(count, n_min=2000, n_max=200000, seed=0, device="cuda", workers=0, host=None):
     """Pressure-correction systems on Delaunay triangle meshes, assembled on the device.
 
     Returns (patterns, vals_list [device], rhs_list [host], sizes). Cell counts are
     log-uniform in [n_min, n_max]; each mesh triangulates ~n/2 uniform points plus the
-    unit square's corners; the 'dirichlet' hull segment (x = 0) has p' = 0, the other
-    hull edges are zero-gradient.
+    unit square's corners and sqrt(n/2) points on each side; the 'dirichlet' side
+    (x = 0) has p' = 0, the other hull edges are zero-gradient. The diffusivity is log-uniform in [0.1, 10] per
+    cell, the right-hand side N(0, 1). `host` takes the output of p_prime_host.
     """
     torch = _lib.require_cuda()
     from .assembly import DeviceSystem, boundary_arrays
     from .device_mesh import DeviceMesh
     from .mesh import build_mesh
-    from .meshgen import delaunay_tri_arrays
-    rng = np.random.default_rng(seed)
-    sizes = np.round(np.exp(rng.uniform(np.log(n_min), np.log(n_max), count))).astype(np.int64)
+    if host is None:
+        host, sizes = p_prime_host(count, n_min, n_max, seed, workers)
+    else:
+        sizes = p_prime_sizes(count, n_min, n_max, seed)
     patterns, vals, rhs = [], [], []
-    for k in range(count):
-        pts, cells, bd = delaunay_tri_arrays(max(int(sizes[k]) // 2, 4), rng)
+    for pts, cells, bd, gamma_h, rhs_h in host:
         m = build_mesh(pts, cells, bd)
         dm = DeviceMesh(m, device)
-        gamma = torch.from_numpy(np.exp(rng.uniform(np.log(0.1), np.log(10.0), m.n_cells))).to(device)
+        gamma = torch.from_numpy(gamma_h).to(device)
         s = DeviceSystem(dm)
         s.diffusion_operator(gamma)
         mf = torch.zeros(m.n_faces, dtype=torch.float64, device=device)
@@ -125,5 +162,5 @@ def p_prime_batch(count, n_min=2000, n_max=200000, seed=0, device="cuda"):
         s.apply_boundary_conditions(bt, bv, bg, gamma, mf)
         patterns.append((m.indptr, m.indices))
         vals.append(s.vals)
-        rhs.append(rng.normal(size=m.n_cells))
+        rhs.append(rhs_h)
     return patterns, vals, rhs, sizes

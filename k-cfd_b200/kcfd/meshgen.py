@@ -125,15 +125,23 @@ def _morton_order(pts):
     return np.argsort(code, kind="stable")
 
 
-def delaunay_tri_arrays(n_points, rng, dirichlet_name="dirichlet", wall_name="wall"):
+def delaunay_tri_arrays(n_points, rng, dirichlet_name="dirichlet", wall_name="wall", side_points=0):
     """Delaunay triangles of n_points uniform points in the unit square plus its corners.
 
     Cells are ordered along a Morton curve of their centroids. Boundary edges are
     the convex hull; hull edges whose midpoint has x < 1e-9 form the Dirichlet
-    segment, the rest the wall patch.
+    segment, the rest the wall patch. With corners alone the hull is the square's
+    four sides, each one long edge under a sliver triangle; side_points > 0 puts that
+    many equally spaced points inside each side, so every side is a chain of
+    side_points + 1 edges.
     """
     from scipy.spatial import Delaunay
-    pts = np.vstack([rng.uniform(0.0, 1.0, (n_points, 2)), [[0, 0], [1, 0], [1, 1], [0, 1]]])
+    extra = np.zeros((0, 2))
+    if side_points > 0:
+        t = np.arange(1, side_points + 1) / (side_points + 1.0)
+        z, o = np.zeros_like(t), np.ones_like(t)
+        extra = np.vstack([np.stack([t, z], 1), np.stack([o, t], 1), np.stack([t, o], 1), np.stack([z, t], 1)])
+    pts = np.vstack([rng.uniform(0.0, 1.0, (n_points, 2)), [[0, 0], [1, 0], [1, 1], [0, 1]], extra])
     tri = Delaunay(pts)
     cells = tri.simplices.astype(np.int64)
     order = _morton_order(pts[cells].mean(axis=1))

@@ -8,12 +8,15 @@ imbalance the pressure-correction equation removes.
 
 Continuous batching: requests are admitted while free slots and the HBM budget allow
 (footprint estimated from the mesh size), every admitted case keeps its mesh,
-matrices and fields resident and gets its own CUDA stream and CUDA graph of one outer
-iteration, and the scheduler enqueues `iters_per_tick` iterations per case and polls
-events without blocking. Cases that arrive while others are on the GPU join as soon as
-a slot and memory free up; their kernels overlap on the device. A case's result does
-not depend on what runs beside it (its solves reduce in a fixed order on its own
-buffers), so it is the same alone and in the mix.
+matrices and fields resident and gets its own CUDA stream (and, for cases small
+enough for the single-CTA solver, a CUDA graph of one outer iteration), and the
+scheduler enqueues `iters_per_tick` iterations per case and polls events without
+blocking. Cases are built (host mesh, device set-up) on a worker thread, so the host
+work of the next case overlaps the GPU work of the running ones. Admission takes
+the queued request with the least estimated work first (policy "sjf", cells x a
+dimension factor) or in arrival order ("fifo"). A case's result does not depend on
+what runs beside it (its solves reduce in a fixed order on its own buffers), so it is
+the same alone and in the mix.
 """
 from __future__ import annotations
 
@@ -132,9 +135,15 @@ class Case:
         return {"U": self.solver.U.values, "p": self.solver.p.values}
 
 
+def work_estimate(req):
+    """Relative work of a request for shortest-job-first admission."""
+    return req.N ** req.ndim * (1.5 if req.ndim == 3 else 1.0)
+
+
 class Server:
     def __init__(self, budget_bytes=150e9, max_active=64, iters_per_tick=10, max_iters=3000, cont_tol=1e-6,
-                 precision="mixed", graph=True, precond_p="ilu0", keep_fields=False, verbose=False):
+                 precision="mixed", graph=True, precond_p="ilu0", keep_fields=False, verbose=False,
+                 policy="fifo", builders=1):
         self.budget = budget_bytes
         self.max_active = max_active
         self.k = iters_per_tick
@@ -143,60 +152,85 @@ class Server:
         self.precision, self.graph, self.precond_p = precision, graph, precond_p
         self.keep_fields = keep_fields
         self.verbose = verbose
+        if policy not in ("fifo", "sjf"):
+            raise ValueError(f"unknown admission policy {policy!r}")
+        self.policy = policy
+        self.builders = max(1, int(builders))
 
     def run(self, requests, serial=False):
         """Serve `requests` in real time (arrival times honoured). serial=True runs one
         case at a time (the serial comparator). Returns a list of Result."""
         torch = _lib.require_cuda()
+        from concurrent.futures import ThreadPoolExecutor
         reqs = sorted(requests, key=lambda r: r.arrival)
         pending = list(reqs)
-        queue, active, results = [], [], []
+        queue, building, active, results = [], [], [], []
         used = 0
         max_active = 1 if serial else self.max_active
+        dev = torch.cuda.current_device()
+
+        def build(r):
+            torch.cuda.set_device(dev)
+            return Case(r, self.precision, self.graph, self.precond_p)
+
         t0 = time.perf_counter()
-        while pending or queue or active:
-            now = time.perf_counter() - t0
-            while pending and pending[0].arrival <= now:
-                queue.append(pending.pop(0))
-            progressed = False
-            # admission: FIFO while a slot and the HBM budget allow
-            while queue and len(active) < max_active:
-                fp = footprint_bytes(queue[0].ndim, queue[0].N, self.precision)
-                if active and used + fp > self.budget:
-                    break
-                r = queue.pop(0)
-                c = Case(r, self.precision, self.graph, self.precond_p)
-                c.admitted = time.perf_counter() - t0
-                c.fp = fp
-                used += fp
-                c.launch(self.k)
-                active.append(c)
-                progressed = True
-            # progress: poll without blocking; finished cases leave, others continue
-            still = []
-            for c in active:
-                if not c.ready():
-                    still.append(c)
-                    continue
-                progressed = True
-                cont = c.continuity()
-                if cont < self.cont_tol or c.done_iters >= self.max_iters:
-                    fin = time.perf_counter() - t0
-                    res = Result(c.req.rid, c.req.ndim, c.req.N, c.cells, c.req.arrival, c.admitted, fin,
-                                 c.done_iters, cont < self.cont_tol, cont,
-                                 c.fields() if self.keep_fields else {})
-                    results.append(res)
-                    used -= c.fp
-                    if self.verbose:
-                        print(f"  done rid={res.rid} {res.ndim}D N={res.N} iters={res.iterations} "
-                              f"latency={res.latency:.3f}s cont={cont:.2e}", flush=True)
-                    del c
-                else:
+        with ThreadPoolExecutor(max_workers=self.builders) as pool:
+            while pending or queue or building or active:
+                now = time.perf_counter() - t0
+                while pending and pending[0].arrival <= now:
+                    queue.append(pending.pop(0))
+                progressed = False
+                # admission: while a slot and the HBM budget allow; the case is built
+                # on a worker thread
+                while queue and len(active) + len(building) < max_active:
+                    pick = 0
+                    if self.policy == "sjf":
+                        pick = min(range(len(queue)), key=lambda i: work_estimate(queue[i]))
+                    r = queue[pick]
+                    fp = footprint_bytes(r.ndim, r.N, self.precision)
+                    if (active or building) and used + fp > self.budget:
+                        break
+                    queue.pop(pick)
+                    used += fp
+                    building.append((r, fp, time.perf_counter() - t0, pool.submit(build, r)))
+                    progressed = True
+                # built cases start their first tick
+                still_b = []
+                for r, fp, adm, fut in building:
+                    if not fut.done():
+                        still_b.append((r, fp, adm, fut))
+                        continue
+                    c = fut.result()
+                    c.admitted, c.fp = adm, fp
                     c.launch(self.k)
-                    still.append(c)
-            active = still
-            if not progressed:
-                time.sleep(0.0002)
+                    active.append(c)
+                    progressed = True
+                building = still_b
+                # progress: poll without blocking; finished cases leave, others continue
+                still = []
+                for c in active:
+                    if not c.ready():
+                        still.append(c)
+                        continue
+                    progressed = True
+                    cont = c.continuity()
+                    if cont < self.cont_tol or c.done_iters >= self.max_iters:
+                        fin = time.perf_counter() - t0
+                        res = Result(c.req.rid, c.req.ndim, c.req.N, c.cells, c.req.arrival, c.admitted, fin,
+                                     c.done_iters, cont < self.cont_tol, cont,
+                                     c.fields() if self.keep_fields else {})
+                        results.append(res)
+                        used -= c.fp
+                        if self.verbose:
+                            print(f"  done rid={res.rid} {res.ndim}D N={res.N} iters={res.iterations} "
+                                  f"latency={res.latency:.3f}s cont={cont:.2e}", flush=True)
+                        del c
+                    else:
+                        c.launch(self.k)
+                        still.append(c)
+                active = still
+                if not progressed:
+                    time.sleep(0.0002)
         torch.cuda.synchronize()
         return results
 

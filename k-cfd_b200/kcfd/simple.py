@@ -173,7 +173,9 @@ class SIMPLESolver:
                     self._step()      # warm-up outside capture (loads kernels, no allocations)
                 torch.cuda.current_stream().wait_stream(s)
                 g = torch.cuda.CUDAGraph()
-                with torch.cuda.graph(g):
+                # thread-local capture: other host threads (a server building the next
+                # case) may allocate and copy meanwhile
+                with torch.cuda.graph(g, capture_error_mode="thread_local"):
                     self._step()
                 self._graph = g
                 n -= 1

@@ -278,6 +278,63 @@ def make_simple(out):
     np.savez_compressed(os.path.join(out, "simple.npz"), **d)
 
 
+def two_fluid_setup(sv, mesh, seed):
+    """Shared set-up of the two-fluid fixtures (also restated by the oracle and the
+    device tests): inlet / outlet / heated bottom wall / adiabatic walls, seeded
+    alpha_g in [0.02, 0.08], T_l in [370, 376] K, T_g in [371.15, 375.15] K (both
+    sides of T_sat, so evaporation and condensation are active), 6-equation energy."""
+    ndim = mesh.ndim
+    rng = np.random.default_rng(seed)
+    n = mesh.n_cells
+    sv.d_b = 0.003
+    sv.solve_energy = True
+    sv.max_outer_iter = 4
+    sv.tol = 1e-12
+    sv.dt = 1e-3
+    sv.initialize(0.05)
+    ul = [0.1] + [0.0] * (ndim - 1)
+    ug = [0.2] + [0.0] * (ndim - 1)
+    sv.set_inlet_bc("inlet", 0.05, U_l=ul, U_g=ug, T_l=372.0, T_g=373.0)
+    sv.set_outlet_bc("outlet", 0.0)
+    for nm in mesh.boundary_patches:
+        if nm.startswith("wall"):
+            sv.set_wall_bc(nm, q_wall=2.0e4 if nm == "wall_bottom" else None)
+    ag = rng.uniform(0.02, 0.08, n)
+    sv.alpha_g.values = ag.copy()
+    sv.alpha_l.values = 1.0 - ag
+    sv.T_l.values = 370.0 + rng.uniform(0.0, 6.0, n)
+    sv.T_g.values = 373.15 + rng.uniform(-2.0, 2.0, n)
+    sv.U_l.values = np.tile(np.array(ul), (n, 1)) * rng.uniform(0.5, 1.5, (n, 1))
+    sv.U_g.values = np.tile(np.array(ug), (n, 1)) * rng.uniform(0.5, 1.5, (n, 1))
+
+
+def make_two_fluid(out, meshes):
+    """TwoFluidSolver (models/two_fluid.py) on the quad channel and the hybrid
+    hex/tet meshes: 3 time steps of dt = 1e-3 with 4 SIMPLE inner iterations each and
+    the 6-equation energy model; fields after every step."""
+    from models.two_fluid import TwoFluidSolver
+    import contextlib
+    import io
+    d = {}
+    for tag, seed in (("quad", 11), ("hybrid", 12)):
+        m = meshes[tag]
+        sv = TwoFluidSolver(m)
+        two_fluid_setup(sv, m, seed)
+        d[tag + "_init_alpha_g"] = sv.alpha_g.values.copy()
+        d[tag + "_init_T_l"] = sv.T_l.values.copy()
+        d[tag + "_init_T_g"] = sv.T_g.values.copy()
+        d[tag + "_init_U_l"] = sv.U_l.values.copy()
+        d[tag + "_init_U_g"] = sv.U_g.values.copy()
+        for step in range(3):
+            with contextlib.redirect_stdout(io.StringIO()):
+                r = sv.solve_transient(sv.dt, sv.dt)
+            assert r["time_steps"] == 1
+            for f in ("alpha_g", "U_l", "U_g", "p", "T_l", "T_g"):
+                d[f"{tag}_{step}_{f}"] = getattr(sv, f).values.copy()
+            d[f"{tag}_{step}_res"] = np.array(r["residuals"])
+    np.savez_compressed(os.path.join(out, "two_fluid.npz"), **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -289,6 +346,7 @@ def main():
     make_operators(a.out, meshes)
     make_solvers(a.out)
     make_simple(a.out)
+    make_two_fluid(a.out, meshes)
     print("golden fixtures written to", a.out)
 
 

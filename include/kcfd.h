@@ -347,6 +347,86 @@ int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream);
  * ILU(0) levels (1 without ILU). No reference counterpart (diagnostics).         */
 int kcfd_solver_info(const kcfd_solver* s, int32_t* info4);
 
+/* ------------------------------------------------ two-fluid system set ----- */
+/* The pieces of the Euler-Euler model (models/two_fluid.py, models/closure.py) that
+ * are not generic FVM operators, for the device TwoFluidSolver. Cell arrays [n],
+ * vectors [n][ndim]; face arrays in device face order; boundary arrays per boundary
+ * face (device order), nc right-hand sides interleaved [n][nc]. Each call ADDS into
+ * the system like the reference's FVMSystem; face terms run one launch per colour. */
+typedef struct {
+    double rho_l, rho_g, mu_l, mu_g, cp_l, cp_g, k_l, k_g, d_b;
+    double g[3];                                 /* gravity (last axis -9.81)   */
+    double h_i_coeff, a_i_coeff, T_sat, h_fg, r_phase_change;
+    double dt;
+} kcfd_tf_params_t;
+
+/* K_drag (drag_coefficient_implicit, models/closure.py:72-92; Schiller-Naumann :13-34) */
+int kcfd_tf_drag(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, const double* alpha_g, const double* U_g,
+                 const double* U_l, double* K, void* stream);
+/* h_i a_i V (Ranz-Marshall, models/two_fluid.py:395-410) */
+int kcfd_tf_interfacial(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, const double* alpha_g, const double* U_g,
+                        const double* U_l, double* hiaiV, void* stream);
+/* Lee evaporation / condensation rate dot_m (models/two_fluid.py:334-360) */
+int kcfd_tf_phase_change(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, const double* alpha_l,
+                         const double* alpha_g, const double* T_l, const double* T_g, double* dot_m, void* stream);
+/* gamma = alpha coef (kind 0), or alpha mu_l + alpha mu_BIT with Sato's bubble-induced
+ * viscosity (kind 1; models/two_fluid.py:551-561, models/closure.py:146-164)      */
+int kcfd_tf_gamma(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, int32_t kind, const double* alpha, double coef,
+                  const double* alpha_g, const double* U_g, const double* U_l, double* gamma, void* stream);
+/* face flux weighting: kind 0 mf alpha[owner] (models/two_fluid.py:566-568); kind 1
+ * mf alpha_upwind cp (models/two_fluid.py:433-444)                                */
+int kcfd_tf_face_flux(const kcfd_dmesh_t* m, int32_t kind, const double* mf, const double* alpha, double cp,
+                      double* out, void* stream);
+/* compute_mass_flux with per-boundary-face values U_b (core/interpolation.py:163-182) */
+int kcfd_tf_mass_flux(const kcfd_dmesh_t* m, double rho, const double* U, const double* U_b, double* mf,
+                      void* stream);
+/* boundary values of masked (zero_gradient) faces := owner values
+ * (_update_zero_gradient_boundaries, models/two_fluid.py:224-250)                 */
+int kcfd_tf_zero_gradient(const kcfd_dmesh_t* m, const int8_t* mask, const double* field, int32_t nc, double* bval,
+                          void* stream);
+/* phase momentum terms for components comp0..comp0+nc-1 (models/two_fluid.py:570-598):
+ * temporal (U_old may be NULL), pressure force -alpha grad p per face, implicit drag,
+ * gravity                                                                           */
+int kcfd_tf_momentum_sources(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, int32_t comp0, int32_t nc, double rho,
+                             const double* alpha, const double* p, const double* K, const double* U_other,
+                             const double* U_old, double* vals, double* diag, double* rhs, void* stream);
+/* apply_boundary_conditions (core/fvm_operators.py:178-225) for nc rhs sharing one matrix */
+int kcfd_tf_boundary(const kcfd_dmesh_t* m, const int8_t* btype, const double* bval, const double* bgrad, int32_t nc,
+                     const double* gamma, const double* mf, double* vals, double* diag, double* rhs, void* stream);
+/* diagonal floor (diag < 1e-20 -> 1e-10, if floor_diag) then under_relax for nc rhs */
+int kcfd_tf_relax(const kcfd_dmesh_t* m, double alpha, const double* phi, int32_t nc, int32_t floor_diag, double* vals,
+                  double* diag, double* rhs, void* stream);
+/* aP = max(diag, 1e-20) (first) or max(aP, max(diag, 1e-20)) (models/two_fluid.py:620-633) */
+int kcfd_tf_update_ap(const kcfd_dmesh_t* m, const double* diag, double* aP, int32_t first, void* stream);
+/* two-phase p' system with the row-0 pin diag += 1e10 (models/two_fluid.py:641-689) */
+int kcfd_tf_pressure_assemble(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, const double* alpha_l,
+                              const double* alpha_g, const double* aP_l, const double* aP_g, const double* mf_l,
+                              const double* mf_g, double* vals, double* diag, double* rhs, void* stream);
+/* p += alpha_p p'; face-difference gradient of p'; U_k += alpha_p (-alpha_k V / aP_k) grad p'
+ * (models/two_fluid.py:697-723); grad: [n][ndim] scratch                           */
+int kcfd_tf_correct(const kcfd_dmesh_t* m, double alpha_p, const double* pp, const double* alpha_l,
+                    const double* alpha_g, const double* aP_l, const double* aP_g, double* grad, double* U_l,
+                    double* U_g, double* p, void* stream);
+/* volume-fraction source dot_m / rho_g V where |dot_m| > 1e-30 (models/two_fluid.py:753-758) */
+int kcfd_tf_alpha_source(const kcfd_dmesh_t* m, double rho_g, const double* dot_m, double* rhs, void* stream);
+/* phase energy terms (models/two_fluid.py:446-496): temporal (T_old may be NULL),
+ * interfacial exchange, latent heat of dm_sign * dot_m, wall heat flux q_b on the
+ * boundary faces with qmask set, weighted by alpha_wall[owner]                      */
+int kcfd_tf_energy_sources(const kcfd_dmesh_t* m, const kcfd_tf_params_t* P, double rho, double cp,
+                           const double* alpha, const double* T_old, const double* T_other, const double* hiaiV,
+                           const double* dot_m, double dm_sign, const int8_t* qmask, const double* q_b,
+                           const double* alpha_wall, double* vals, double* diag, double* rhs, void* stream);
+/* post-solve guards: mode 0 restore old if any NaN; 1 restore old if any NaN/inf,
+ * else clip to [lo, hi]; 2 zero if any NaN. flag: one device int of scratch.       */
+int kcfd_tf_guard(int64_t count, double* x, const double* old, int32_t mode, double lo, double hi, int32_t* flag,
+                  void* stream);
+/* alpha_g clipped to [0, 1], alpha_l = 1 - alpha_g, maxdiff = max |alpha_g - alpha_old| */
+int kcfd_tf_alpha_finish(int32_t n, double* alpha_g, double* alpha_l, const double* alpha_old, double* maxdiff,
+                         void* stream);
+/* dst[i*dst_stride + dst_off + c] = src[i*src_stride + src_off + c], c < ncopy      */
+int kcfd_tf_copy(int32_t n, int32_t ncopy, const double* src, int32_t src_stride, int32_t src_off, double* dst,
+                 int32_t dst_stride, int32_t dst_off, void* stream);
+
 /* ------------------------------------------- allocation-free solve ---------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc --
  * code running during CUDA graph capture, real-time loops that must not block on

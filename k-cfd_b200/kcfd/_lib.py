@@ -44,6 +44,12 @@ class SolverOpts(C.Structure):
                 ("max_refine", i32), ("inner_maxiter", i32)]
 
 
+class TfParams(C.Structure):
+    """kcfd_tf_params_t: two-fluid properties and model constants."""
+    _fields_ = [(n, f64) for n in ("rho_l", "rho_g", "mu_l", "mu_g", "cp_l", "cp_g", "k_l", "k_g", "d_b")] + \
+        [("g", f64 * 3)] + [(n, f64) for n in ("h_i_coeff", "a_i_coeff", "T_sat", "h_fg", "r_phase_change", "dt")]
+
+
 # name -> (restype, argtypes)
 SIGNATURES = {
     "kcfd_version": (i32, []),
@@ -62,6 +68,24 @@ SIGNATURES = {
     "kcfd_solver_solve": (i32, [vp, C.POINTER(Csr), vp, vp, vp, vp, vp, vp]),
     "kcfd_solver_error": (i32, [vp, P_i32, vp]),
     "kcfd_solver_info": (i32, [vp, P_i32]),
+    "kcfd_tf_drag": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_interfacial": (i32, [vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_phase_change": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_gamma": (i32, [vp, vp, i32, vp, f64, vp, vp, vp, vp, vp]),
+    "kcfd_tf_face_flux": (i32, [vp, i32, vp, vp, f64, vp, vp]),
+    "kcfd_tf_mass_flux": (i32, [vp, f64, vp, vp, vp, vp]),
+    "kcfd_tf_zero_gradient": (i32, [vp, vp, vp, i32, vp, vp]),
+    "kcfd_tf_momentum_sources": (i32, [vp, vp, i32, i32, f64, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_boundary": (i32, [vp, vp, vp, vp, i32, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_relax": (i32, [vp, f64, vp, i32, i32, vp, vp, vp, vp]),
+    "kcfd_tf_update_ap": (i32, [vp, vp, vp, i32, vp]),
+    "kcfd_tf_pressure_assemble": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_correct": (i32, [vp, f64, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_alpha_source": (i32, [vp, f64, vp, vp, vp]),
+    "kcfd_tf_energy_sources": (i32, [vp, vp, f64, f64, vp, vp, vp, vp, vp, f64, vp, vp, vp, vp, vp, vp, vp]),
+    "kcfd_tf_guard": (i32, [i64, vp, vp, i32, f64, f64, vp, vp]),
+    "kcfd_tf_alpha_finish": (i32, [i32, vp, vp, vp, vp, vp]),
+    "kcfd_tf_copy": (i32, [i32, i32, vp, i32, i32, vp, i32, i32, vp]),
     "kcfd_mass_flux": (i32, [vp, vp, vp, f64, vp, vp]),
     "kcfd_momentum_assemble": (i32, [vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_pressure_assemble": (i32, [vp, vp, f64, vp, vp, vp, vp, vp, vp, vp]),

@@ -198,6 +198,18 @@ __global__ void g_fill(int64_t m, const int* __restrict__ src, const double* __r
     }
 }
 
+// y = A M^-1 q on the rows of ILU level 0 is q itself: level-0 rows have no lower
+// entries, so their factor rows are A's rows (u_ij = a_ij, u_ii = a_ii), and the
+// backward sweep sets z_i = (q_i - sum_j a_ij z_j) / a_ii, so that
+// a_ii z_i + sum_j a_ij z_j = q_i whatever the other levels hold. The SpMV kernels
+// therefore copy q there and multiply only the rows of the later levels (read from
+// the first slice boundary at or below the level-1 start, so warps stay on slices).
+// Returns the first row the SpMV loop must treat (0 without the identity).
+template <int PREC>
+__device__ __forceinline__ int level0_rows(const Args& a) {
+    return (PREC == KCFD_PREC_ILU0 && a.nlev >= 2) ? a.lev[1] : 0;
+}
+
 template <int NRHS>
 __global__ void __launch_bounds__(kBlock) g_init(Args a) {
     St& S = *a.st;
@@ -376,7 +388,15 @@ __global__ void __launch_bounds__(kBlock) g_spmv_v(Args a) {
     double red[NRHS];
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) red[c] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+    const int n0 = level0_rows<PREC>(a);
+    const int stride = gridDim.x * blockDim.x;
+    for (int q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < n0 * NRHS; q0 += stride) {
+        const double vv = a.p[q0];
+        a.v[q0] = vv;
+        red[q0 % NRHS] += a.rh[q0] * vv;
+    }
+    for (int i = (n0 & ~31) + blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
+        if (i < n0) continue;
         int base, w;
         sell_row(a.A, i, base, w);
         double rhv[NRHS], acc[NRHS];
@@ -504,13 +524,27 @@ __global__ void __launch_bounds__(kBlock) g_spmv_t(Args a) {
     double red[2 * NRHS];
 #pragma unroll
     for (int k = 0; k < 2 * NRHS; ++k) red[k] = 0.0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
-        if (any_sc) {
+    const int stride = gridDim.x * blockDim.x;
+    if (any_sc) {
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
 #pragma unroll
             for (int c = 0; c < NRHS; ++c)
                 if (sc[c]) a.x[(size_t)i * NRHS + c] += al[c] * ph[(size_t)i * NRHS + c];
         }
-        if (!active) continue;
+    }
+    const int n0 = active ? level0_rows<PREC>(a) : 0;
+    if (active) {
+        for (int q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < n0 * NRHS; q0 += stride) {
+            const int c = q0 % NRHS;
+            if (dn[c]) continue;
+            const double tv = a.r[q0];  // t = s on level 0
+            a.t[q0] = tv;
+            red[c] += tv * tv;
+            red[NRHS + c] += tv * tv;
+        }
+    }
+    for (int i = (n0 & ~31) + blockIdx.x * blockDim.x + threadIdx.x; active && i < a.n; i += stride) {
+        if (i < n0) continue;
         int base, w;
         sell_row(a.A, i, base, w);
         double sv[NRHS], acc[NRHS];

@@ -122,6 +122,13 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the nine phase kernels
+# of one p' Krylov iteration on the 128^3 cavity, from one ncu capture of the graph
+# engine (profiles/graph_engine_p_solve_cavity128.md); the roofline's traffic is this
+# times the solve's Krylov count (the kernels and their sizes repeat every iteration).
+NCU_P_ITER_DRAM_BYTES_128 = 890082048
+
+
 def solver_bytes(n, nnz, iters, precond, w, nrhs=1):
     """Algorithmic bytes of BiCGSTAB iterations (each array counted once per use):
     SpMV nnz(w+4) + 4(n+1) + 2 n w nrhs; ILU(0) apply nnz(w+4) + 8(n+1) + 4 n w;
@@ -225,7 +232,11 @@ def p_solve_roofline(s, peak, reps=3):
     return {"bound": "hbm", "kernel": kern, "unit_of_work": "one p' solve (Krylov iterations x bytes/iteration)",
             "achieved": round(ach, 1), "peak": peak[0], "unit": "GB/s", "frac": round(ach / peak[0], 3),
             "moved": moved,
-            "peak_source": peak[1], "traffic": None, "launch_ms": round(t * 1e3, 3),
+            "peak_source": peak[1],
+            "traffic": (int(NCU_P_ITER_DRAM_BYTES_128 * int(s.s_p.iters[0]))
+                        if (n == 128 ** 3 and info["team"] == 3) else None),
+            "traffic_source": "ncu capture of one Krylov iteration (9 kernels) x Krylov count" if n == 128 ** 3
+            else None, "launch_ms": round(t * 1e3, 3),
             "krylov_iters": int(s.s_p.iters[0]), "bytes_per_krylov_iter": int(solver_bytes(n, nnz, 1, "ilu0", w)),
             "spmv": spmv}
 

@@ -96,19 +96,15 @@ __device__ __forceinline__ bool last_block_sum(const Args& a, int slot, double (
     __syncthreads();
     if (!is_last) return false;
     __threadfence();
-    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
-    if (w == 0) {
+    // every thread of the last block sums a strided share of the partials, then the
+    // block tree combines them: a fixed order for a given grid
 #pragma unroll
-        for (int k = 0; k < K; ++k) {
-            double tsum = 0.0;
-            for (int j = lane; j < (int)gridDim.x; j += 32) tsum += __ldcg(part + (size_t)k * a.gmax + j);
-            tsum = warp_sum(tsum);
-            if (lane == 0) sm[k * 32] = tsum;
-        }
+    for (int k = 0; k < K; ++k) {
+        double tsum = 0.0;
+        for (int j = threadIdx.x; j < (int)gridDim.x; j += blockDim.x) tsum += __ldcg(part + (size_t)k * a.gmax + j);
+        v[k] = tsum;
     }
-    __syncthreads();
-#pragma unroll
-    for (int k = 0; k < K; ++k) v[k] = sm[k * 32];
+    block_sum<K>(v, sm);
     if (threadIdx.x == 0) a.cnt[slot] = 0u;  // ready for the next use
     return true;
 }

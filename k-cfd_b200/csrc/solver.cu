@@ -666,13 +666,16 @@ __device__ void solve_fp64(Team& tm, const SolveArgs& a, double* smem) {
 template <int NRHS>
 struct MState {
     double thr[NRHS], rn[NRHS], bn[NRHS], rn_prev[NRHS];
-    int done[NRHS], applied[NRHS], revert[NRHS];
+    int done[NRHS], applied[NRHS], revert[NRHS], capped[NRHS];
     int left, stop_now, total_it, cap, grow, retry;
     double inner_atol;
 };
 
-// A refinement step that does not lower the FP64 residual is undone and retried from
-// the same iterate with twice the inner iteration cap, up to this many doublings.
+// A refinement step that does not lower the FP64 residual is undone. If its inner run
+// stopped at the iteration cap (not at the inner tolerance), it is retried from the
+// same iterate with twice the cap, up to this many doublings; an inner run that met
+// its tolerance and still did not help means FP32 cannot resolve the system, and the
+// right-hand side stops with BREAKDOWN.
 constexpr int kMaxGrow = 5;
 
 // MIXED solve: FP64 outer refinement around capped FP32 inner BiCGSTAB runs.
@@ -693,6 +696,7 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
     if (t0) {
         for (int c = 0; c < NRHS; ++c) {
             ms.applied[c] = 0;
+            ms.capped[c] = 0;
             ms.done[c] = 0;
             ms.rn_prev[c] = INFINITY;
             ms.thr[c] = 0.0;
@@ -739,7 +743,7 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
                     // then retry with a larger inner cap, or give up
                     ms.revert[c] = 1;
                     ms.rn[c] = ms.rn_prev[c];
-                    if (ms.grow < kMaxGrow && ms.total_it < a.maxiter) {
+                    if (ms.capped[c] && ms.grow < kMaxGrow && ms.total_it < a.maxiter) {
                         ms.retry = 1;
                     } else {
                         ms.done[c] = 1;
@@ -809,6 +813,7 @@ __device__ void solve_mixed(Team& tm, const SolveArgs& a, double* smem) {
                 } else {
                     ms.applied[c] = 1;
                     ms.rn_prev[c] = ms.rn[c];
+                    ms.capped[c] = st.status[c] == KCFD_MAXITER;
                 }
             }
             ms.total_it += max(max_it, 1);

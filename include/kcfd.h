@@ -224,6 +224,9 @@ typedef struct {
     const int32_t* face_ref;   /* [F]  reference face id */
     const int32_t* color_ptr;  /* HOST [n_colors_int + n_colors_bnd + 1] face ranges */
     int32_t n_colors_int, n_colors_bnd;
+    const int32_t* cf_ptr;     /* [n+1] faces of each cell (NULL: not provided)   */
+    const int32_t* cf_face;    /* device faces of the cells, each cell's in ascending
+                                  reference face id (the reference's summation order) */
 } kcfd_dmesh_t;
 
 /* Boundary conditions per boundary face (index = device face - n_internal).

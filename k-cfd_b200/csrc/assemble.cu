@@ -44,6 +44,8 @@ struct DM {
     const int* __restrict__ slot_no;
     const int* __restrict__ diag_slot;
     const int* __restrict__ indptr;
+    const int* __restrict__ cf_ptr;
+    const int* __restrict__ cf_face;
 };
 
 static DM to_dm(const kcfd_dmesh_t* m) {
@@ -52,6 +54,7 @@ static DM to_dm(const kcfd_dmesh_t* m) {
     d.owner = m->owner; d.neigh = m->neigh; d.area = m->area; d.normal = m->normal; d.fcenter = m->fcenter;
     d.cc = m->ccenter; d.vol = m->volume; d.gc = m->gc; d.dlen = m->dlen; d.dorth = m->dorth;
     d.slot_on = m->slot_on; d.slot_no = m->slot_no; d.diag_slot = m->diag_slot; d.indptr = m->indptr;
+    d.cf_ptr = m->cf_ptr; d.cf_face = m->cf_face;
     return d;
 }
 
@@ -325,11 +328,61 @@ __global__ void k_gg_bnd(DM m, int f0, int f1, const double* __restrict__ phi, c
     }
 }
 
+// 1/V per gradient entry, flat over [n][KD] so that loads and stores coalesce.
 __global__ void k_gg_cells(int n, int KD, const double* __restrict__ vol, double* __restrict__ g) {
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double v = vol[i];
-        if (v > 1e-30)
-            for (int q = 0; q < KD; ++q) g[i * KD + q] = g[i * KD + q] / v;
+    const int64_t m = (int64_t)n * KD;
+    for (int64_t j = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; j < m; j += (int64_t)gridDim.x * blockDim.x) {
+        const double v = vol[j / KD];
+        if (v > 1e-30) g[j] = g[j] / v;
+    }
+}
+
+// Green-Gauss per cell: the cell sums the fluxes of its own faces in ascending
+// reference face id (the order in which core/gradient.py:12-48 accumulates them),
+// adding on the owner side and subtracting on the neighbour side, and writes its
+// gradient once, divided by the volume. No face colours, no read-modify-write.
+template <int D, int K>
+__global__ void k_gg_cell(DM m, const double* __restrict__ phi, const int8_t* __restrict__ bt,
+                          const double* __restrict__ bv, double* __restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+        double acc[K][D];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int d = 0; d < D; ++d) acc[k][d] = 0.0;
+        const int e1 = m.cf_ptr[i + 1];
+        for (int e = m.cf_ptr[i]; e < e1; ++e) {
+            const int f = m.cf_face[e];
+            const int o = m.owner[f];
+            const double A = m.area[f];
+            double pf[K];
+            bool own = true;
+            if (f < m.Fi) {
+                const int nb = m.neigh[f];
+                own = (o == i);
+                const double w = m.gc[f];
+#pragma unroll
+                for (int k = 0; k < K; ++k) pf[k] = w * phi[o * K + k] + (1.0 - w) * phi[nb * K + k];
+            } else {
+                const int bi = f - m.Fi;
+                const bool use = bt[bi] == 1;
+#pragma unroll
+                for (int k = 0; k < K; ++k) pf[k] = use ? bv[bi * K + k] : phi[o * K + k];
+            }
+#pragma unroll
+            for (int k = 0; k < K; ++k)
+#pragma unroll
+                for (int d = 0; d < D; ++d) {
+                    const double fl = pf[k] * m.normal[f * D + d] * A;
+                    if (own) acc[k][d] += fl;
+                    else acc[k][d] -= fl;
+                }
+        }
+        const double v = m.vol[i];
+#pragma unroll
+        for (int k = 0; k < K; ++k)
+#pragma unroll
+            for (int d = 0; d < D; ++d) g[(i * K + k) * D + d] = (v > 1e-30) ? acc[k][d] / v : acc[k][d];
     }
 }
 
@@ -549,6 +602,15 @@ int kcfd_gg_gradient(const kcfd_dmesh_t* m, int32_t ncomp, const double* phi, co
     KCFD_REQUIRE(ncomp == 1 || ncomp == m->ndim, "kcfd_gg_gradient: ncomp must be 1 or ndim");
     cudaStream_t st = (cudaStream_t)stream;
     DM d = to_dm(m);
+    if (d.cf_ptr && d.cf_face) {
+        const int nb = blocks_for(d.n);
+        if (d.D == 2 && ncomp == 1) k_gg_cell<2, 1><<<nb, kThreads, 0, st>>>(d, phi, btype, bval, grad);
+        else if (d.D == 2) k_gg_cell<2, 2><<<nb, kThreads, 0, st>>>(d, phi, btype, bval, grad);
+        else if (ncomp == 1) k_gg_cell<3, 1><<<nb, kThreads, 0, st>>>(d, phi, btype, bval, grad);
+        else k_gg_cell<3, 3><<<nb, kThreads, 0, st>>>(d, phi, btype, bval, grad);
+        KCFD_CUDA(cudaGetLastError());
+        return KCFD_OK;
+    }
     KCFD_CUDA(cudaMemsetAsync(grad, 0, sizeof(double) * d.n * ncomp * d.D, st));
 #define KC_GG(DD, KK)                                                                                   \
     for_colors(m, true, [&](int f0, int f1, int nb) { k_gg_int<DD, KK><<<nb, kThreads, 0, st>>>(d, f0, f1, phi, grad); }); \

@@ -25,7 +25,8 @@ class DMeshDesc(C.Structure):
                [(n, C.c_void_p) for n in ("owner", "neigh", "area", "normal", "fcenter", "ccenter", "volume", "gc",
                                           "dlen", "dorth", "slot_on", "slot_no", "diag_slot", "indptr", "face_ref",
                                           "color_ptr")] + \
-               [("n_colors_int", C.c_int32), ("n_colors_bnd", C.c_int32)]
+               [("n_colors_int", C.c_int32), ("n_colors_bnd", C.c_int32), ("cf_ptr", C.c_void_p),
+                ("cf_face", C.c_void_p)]
 
 
 class BCDesc(C.Structure):
@@ -86,6 +87,14 @@ class DeviceMesh:
             "diag_slot": dev(mesh.diag_slot, i32), "indptr": dev(mesh.indptr, i32),
             "indices": dev(mesh.indices, i32), "face_ref": dev(order, i32),
         }
+        # faces of each cell, ascending reference face id, as device face indices
+        dev_of_ref = np.empty(F, dtype=np.int64)
+        dev_of_ref[order] = np.arange(F)
+        cf = np.sort(np.where(mesh.cell_faces >= 0, mesh.cell_faces, np.iinfo(np.int64).max), axis=1)
+        valid = cf != np.iinfo(np.int64).max
+        cf_ptr = np.concatenate([[0], np.cumsum(valid.sum(axis=1))])
+        self.t["cf_ptr"] = dev(cf_ptr, i32)
+        self.t["cf_face"] = dev(dev_of_ref[cf[valid]], i32)
         self._color_ptr_np = np.ascontiguousarray(color_ptr, dtype=np.int32)
         d = DMeshDesc()
         d.ndim, d.n_cells, d.n_faces, d.n_internal = D, n, F, Fi
@@ -94,6 +103,7 @@ class DeviceMesh:
             setattr(d, k, self.t[k].data_ptr())
         d.color_ptr = self._color_ptr_np.ctypes.data
         d.n_colors_int, d.n_colors_bnd = nci, ncb
+        d.cf_ptr, d.cf_face = self.t["cf_ptr"].data_ptr(), self.t["cf_face"].data_ptr()
         self.desc = d
         self.nnz = mesh.nnz
         self.cell_color = mesh.cell_color

@@ -315,6 +315,10 @@ int kcfd_gg_gradient(const kcfd_dmesh_t* m, int32_t ncomp, const double* phi, co
 /* Reductions use a caller-provided scratch of KCFD_REDUCE_SCRATCH doubles.       */
 #define KCFD_REDUCE_SCRATCH 8192
 
+/* least_squares_gradient (core/gradient.py:51-99) of a scalar: phi [n], phi_b per
+ * boundary face (the patch values), grad [n][ndim]; needs the cell-face list.      */
+int kcfd_lsq_gradient(const kcfd_dmesh_t* m, const double* phi, const double* phi_b, double* grad, void* stream);
+
 /* SIMPLE correction (models/single_phase.py:355-377): U -= dP grad(p'),
  * p += alpha_p p'; norms2[0] = ||p'||^2, norms2[1] = ||p||^2 (after the update),
  * summed in a fixed order. grad_pp: [n][ndim].                                     */

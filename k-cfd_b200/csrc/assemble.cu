@@ -386,6 +386,93 @@ __global__ void k_gg_cell(DM m, const double* __restrict__ phi, const int8_t* __
     }
 }
 
+// Least-squares gradient per cell (core/gradient.py:51-99): over the cell's faces,
+// dx = x_N - x_P (internal, N the other cell) or x_f - x_P (boundary, with the face's
+// boundary value), dphi likewise; grad solves (A^T A) g = A^T dphi by Gaussian
+// elimination with partial pivoting (as LAPACK's gesv), zero for cells with fewer
+// than D faces or an exactly singular A^T A.
+template <int D>
+__global__ void k_lsq(DM m, const double* __restrict__ phi, const double* __restrict__ pb, double* __restrict__ g) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < m.n; i += gridDim.x * blockDim.x) {
+        double M[D][D + 1];
+#pragma unroll
+        for (int p = 0; p < D; ++p)
+#pragma unroll
+            for (int q = 0; q <= D; ++q) M[p][q] = 0.0;
+        double xp[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) xp[d] = m.cc[i * D + d];
+        const double pi = phi[i];
+        const int e0 = m.cf_ptr[i], e1 = m.cf_ptr[i + 1];
+        for (int e = e0; e < e1; ++e) {
+            const int f = m.cf_face[e];
+            double dx[D], dp;
+            if (f < m.Fi) {
+                const int o = m.owner[f];
+                const int nb = (o == i) ? m.neigh[f] : o;
+#pragma unroll
+                for (int d = 0; d < D; ++d) dx[d] = m.cc[nb * D + d] - xp[d];
+                dp = phi[nb] - pi;
+            } else {
+#pragma unroll
+                for (int d = 0; d < D; ++d) dx[d] = m.fcenter[f * D + d] - xp[d];
+                dp = pb[f - m.Fi] - pi;
+            }
+#pragma unroll
+            for (int p = 0; p < D; ++p) {
+#pragma unroll
+                for (int q = 0; q < D; ++q) M[p][q] += dx[p] * dx[q];
+                M[p][D] += dx[p] * dp;
+            }
+        }
+        double out[D];
+#pragma unroll
+        for (int d = 0; d < D; ++d) out[d] = 0.0;
+        bool ok = (e1 - e0) >= D;
+        if (ok) {
+#pragma unroll
+            for (int c = 0; c < D; ++c) {
+                int piv = c;
+                double best = fabs(M[c][c]);
+#pragma unroll
+                for (int r = c + 1; r < D; ++r)
+                    if (fabs(M[r][c]) > best) {
+                        best = fabs(M[r][c]);
+                        piv = r;
+                    }
+                if (best == 0.0) ok = false;
+                if (piv != c) {
+#pragma unroll
+                    for (int q = 0; q <= D; ++q) {
+                        const double t = M[c][q];
+                        M[c][q] = M[piv][q];
+                        M[piv][q] = t;
+                    }
+                }
+                if (ok) {
+#pragma unroll
+                    for (int r = c + 1; r < D; ++r) {
+                        const double l = M[r][c] / M[c][c];
+#pragma unroll
+                        for (int q = c; q <= D; ++q) M[r][q] -= l * M[c][q];
+                    }
+                }
+            }
+            if (ok) {
+#pragma unroll
+                for (int r = D - 1; r >= 0; --r) {
+                    double v = M[r][D];
+#pragma unroll
+                    for (int q = r + 1; q < D; ++q) v -= M[r][q] * out[q];
+                    out[r] = v / M[r][r];
+                }
+            }
+        }
+#pragma unroll
+        for (int d = 0; d < D; ++d) g[i * D + d] = ok ? out[d] : 0.0;
+    }
+}
+
 // ------------------------------------------------------------- reductions --------
 constexpr int kRedBlocks = 1024;
 
@@ -621,6 +708,18 @@ int kcfd_gg_gradient(const kcfd_dmesh_t* m, int32_t ncomp, const double* phi, co
     else { KC_GG(3, 3) }
 #undef KC_GG
     k_gg_cells<<<blocks_for(d.n), kThreads, 0, st>>>(d.n, ncomp * d.D, d.vol, grad);
+    KCFD_CUDA(cudaGetLastError());
+    return KCFD_OK;
+}
+
+int kcfd_lsq_gradient(const kcfd_dmesh_t* m, const double* phi, const double* phi_b, double* grad, void* stream) {
+    if (int e = check_mesh(m)) return e;
+    KCFD_REQUIRE(phi && phi_b && grad, "kcfd_lsq_gradient: NULL argument");
+    KCFD_REQUIRE(m->cf_ptr && m->cf_face, "kcfd_lsq_gradient: the mesh descriptor has no cell-face list");
+    cudaStream_t st = (cudaStream_t)stream;
+    DM d = to_dm(m);
+    if (d.D == 2) k_lsq<2><<<blocks_for(d.n), kThreads, 0, st>>>(d, phi, phi_b, grad);
+    else k_lsq<3><<<blocks_for(d.n), kThreads, 0, st>>>(d, phi, phi_b, grad);
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }

@@ -68,6 +68,7 @@ SIGNATURES = {
     "kcfd_solver_solve": (i32, [vp, C.POINTER(Csr), vp, vp, vp, vp, vp, vp]),
     "kcfd_solver_error": (i32, [vp, P_i32, vp]),
     "kcfd_solver_info": (i32, [vp, P_i32]),
+    "kcfd_lsq_gradient": (i32, [vp, vp, vp, vp, vp]),
     "kcfd_tf_drag": (i32, [vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_tf_interfacial": (i32, [vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_tf_phase_change": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),

@@ -252,3 +252,35 @@ def muscl_deferred_correction(mesh, phi, mf, grad, limiter_name="van_leer"):
     m = _interleave(keep, keep)
     np.add.at(corr, idx[m], val[m])
     return corr
+
+
+def least_squares_gradient(mesh, phi, phi_face_b):
+    """core/gradient.py:51-99: per cell, over its faces in the cell's own face order,
+    dx = x_N - x_P (internal; N the other cell) or x_f - x_P (boundary, with the
+    patch value), dphi likewise; grad = solve(A^T A, A^T dphi); zero for cells with
+    fewer than ndim faces or a singular A^T A. phi_face_b: per-face boundary value."""
+    nd = mesh.ndim
+    n = mesh.n_cells
+    cf = mesh.cell_faces
+    grad = np.zeros((n, nd))
+    for ci in range(n):
+        fids = cf[ci][cf[ci] >= 0]
+        if len(fids) < nd:
+            continue
+        xP = mesh.ccenter[ci, :nd]
+        rows, rhs = [], []
+        for f in fids:
+            if mesh.neighbour[f] >= 0:
+                nb = mesh.neighbour[f] if mesh.owner[f] == ci else mesh.owner[f]
+                rows.append(mesh.ccenter[nb, :nd] - xP)
+                rhs.append(phi[nb] - phi[ci])
+            else:
+                rows.append(mesh.fcenter[f, :nd] - xP)
+                rhs.append(phi_face_b[f] - phi[ci])
+        A = np.array(rows)
+        b = np.array(rhs)
+        try:
+            grad[ci] = np.linalg.solve(A.T @ A, A.T @ b)
+        except np.linalg.LinAlgError:
+            pass
+    return grad

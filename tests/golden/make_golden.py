@@ -142,7 +142,7 @@ def make_operators(out, meshes):
     from core.fvm_operators import (FVMSystem, diffusion_operator, convection_operator_upwind,
                                     temporal_operator, source_term, linearized_source,
                                     apply_boundary_conditions, under_relax)
-    from core.gradient import green_gauss_gradient
+    from core.gradient import green_gauss_gradient, least_squares_gradient
     from core.interpolation import compute_mass_flux, muscl_deferred_correction
     for name in ("quad", "tri", "hex", "hybrid"):
         m = meshes[name]
@@ -192,6 +192,7 @@ def make_operators(out, meshes):
         under_relax(s, phi, 0.7)
         d.update(_system_arrays(s, "full_"))
         d["gg"] = green_gauss_gradient(phi)
+        d["lsq"] = least_squares_gradient(phi)
         d["mflux"] = compute_mass_flux(U, 1.7, m)
         for lim in ("minmod", "superbee", "van_albada", "van_leer"):
             d["muscl_" + lim] = muscl_deferred_correction(m, phi, mf, d["gg"], lim)

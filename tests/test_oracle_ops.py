@@ -70,6 +70,8 @@ def test_gradient_flux_muscl_match_reference(name):
     fb = fvm.face_patch_values(m, phib, d["phi"])
     g = fvm.green_gauss_gradient(m, d["phi"], fb)
     np.testing.assert_allclose(g, d["gg"], rtol=1e-13, atol=1e-13)
+    gl = fvm.least_squares_gradient(m, d["phi"], fb)
+    np.testing.assert_allclose(gl, d["lsq"], rtol=1e-12, atol=1e-12)
     ub = _patch_split(m, d["U_b"])
     ufb = fvm.face_patch_values(m, ub, d["U"])
     mf = fvm.compute_mass_flux(m, d["U"], ufb, 1.7)

@@ -138,7 +138,8 @@ typedef struct {
                             (FP64 only: phase kernels in one CUDA graph per solve
                             with a device-side loop; inside a stream capture the
                             solve runs on the team-2 kernel). Auto: 1 for
-                            n*nrhs <= 40000, else 3 (FP64) or 2 (MIXED).
+                            n*nrhs <= 1024, 2 up to 40000 and for MIXED,
+                            else 3.                                              
                             KCFD_ENGINE_EAGER=1 in the environment at creation
                             launches the engine's kernels from a host loop
                             instead (for profilers; same results).             */

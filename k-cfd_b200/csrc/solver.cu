@@ -1618,10 +1618,16 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     for (int k = 0; k < nnz; ++k)
         if (ix[k] < 0 || ix[k] >= n) return fail("kcfd_solver_create: column index %d out of range at %d", ix[k], k);
     // team and launch shape
-    // auto: one CTA for small systems; large FP64 systems on the graph engine, large
-    // mixed ones on the persistent grid kernel
+    // auto: one CTA for tiny systems; the persistent grid kernel up to 40,000 unknowns
+    // (and for every mixed solve); the graph engine for large FP64 systems. Measured on
+    // a 4,096-row p' system: one CTA 35 us per Krylov iteration, the grid kernel 18 us,
+    // the graph engine 25 us. A caller that runs many small solves concurrently (the
+    // served loop) asks for one CTA explicitly, so that they overlap.
     int team = opts->team;
-    if (team == 0) team = ((int64_t)n * nrhs <= 40000) ? 1 : (mixed ? 2 : 3);
+    if (team == 0) {
+        const int64_t unk = (int64_t)n * nrhs;
+        team = (unk <= 1024) ? 1 : ((mixed || unk <= 40000) ? 2 : 3);
+    }
     if (team < 1 || team > 3) return fail("kcfd_solver_create: team must be 0..3");
     if (team == 3 && mixed) return fail("kcfd_solver_create: the graph engine (team 3) runs FP64 only");
     s->team = team;

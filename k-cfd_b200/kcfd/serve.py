@@ -99,8 +99,11 @@ class Case:
             m = build_mesh(nodes, cells, bd, ndim=3, cell_face_node_list=cf)
         self.stream = torch.cuda.Stream()
         with torch.cuda.stream(self.stream):
+            # one CTA per solve for the small cases, so that concurrent cases overlap on
+            # the device; the large ones take the grid-wide solvers
+            team = 1 if m.n_cells * m.ndim <= 40000 else 0
             s = SIMPLESolver(m, rho=1.0, mu=1.0 / req.Re, precision=precision, precond_p=precond_p, rtol=rtol,
-                             graph=graph)
+                             graph=graph, team=team)
             for nm in m.boundary_patches:
                 lid = [1.0] + [0.0] * (m.ndim - 1)
                 s.set_velocity_bc(nm, "dirichlet", lid if nm == "lid" else [0.0] * m.ndim)

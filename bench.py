@@ -570,9 +570,12 @@ def run_c5(args):
     if args.plain:
         sres = Server(max_active=1, policy="fifo", **common).run(reqs, serial=True)
         serial = summarize(sres)
-        same = all(np.array_equal(a.fields["U"], b.fields["U"]) for a, b in
-                   zip(sorted(res, key=lambda r: r.rid), sorted(sres, key=lambda r: r.rid)))
-        serial["fields_bitwise_equal_to_batched"] = bool(same)
+        # the serial run takes the library's single-case solvers (the grid kernel for
+        # small cases), the served run one CTA per small case: same algorithm, other
+        # reduction partition, so the fields agree to the solver tolerance
+        diffs = [float(np.linalg.norm(a.fields["U"] - b.fields["U"]) / max(np.linalg.norm(b.fields["U"]), 1e-300))
+                 for a, b in zip(sorted(res, key=lambda r: r.rid), sorted(sres, key=lambda r: r.rid))]
+        serial["max_rel_l2_U_vs_batched"] = max(diffs)
     line = {
         "metric": C5_METRIC, "value": round(ours["cases_per_s"], 3), "unit": "cases/s", "n_gpus": 1,
         "steps": len(reqs), "warmup": 2, "ms_per_step": round(1e3 / max(ours["cases_per_s"], 1e-9), 1),

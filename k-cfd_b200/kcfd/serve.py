@@ -84,7 +84,8 @@ def footprint_bytes(ndim, N, precision="mixed"):
 
 
 class Case:
-    def __init__(self, req, precision="mixed", graph=True, precond_p="ilu0", rtol=1e-8, device="cuda"):
+    def __init__(self, req, precision="mixed", graph=True, precond_p="ilu0", rtol=1e-8, device="cuda",
+                 small_team=1):
         torch = _lib.require_cuda()
         from .mesh import build_mesh
         from .meshgen import CAVITY_2D_NAMES, CAVITY_3D_NAMES, hex_box_arrays, quad_box_arrays
@@ -99,9 +100,10 @@ class Case:
             m = build_mesh(nodes, cells, bd, ndim=3, cell_face_node_list=cf)
         self.stream = torch.cuda.Stream()
         with torch.cuda.stream(self.stream):
-            # one CTA per solve for the small cases, so that concurrent cases overlap on
-            # the device; the large ones take the grid-wide solvers
-            team = 1 if m.n_cells * m.ndim <= 40000 else 0
+            # small_team=1: one CTA per solve for the small cases, so that concurrent cases
+            # overlap on the device (0: the library's choice, best for one case alone);
+            # the large ones take the grid-wide solvers either way
+            team = small_team if m.n_cells * m.ndim <= 40000 else 0
             s = SIMPLESolver(m, rho=1.0, mu=1.0 / req.Re, precision=precision, precond_p=precond_p, rtol=rtol,
                              graph=graph, team=team)
             for nm in m.boundary_patches:
@@ -174,7 +176,8 @@ class Server:
 
         def build(r):
             torch.cuda.set_device(dev)
-            return Case(r, self.precision, self.graph, self.precond_p)
+            # alone, a case takes the library's fastest single-case solvers
+            return Case(r, self.precision, self.graph, self.precond_p, small_team=0 if serial else 1)
 
         t0 = time.perf_counter()
         with ThreadPoolExecutor(max_workers=self.builders) as pool:

@@ -850,7 +850,8 @@ def run_reference(args):
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_full, 1),
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"3D jittered lid-driven cavity {N}^3 (oracle numpy/scipy on host cores)"},
-            "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": os.cpu_count(), "kind": "port",
+            "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": 1, "kind": "port",
+                             "host_cores_available": os.cpu_count(),
                              "sample": f"per step: 1 outer iteration at {CPU_SAMPLE_N}^3 ({t:.2f} s), scaled "
                                        f"x{cell_scale:.1f} (cells) and p' share x{its_scale:.2f} (Krylov growth ~N)"},
             "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}

@@ -219,7 +219,8 @@ def limiter(name, r):
     if name == "van_albada":
         return np.where(r > 0, (r * r + r) / (r * r + 1.0), 0.0)
     if name == "van_leer":
-        return np.where(r > 0, 2.0 * r / (1.0 + r), 0.0)
+        with np.errstate(divide="ignore", invalid="ignore"):  # r = -1 lies in the discarded branch
+            return np.where(r > 0, 2.0 * r / (1.0 + r), 0.0)
     raise ValueError(f"Unknown limiter: {name}")
 
 

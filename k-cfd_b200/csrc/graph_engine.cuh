@@ -71,6 +71,16 @@ struct Args {
     int eager;          // 1: launched from a host loop (no graph, no condition to set)
 };
 
+// Programmatic dependent launch: the phase kernels of one iteration are launched so
+// that the next kernel's CTAs may be scheduled while this one drains. Each phase
+// kernel first waits for the full completion (and memory visibility) of the kernel
+// before it, then allows its own successor to launch. Without the launch attribute
+// both instructions return at once.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+}
+
 // Rows per thread and per step of the vector kernels: U rows spaced by the grid
 // stride, all loads issued before any store (memory-level parallelism).
 template <int NRHS>
@@ -266,6 +276,7 @@ __global__ void __launch_bounds__(kBlock) g_init(Args a) {
 // the level-0 rows of the ILU forward sweep (phat = p there).
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_p(Args a) {
+    pdl_enter();
     const St& S = *a.st;
     if (blockIdx.x == 0 && threadIdx.x == 0) a.st->trips += 1;
     if (!S.active) return;
@@ -323,6 +334,7 @@ __global__ void __launch_bounds__(kBlock) g_p(Args a) {
 // scaling (no upper entries there) is applied too.
 template <int NRHS>
 __global__ void __launch_bounds__(kBlock) g_fwd(Args a, int l, int which) {
+    pdl_enter();
     const St& S = *a.st;
     if (!S.active) return;
     const double* q = which ? a.r : a.p;
@@ -353,6 +365,7 @@ __global__ void __launch_bounds__(kBlock) g_fwd(Args a, int l, int which) {
 // the whole preconditioner after the level-0 copy.
 template <int NRHS>
 __global__ void __launch_bounds__(kBlock) g_bwd(Args a, int l, int which) {
+    pdl_enter();
     const St& S = *a.st;
     if (!S.active) return;
     double* z = which ? a.sh : a.ph;
@@ -378,6 +391,7 @@ __global__ void __launch_bounds__(kBlock) g_bwd(Args a, int l, int which) {
 
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_spmv_v(Args a) {
+    pdl_enter();
     St& S = *a.st;
     if (!S.active) return;
     const double* ph = (PREC == KCFD_PREC_NONE) ? a.p : a.ph;
@@ -426,6 +440,7 @@ __global__ void __launch_bounds__(kBlock) g_spmv_v(Args a) {
 // s = r - alpha v (in r); shat = M^-1 s for Jacobi / level-0 copy for ILU; ||s||.
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_s(Args a) {
+    pdl_enter();
     St& S = *a.st;
     if (!S.active) return;
     constexpr int U = Ilp<NRHS>::U;
@@ -502,6 +517,7 @@ __global__ void __launch_bounds__(kBlock) g_s(Args a) {
 // and t.s, t.t for the others.
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_spmv_t(Args a) {
+    pdl_enter();
     St& S = *a.st;
     int sc[NRHS], dn[NRHS];
     double al[NRHS];
@@ -574,6 +590,7 @@ __global__ void __launch_bounds__(kBlock) g_spmv_t(Args a) {
 // and the loop condition.
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_xr(Args a) {
+    pdl_enter();
     St& S = *a.st;
     // unconditional bound on the loop, whatever the state logic does
     if (!a.eager && blockIdx.x == 0 && threadIdx.x == 0 && S.trips > a.maxiter + 2) cudaGraphSetConditional(a.cond, 0u);

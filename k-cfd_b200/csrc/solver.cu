@@ -1112,6 +1112,7 @@ struct kcfd_solver {
         const double* vals_key = nullptr;  // caller values the graph was built for (non-permuted)
         int gmax = 0;
         int eager = 0;                     // host-driven loop instead of the graph
+        bool pdl = true;                   // phase kernels with programmatic dependent launch
         bool ready = false;                // args (and graph) built
         ge::Args args;
         ge::Sell A, L, U;                  // sliced-ELL copies (L, U: ILU only)
@@ -1257,25 +1258,41 @@ GeGrid ge_grids(int n, int sms, int gmax) {
     return r;
 }
 
+// Launch of one phase kernel, with programmatic dependent launch when pdl is set.
+template <typename... KArgs, typename... Act>
+void ge_launch(void (*k)(KArgs...), int grid, cudaStream_t cs, bool pdl, Act&&... args) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(grid);
+    cfg.blockDim = dim3(ge::kBlock);
+    cfg.stream = cs;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    at[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = pdl ? at : nullptr;
+    cfg.numAttrs = pdl ? 1 : 0;
+    cudaLaunchKernelEx(&cfg, k, std::forward<Act>(args)...);
+}
+
 // One loop trip: the phase kernels of one BiCGSTAB iteration.
 template <int NRHS, int PREC>
-void ge_body(const ge::Args& a, const GeGrid& G, cudaStream_t cs) {
-    ge::g_p<NRHS, PREC><<<G.p, ge::kBlock, 0, cs>>>(a);
+void ge_body(const ge::Args& a, const GeGrid& G, cudaStream_t cs, bool pdl) {
+    ge_launch(ge::g_p<NRHS, PREC>, G.p, cs, pdl, a);
     auto sweeps = [&](int which) {
         if (PREC != KCFD_PREC_ILU0) return;
         if (a.nlev == 1) {
-            ge::g_bwd<NRHS><<<G.bwd, ge::kBlock, 0, cs>>>(a, 0, which);
+            ge_launch(ge::g_bwd<NRHS>, G.bwd, cs, pdl, a, 0, which);
             return;
         }
-        for (int l = 1; l < a.nlev; ++l) ge::g_fwd<NRHS><<<G.fwd, ge::kBlock, 0, cs>>>(a, l, which);
-        for (int l = a.nlev - 2; l >= 0; --l) ge::g_bwd<NRHS><<<G.bwd, ge::kBlock, 0, cs>>>(a, l, which);
+        for (int l = 1; l < a.nlev; ++l) ge_launch(ge::g_fwd<NRHS>, G.fwd, cs, pdl, a, l, which);
+        for (int l = a.nlev - 2; l >= 0; --l) ge_launch(ge::g_bwd<NRHS>, G.bwd, cs, pdl, a, l, which);
     };
     sweeps(0);
-    ge::g_spmv_v<NRHS, PREC><<<G.sv, ge::kBlock, 0, cs>>>(a);
-    ge::g_s<NRHS, PREC><<<G.s, ge::kBlock, 0, cs>>>(a);
+    ge_launch(ge::g_spmv_v<NRHS, PREC>, G.sv, cs, pdl, a);
+    ge_launch(ge::g_s<NRHS, PREC>, G.s, cs, pdl, a);
     sweeps(1);
-    ge::g_spmv_t<NRHS, PREC><<<G.st, ge::kBlock, 0, cs>>>(a);
-    ge::g_xr<NRHS, PREC><<<G.xr, ge::kBlock, 0, cs>>>(a);
+    ge_launch(ge::g_spmv_t<NRHS, PREC>, G.st, cs, pdl, a);
+    ge_launch(ge::g_xr<NRHS, PREC>, G.xr, cs, pdl, a);
 }
 
 // Eager form: init, body trips in chunks with a host read of the active flag, final.
@@ -1292,7 +1309,7 @@ int ge_eager(kcfd_solver* s, cudaStream_t st) {
         KCFD_CUDA(cudaMemcpyAsync(&active, &a.st->active, sizeof(int), cudaMemcpyDeviceToHost, st));
         KCFD_CUDA(cudaStreamSynchronize(st));
         if (!active) break;
-        for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC>(a, G, st);
+        for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC>(a, G, st, s->g.pdl);
         KCFD_CUDA(cudaGetLastError());
     }
     ge::g_final<NRHS><<<1, 256, 0, st>>>(a);
@@ -1386,19 +1403,31 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     KCFD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        ge_body<NRHS, PREC>(a, G, cs);
+        ge_body<NRHS, PREC>(a, G, cs, g.pdl);
         cudaGraph_t outg = nullptr;
         const cudaError_t e2 = cudaStreamEndCapture(cs, &outg);
         if (e == cudaSuccess) e = e2;
     }
     const cudaError_t e3 = cudaStreamDestroy(cs);
-    KCFD_CUDA(e);
     KCFD_CUDA(e3);
-    kp.func = (void*)ge::g_final<NRHS>;
-    kp.gridDim = dim3(1);
-    kp.blockDim = dim3(256);
-    KCFD_CUDA(cudaGraphAddKernelNode(&n_fin, g.graph, &n_cond, 1, &kp));
-    KCFD_CUDA(cudaGraphInstantiate(&g.exec, g.graph, 0));
+    if (e == cudaSuccess) {
+        kp.func = (void*)ge::g_final<NRHS>;
+        kp.gridDim = dim3(1);
+        kp.blockDim = dim3(256);
+        e = cudaGraphAddKernelNode(&n_fin, g.graph, &n_cond, 1, &kp);
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&g.exec, g.graph, 0);
+    if (e != cudaSuccess && g.pdl) {
+        // a driver that does not take programmatic edges inside the loop body: plain launches
+        cudaGetLastError();
+        if (g.exec) cudaGraphExecDestroy(g.exec);
+        cudaGraphDestroy(g.graph);
+        g.exec = nullptr;
+        g.graph = nullptr;
+        g.pdl = false;
+        return ge_build<NRHS, PREC>(s, A);
+    }
+    KCFD_CUDA(e);
     g.vals_key = A->vals64;
     g.ready = true;
     return KCFD_OK;
@@ -1634,6 +1663,8 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     if (team == 3) {
         const char* ev = std::getenv("KCFD_ENGINE_EAGER");
         s->g.eager = (ev && ev[0] == '1') ? 1 : 0;
+        const char* pv = std::getenv("KCFD_ENGINE_PDL");
+        s->g.pdl = !(pv && pv[0] == '0');
     }
     int lanes = opts->lanes;
     if (lanes <= 0) {

@@ -216,7 +216,7 @@ def p_solve_roofline(s, peak, reps=3):
     torch.cuda.synchronize()
     ts = e0.elapsed_time(e1) / 1e3 / K
     sb = nnz * 12 + 4 * (n + 1) + 16 * n
-    spmv = {"kernel": "spmv_kernel<double> (kcfd_spmv_f64, row per thread)", "bytes": int(sb), "launch_us": round(ts * 1e6, 2),
+    spmv = {"kernel": "spmv_row_kernel<double> (kcfd_spmv_f64, row per thread, entries loaded before the x gathers)", "bytes": int(sb), "launch_us": round(ts * 1e6, 2),
             "achieved": round(sb / ts / 1e9, 1), "frac": round(sb / ts / 1e9 / peak[0], 3)}
     # bytes the engine actually moves: on ILU level 0 the SpMV phases copy q instead of
     # multiplying (A M^-1 q = q there), so two SpMVs skip those rows' values, columns

@@ -142,9 +142,11 @@ typedef struct {
                             else 3.                                              
                             KCFD_ENGINE_EAGER=1 in the environment at creation
                             launches the engine's kernels from a host loop
-                            instead (for profilers; same results).             */
+                            instead (for profilers; same results);
+                            KCFD_ENGINE_PDL=0 launches its phase kernels
+                            without programmatic dependent launch.            */
     int32_t lanes;       /* SpMV lanes per row: 0 auto, 1..32                  */
-    int32_t block;       /* threads per CTA: 0 auto                            */
+    int32_t block;       /* threads per CTA: 0 auto (team 1: 512, team 2: 512) */
     double  rtol;        /* relative tolerance                                 */
     double  atol;        /* absolute tolerance (KCFD_STOP_SCIPY)               */
     double  inner_rtol;  /* MIXED: inner FP32 solve reduction per refinement   */

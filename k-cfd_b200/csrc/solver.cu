@@ -847,8 +847,11 @@ __global__ void __launch_bounds__(grid_block(NRHS), 1) solve_grid_kernel(SolveAr
     else solve_fp64<NRHS, PREC>(tm, a, smem);
 }
 
-template <int MIXED, int NRHS, int PREC>
-__global__ void __launch_bounds__(1024) solve_cta_kernel(SolveArgs a) {
+// One CTA per solve. MAXB is the largest block it is launched with: 1024 threads cap
+// a thread at 64 registers (the FP64 phases then spill to local memory); the
+// 512-thread instance has 128.
+template <int MIXED, int NRHS, int PREC, int MAXB = 1024>
+__global__ void __launch_bounds__(MAXB, 1) solve_cta_kernel(SolveArgs a) {
     __shared__ double smem[32 * kMaxK];
     CtaTeam tm;
     if (MIXED) solve_mixed<NRHS, PREC>(tm, a, smem);
@@ -1126,13 +1129,14 @@ struct kcfd_solver {
 namespace {
 
 template <int MIXED, int NRHS, int PREC>
-void* pick_kernel(bool grid) {
-    return grid ? (void*)solve_grid_kernel<MIXED, NRHS, PREC> : (void*)solve_cta_kernel<MIXED, NRHS, PREC>;
+void* pick_kernel(bool grid, int block) {
+    if (grid) return (void*)solve_grid_kernel<MIXED, NRHS, PREC>;
+    return block <= 512 ? (void*)solve_cta_kernel<MIXED, NRHS, PREC, 512> : (void*)solve_cta_kernel<MIXED, NRHS, PREC, 1024>;
 }
 
-void* solve_kernel_ptr(int mixed, int nrhs, int prec, bool grid) {
+void* solve_kernel_ptr(int mixed, int nrhs, int prec, bool grid, int block) {
 #define KC_CASE(M, R, P) \
-    if (mixed == M && nrhs == R && prec == P) return pick_kernel<M, R, P>(grid);
+    if (mixed == M && nrhs == R && prec == P) return pick_kernel<M, R, P>(grid, block);
     KC_CASE(0, 1, 0) KC_CASE(0, 1, 1) KC_CASE(0, 1, 2)
     KC_CASE(0, 2, 0) KC_CASE(0, 2, 1) KC_CASE(0, 2, 2)
     KC_CASE(0, 3, 0) KC_CASE(0, 3, 1) KC_CASE(0, 3, 2)
@@ -1677,7 +1681,9 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     if ((lanes & (lanes - 1)) != 0 || lanes < 1 || lanes > 32) return fail("kcfd_solver_create: lanes must be 1..32 pow2");
     s->lanes = lanes;
     const int max_grid_block = grid_block(nrhs);
-    s->block = opts->block > 0 ? opts->block : (team == 1 ? 1024 : max_grid_block);
+    // one CTA: 512 threads with 128 registers (measured 30.5 us per Jacobi BiCGSTAB
+    // iteration on the 64^2 cavity p' system against 32.3 us for 1024 threads at 64)
+    s->block = opts->block > 0 ? opts->block : (team == 1 ? 512 : max_grid_block);
     if (team >= 2 && s->block > max_grid_block) s->block = max_grid_block;
     if (team == 1 && s->block > 1024) s->block = 1024;
     if (s->block % 32 != 0 || s->block < 32) return fail("kcfd_solver_create: block must be a multiple of 32");
@@ -1749,7 +1755,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     }
     // team 3 keeps the grid kernel's launch shape too: it factors ILU(0) with the
     // grid factor kernel and solves on the grid kernel inside stream captures
-    void* kern = solve_kernel_ptr(mixed, nrhs, opts->precond, team >= 2);
+    void* kern = solve_kernel_ptr(mixed, nrhs, opts->precond, team >= 2, s->block);
     if (team >= 2) {
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, s->block, 0) != cudaSuccess || per_sm < 1) {
@@ -1871,7 +1877,7 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
         if (cap == cudaStreamCaptureStatusNone)
             return ge_solve(s, A, b, x, iters, relres, status, (cudaStream_t)stream);
     }
-    void* kern = solve_kernel_ptr(mixed, s->o.nrhs, s->o.precond, s->team >= 2);
+    void* kern = solve_kernel_ptr(mixed, s->o.nrhs, s->o.precond, s->team >= 2, s->block);
     KCFD_REQUIRE(kern != nullptr, "kcfd_solver_solve: no kernel for this configuration");
     void* args[] = {&a};
     return launch_team(s, kern, args, (cudaStream_t)stream);
@@ -2248,25 +2254,75 @@ __global__ void spmv_kernel(int n, const int* __restrict__ ip, const int* __rest
     }
 }
 
+// Short rows (FVM rows of 4-8 entries), one row per thread: the first kRowBatch
+// columns and values of the row are all loaded before the first gather of x, so a
+// thread waits for three memory round trips per row (row pointers, entries, x)
+// instead of one per entry; longer rows finish in a loop. Entries are summed in row
+// order, as the lane kernel does with one lane.
+constexpr int kRowBatch = 8;
+template <typename VM, typename VX, int NRHS>
+__global__ void __launch_bounds__(256) spmv_row_kernel(int n, const int* __restrict__ ip, const int* __restrict__ ix,
+                                                       const VM* __restrict__ val, const VX* __restrict__ x,
+                                                       VX* __restrict__ y) {
+    for (int r = blockIdx.x * blockDim.x + threadIdx.x; r < n; r += gridDim.x * blockDim.x) {
+        const int kb = __ldg(ip + r), ke = __ldg(ip + r + 1);
+        int c[kRowBatch];
+        double v[kRowBatch];
+#pragma unroll
+        for (int k = 0; k < kRowBatch; ++k) {
+            const bool in = kb + k < ke;
+            c[k] = in ? __ldg(ix + kb + k) : 0;
+            v[k] = in ? (double)__ldg(val + kb + k) : 0.0;
+        }
+        double acc[NRHS];
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) acc[q] = 0.0;
+#pragma unroll
+        for (int k = 0; k < kRowBatch; ++k)
+            if (kb + k < ke) {
+#pragma unroll
+                for (int q = 0; q < NRHS; ++q) acc[q] += v[k] * (double)x[(size_t)c[k] * NRHS + q];
+            }
+        for (int k = kb + kRowBatch; k < ke; ++k) {
+            const int j = __ldg(ix + k);
+            const double a = (double)__ldg(val + k);
+#pragma unroll
+            for (int q = 0; q < NRHS; ++q) acc[q] += a * (double)x[(size_t)j * NRHS + q];
+        }
+#pragma unroll
+        for (int q = 0; q < NRHS; ++q) y[(size_t)r * NRHS + q] = (VX)acc[q];
+    }
+}
+
 template <typename V>
 int spmv_launch(const kcfd_csr_t* A, const V* vals, const V* x, V* y, int nrhs, cudaStream_t st) {
+    if (nrhs < 1 || nrhs > 3) {
+        set_error("kcfd_spmv: nrhs must be 1, 2 or 3");
+        return KCFD_BAD_INPUT;
+    }
     // one lane streams up to ~8 entries of a row, as in the solver kernels
     const double avg = (double)A->nnz / std::max(A->n, 1);
     int L = 1;
     while (L < 32 && 8 * L < avg) L <<= 1;
     const int threads = 256;
+    if (L == 1) {
+        // 8 resident CTAs per SM, rows taken grid-stride (measured fastest on the
+        // 128^3 7-point matrix: 39.4 us against 41-43 us for one CTA per 256 rows)
+        const int blocks = (int)std::max<int64_t>(1, std::min<int64_t>(((int64_t)A->n + threads - 1) / threads, 148 * 8));
+        if (nrhs == 1) spmv_row_kernel<V, V, 1><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y);
+        else if (nrhs == 2) spmv_row_kernel<V, V, 2><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y);
+        else spmv_row_kernel<V, V, 3><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y);
+        KCFD_CUDA(cudaGetLastError());
+        return KCFD_OK;
+    }
     int blocks = (int)std::min<int64_t>(((int64_t)A->n * L + threads - 1) / threads, 148 * 16);
     blocks = std::max(blocks, 1);
     if (nrhs == 1)
         spmv_kernel<V, V, 1><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y, L);
     else if (nrhs == 2)
         spmv_kernel<V, V, 2><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y, L);
-    else if (nrhs == 3)
+    else
         spmv_kernel<V, V, 3><<<blocks, threads, 0, st>>>(A->n, A->indptr, A->indices, vals, x, y, L);
-    else {
-        set_error("kcfd_spmv: nrhs must be 1, 2 or 3");
-        return KCFD_BAD_INPUT;
-    }
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }

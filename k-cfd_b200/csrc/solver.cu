@@ -136,6 +136,49 @@ template <typename VM, typename VX, int NRHS, bool DIFF = false, class Epi>
 __device__ __forceinline__ void spmv_range(const int* __restrict__ ip, const int* __restrict__ ix,
                                            const VM* __restrict__ val, const VX* x, int r0, int r1, int L,
                                            Epi epi) {
+    if (L == 1) {
+        // one thread per row: the first 8 columns and values are loaded before the
+        // first gather of x (three memory round trips per row instead of one per
+        // entry); entries are summed in row order as below
+        constexpr int E = 8;
+        for (int row = r0 + (int)threadIdx.x; row < r1; row += blockDim.x) {
+            const int kb = __ldg(ip + row), ke = __ldg(ip + row + 1);
+            int cj[E];
+            double av[E];
+#pragma unroll
+            for (int k = 0; k < E; ++k) {
+                const bool in = kb + k < ke;
+                cj[k] = in ? __ldg(ix + kb + k) : row;
+                av[k] = in ? (double)val[kb + k] : 0.0;
+            }
+            double xi[NRHS], acc[NRHS];
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) {
+                acc[c] = 0.0;
+                if (DIFF) xi[c] = (double)x[(size_t)row * NRHS + c];
+            }
+            auto term = [&](int j, double a) {
+                if (DIFF) {
+                    if (j == row) {
+#pragma unroll
+                        for (int c = 0; c < NRHS; ++c) acc[c] += a * xi[c];
+                    } else {
+#pragma unroll
+                        for (int c = 0; c < NRHS; ++c) acc[c] += a * ((double)x[(size_t)j * NRHS + c] - xi[c]);
+                    }
+                } else {
+#pragma unroll
+                    for (int c = 0; c < NRHS; ++c) acc[c] += a * (double)x[(size_t)j * NRHS + c];
+                }
+            };
+#pragma unroll
+            for (int k = 0; k < E; ++k)
+                if (kb + k < ke) term(cj[k], av[k]);
+            for (int k = kb + E; k < ke; ++k) term(__ldg(ix + k), (double)val[k]);
+            epi(row, acc);
+        }
+        return;
+    }
     const int lane = threadIdx.x & 31;
     const int sub = lane / L, sl = lane % L;
     const int rows_per_warp = 32 / L;

@@ -446,8 +446,11 @@ def run_c4(args):
     byts = sum(_c4_bytes(int(n_sys[k]), int(nnz_sys[k]), int(its[k]), mixed) for k in range(len(mine)))
     launch = t / args.steps
     peak = measured_peak()
-    roof = {"bound": "hbm", "kernel": f"batch_kernel<MIXED={int(mixed)}, JACOBI, 512 | 256> (one CTA per system, "
-                                      "largest first, two size tiers)",
+    tiers = bs.tiers()
+    roof = {"bound": "hbm", "kernel": f"batch_cluster_kernel<MIXED={int(mixed)}, JACOBI> (systems of >= 131,072 rows, "
+                                      f"one thread-block cluster of {tiers['cluster_size']} CTAs each) + "
+                                      f"batch_kernel<MIXED={int(mixed)}, JACOBI, 512 | 256> (one CTA per system), "
+                                      "largest first, three size tiers",
             "unit_of_work": "one launch solving all systems", "achieved": round(byts / launch / 1e9, 1),
             "peak": peak[0], "unit": "GB/s", "frac": round(byts / launch / 1e9 / peak[0], 3),
             "peak_source": peak[1], "traffic": None, "launch_ms": round(launch * 1e3, 3)}
@@ -535,7 +538,8 @@ def run_c4(args):
                        "parallelism": f"LPT shards x{world}" if world > 1 else "1 GPU",
                        "l2": "working set >> 126 MB L2; no flush needed", "generation_s": round(gen_s, 1)},
             "clocks": clocks, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "plain_fp64_dropin": plain,
-            "gpu_launches": 2 * args.steps,
+            "gpu_launches": (1 + sum(1 for k in ("cluster", "big", "small") if tiers[k] > 0)) * args.steps,
+            "tiers": tiers,
             "status_ok": int((st == 0).sum()), "max_true_relres": worst,
             "krylov_iters": {"min": int(its.min()), "median": int(np.median(its)), "max": int(its.max())},
         }

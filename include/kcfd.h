@@ -176,18 +176,23 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
 
 /* ------------------------------------------------------ batched systems ---- */
 /* Many independent systems (e.g. the pressure-correction systems of many meshes) of
- * uneven sizes solved together over packed CSR with per-system offsets: each CTA takes
- * the next system from a largest-first queue and solves it alone (FP64 or MIXED
- * BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule per system). Two
- * tiers run concurrently: systems of at least big_rows rows on 512-thread CTAs (one
- * per SM), the rest on 256-thread CTAs; one persistent launch per tier. A system's
- * tier depends only on its own size, so its result is the same alone and in any mix.
- * No counterpart API in the reference, which solves one system per call
- * (core/linear_solver.py:14-70); results per system equal that path's semantics.     */
+ * uneven sizes solved together over packed CSR with per-system offsets: each team
+ * takes the next system from a largest-first queue and solves it alone (FP64 or MIXED
+ * BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule per system). Three
+ * tiers run concurrently, one persistent launch each: systems of at least
+ * cluster_rows rows are solved by the cluster_size CTAs of one thread-block cluster
+ * (512 threads each, one per SM, rows split between them, bounded software
+ * barriers); systems of at least big_rows rows by one 512-thread CTA; the rest by one
+ * 256-thread CTA. A system's tier depends only on its own size (and, for the cluster
+ * tier, on whether a cluster can be resident at all), so its result is the same alone
+ * and in any mix. No counterpart API in the reference, which solves one system per
+ * call (core/linear_solver.py:14-70); results per system equal that path's semantics. */
 typedef struct kcfd_batch kcfd_batch;
 typedef struct {
     int32_t precond, stop, mode, maxiter, lanes, max_refine, inner_maxiter;
-    int32_t big_rows;  /* tier threshold in rows: 0 default (16384), < 0 one tier */
+    int32_t big_rows;      /* tier threshold in rows: 0 default (16384), < 0 none      */
+    int32_t cluster_rows;  /* cluster tier threshold: 0 default (131072), < 0 none     */
+    int32_t cluster_size;  /* CTAs per cluster team: 0 default (4), 2..8               */
     double  rtol, atol, inner_rtol;
 } kcfd_batch_opts_t;
 /* indptr_host: per system n[s]+1 local row pointers, concatenated; indices_host:
@@ -197,6 +202,9 @@ int  kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const
 void kcfd_batch_destroy(kcfd_batch* b);
 /* info[0..3] = nsys, total rows, total entries, CTAs per launch */
 int  kcfd_batch_info(const kcfd_batch* b, int64_t* info);
+/* tiers[5]: systems in the cluster, big and small tiers, clusters launched, CTAs
+ * per cluster.                                                                     */
+int  kcfd_batch_tiers(const kcfd_batch* b, int32_t* tiers);
 /* vals64, rhs, x: packed device arrays (system s at its row / entry offset); x holds
  * x0 on entry. iters/relres/status: device arrays of nsys entries.                 */
 int  kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, double* x, int32_t* iters,

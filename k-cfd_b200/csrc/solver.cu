@@ -973,6 +973,85 @@ __global__ void batch_prep_kernel(BatchArgs B) {
     }
 }
 
+// SolveArgs of system sid of a batch (everything but the team control).
+template <typename V>
+__device__ SolveArgs batch_args(const BatchArgs& B, int sid) {
+    const BatchSys S = B.sys[sid];
+    SolveArgs a;
+    memset(&a, 0, sizeof(a));
+    a.n = S.n;
+    a.lanes = B.lanes;
+    a.indptr = B.indptr + S.ptr_off;
+    a.indices = B.indices + S.nnz_off;
+    a.vals64 = B.vals64 + S.nnz_off;
+    a.vals32 = B.vals32 ? B.vals32 + S.nnz_off : nullptr;
+    a.dinv = (V*)B.dinv + S.row_off;
+    a.lev_ptr = B.lev + 2 * sid;
+    a.nlev = 1;
+    a.work = (V*)B.work + 9 * S.row_off;
+    a.x = B.x + S.row_off;
+    a.b = B.b + S.row_off;
+    a.r64 = B.r64 ? B.r64 + S.row_off : nullptr;
+    a.stop = B.stop;
+    a.maxiter = B.maxiter;
+    a.max_refine = B.max_refine;
+    a.inner_maxiter = B.inner_maxiter;
+    a.rtol = B.rtol;
+    a.atol = B.atol;
+    a.inner_rtol = B.inner_rtol;
+    a.iters_out = B.iters + sid;
+    a.relres_out = B.relres + sid;
+    a.status_out = B.status + sid;
+    return a;
+}
+
+// Team control of the cluster tier: per cluster a barrier counter, a published queue
+// entry and the reduction partials; one error flag for the launch.
+struct ClusterCtl {
+    unsigned int* bar;  // [clusters], zeroed before each launch
+    int* slot;          // [clusters]
+    double* partials;   // [clusters][kSlots * kMaxK * cluster size]
+    int* err;
+    long long budget;
+};
+
+// Cluster tier: the largest systems, each solved by the CTAs of one thread-block
+// cluster (512 threads per CTA, one CTA per SM) as a team that splits the rows and
+// meets at bounded software barriers (GridTeam over the cluster's CTAs, which the
+// hardware schedules together). Rank 0 takes the next system from the queue and
+// publishes it; a system's result depends only on the system and the cluster size.
+template <int MIXED, int PREC>
+__global__ void __launch_bounds__(512, 1) batch_cluster_kernel(BatchArgs B, ClusterCtl C) {
+    __shared__ double smem[32 * kMaxK];
+    using V = typename std::conditional<MIXED, float, double>::type;
+    int crank, csize, cid;
+    cluster_ids(crank, csize, cid);
+    TeamCtl ctl;
+    ctl.bar = C.bar + cid;
+    ctl.partials = C.partials + (size_t)cid * kSlots * kMaxK * csize;
+    ctl.err = C.err;
+    ctl.budget = C.budget;
+    GridTeam tm(ctl, crank, csize);
+    for (;;) {
+        if (crank == 0 && threadIdx.x == 0) C.slot[cid] = atomicAdd(B.queue, 1);
+        if (!tm.sync()) break;
+        const int q = __ldcg(C.slot + cid);
+        // every member has read the entry before rank 0 can overwrite it
+        if (!tm.sync()) break;
+        if (q >= B.nq) break;
+        const int sid = B.order[q];
+        SolveArgs a = batch_args<V>(B, sid);
+        a.ctl = ctl;
+        if (MIXED) solve_mixed<1, PREC>(tm, a, smem);
+        else solve_fp64<1, PREC>(tm, a, smem);
+        if (*(volatile int*)C.err != 0) {
+            // a barrier wait expired: the system has no result
+            if (crank == 0 && threadIdx.x == 0) B.status[sid] = 5 /*KCFD_TIMEOUT*/;
+            break;
+        }
+    }
+}
+
 template <int MIXED, int PREC, int BLOCK>
 __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 2 : 1) batch_kernel(BatchArgs B) {
     __shared__ double smem[32 * kMaxK];
@@ -986,32 +1065,7 @@ __global__ void __launch_bounds__(BLOCK, BLOCK == 256 ? 2 : 1) batch_kernel(Batc
         __syncthreads();
         if (q >= B.nq) break;
         const int sid = B.order[q];
-        const BatchSys S = B.sys[sid];
-        SolveArgs a;
-        memset(&a, 0, sizeof(a));
-        a.n = S.n;
-        a.lanes = B.lanes;
-        a.indptr = B.indptr + S.ptr_off;
-        a.indices = B.indices + S.nnz_off;
-        a.vals64 = B.vals64 + S.nnz_off;
-        a.vals32 = B.vals32 ? B.vals32 + S.nnz_off : nullptr;
-        a.dinv = (V*)B.dinv + S.row_off;
-        a.lev_ptr = B.lev + 2 * sid;
-        a.nlev = 1;
-        a.work = (V*)B.work + 9 * S.row_off;
-        a.x = B.x + S.row_off;
-        a.b = B.b + S.row_off;
-        a.r64 = B.r64 ? B.r64 + S.row_off : nullptr;
-        a.stop = B.stop;
-        a.maxiter = B.maxiter;
-        a.max_refine = B.max_refine;
-        a.inner_maxiter = B.inner_maxiter;
-        a.rtol = B.rtol;
-        a.atol = B.atol;
-        a.inner_rtol = B.inner_rtol;
-        a.iters_out = B.iters + sid;
-        a.relres_out = B.relres + sid;
-        a.status_out = B.status + sid;
+        SolveArgs a = batch_args<V>(B, sid);
         if (MIXED) solve_mixed<1, PREC>(tm, a, smem);
         else solve_fp64<1, PREC>(tm, a, smem);
         __syncthreads();
@@ -1960,19 +2014,28 @@ struct kcfd_batch {
     int* lev = nullptr;
     void* work = nullptr;
     double* r64 = nullptr;
-    // tiers: order[0..nbig) big systems (512-thread CTAs), then the rest
-    int nbig = 0, grid_big = 0;
-    cudaStream_t side = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
+    // tiers: order[0..nhuge) cluster teams, then nbig big systems (512-thread CTAs),
+    // then the rest
+    int nhuge = 0, nbig = 0, grid_big = 0;
+    int csize = 0, ncl = 0;               // cluster tier: CTAs per cluster, clusters launched
+    unsigned int* cbar = nullptr;         // [ncl] barrier counters
+    int* cslot = nullptr;                 // [ncl] published queue entries
+    double* cpart = nullptr;              // [ncl][kSlots][kMaxK][csize]
+    int* cerr = nullptr;
+    cudaStream_t side = nullptr, side2 = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
 };
 
 namespace {
 int free_batch(kcfd_batch* b) {
     if (!b) return KCFD_OK;
     if (b->side) cudaStreamDestroy(b->side);
+    if (b->side2) cudaStreamDestroy(b->side2);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
-    void* ps[] = {b->sys, b->order, b->queue, b->indptr, b->indices, b->vals32, b->dinv, b->lev, b->work, b->r64};
+    if (b->ev_join2) cudaEventDestroy(b->ev_join2);
+    void* ps[] = {b->sys,  b->order, b->queue, b->indptr, b->indices, b->vals32, b->dinv,
+                  b->lev,  b->work,  b->r64,   b->cbar,   b->cslot,   b->cpart,  b->cerr};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete b;
@@ -1988,6 +2051,27 @@ void* batch_kernel_ptr_t(int mixed, int precond) {
 }
 void* batch_kernel_ptr(int mixed, int precond, bool big) {
     return big ? batch_kernel_ptr_t<512>(mixed, precond) : batch_kernel_ptr_t<256>(mixed, precond);
+}
+void* batch_cluster_ptr(int mixed, int precond) {
+    if (mixed)
+        return precond == KCFD_PREC_JACOBI ? (void*)batch_cluster_kernel<1, KCFD_PREC_JACOBI>
+                                           : (void*)batch_cluster_kernel<1, KCFD_PREC_NONE>;
+    return precond == KCFD_PREC_JACOBI ? (void*)batch_cluster_kernel<0, KCFD_PREC_JACOBI>
+                                       : (void*)batch_cluster_kernel<0, KCFD_PREC_NONE>;
+}
+cudaLaunchConfig_t cluster_config(int clusters, int csize, cudaStream_t st, cudaLaunchAttribute* at) {
+    cudaLaunchConfig_t cfg;
+    std::memset(&cfg, 0, sizeof(cfg));
+    cfg.gridDim = dim3(clusters * csize);
+    cfg.blockDim = dim3(512);
+    cfg.stream = st;
+    at[0].id = cudaLaunchAttributeClusterDimension;
+    at[0].val.clusterDim.x = csize;
+    at[0].val.clusterDim.y = 1;
+    at[0].val.clusterDim.z = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cfg;
 }
 }  // namespace
 
@@ -2045,32 +2129,59 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
     }
     b->n_total = ro;
     b->nnz_total = zo;
-    // largest first (longest-processing-time order for the dynamic queues); the
-    // systems of at least big_rows rows form the first tier
-    std::vector<int> order(nsys);
-    for (int s = 0; s < nsys; ++s) order[s] = s;
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nnz[x] > nnz[y]; });
-    const int big_rows = b->o.big_rows == 0 ? 16384 : b->o.big_rows;
-    std::stable_partition(order.begin(), order.end(), [&](int x) { return big_rows > 0 && n[x] >= big_rows; });
-    b->nbig = 0;
-    for (int s = 0; s < nsys; ++s) b->nbig += (big_rows > 0 && n[s] >= big_rows) ? 1 : 0;
+    // largest first (longest-processing-time order for the dynamic queues); systems of
+    // at least cluster_rows rows go to cluster teams, then those of at least big_rows
+    // rows to 512-thread CTAs, the rest to 256-thread CTAs
     const bool mixed = b->o.mode == KCFD_MODE_MIXED;
     const size_t vsz = mixed ? 4 : 8;
     int dev = 0, sms = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    std::vector<int> order(nsys);
+    for (int s = 0; s < nsys; ++s) order[s] = s;
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nnz[x] > nnz[y]; });
+    const int big_rows = b->o.big_rows == 0 ? 16384 : b->o.big_rows;
+    // defaults measured on 1,024 Delaunay p' systems of 2e3-2e5 rows (FP64, Jacobi):
+    // one CTA per system 74.3 systems/s; clusters of 4 from 131,072 rows 108.7 (of 8:
+    // 105.4; of 4 or 8 from 65,536 rows: 98.6, 92.2)
+    int cl_rows = b->o.cluster_rows == 0 ? 131072 : b->o.cluster_rows;
+    b->csize = b->o.cluster_size == 0 ? 4 : b->o.cluster_size;
+    if (b->csize < 2 || b->csize > 8) {
+        free_batch(b);
+        set_error("kcfd_batch_create: cluster_size must be 0 (default 4) or 2..8");
+        return KCFD_BAD_INPUT;
+    }
+    int ncl_max = 0;
+    if (cl_rows > 0) {
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = cluster_config(1, b->csize, nullptr, at);
+        if (cudaOccupancyMaxActiveClusters(&ncl_max, batch_cluster_ptr(mixed, b->o.precond), &cfg) != cudaSuccess)
+            ncl_max = 0;
+        cudaGetLastError();
+        if (ncl_max < 1) cl_rows = -1;  // no cluster can be resident: the big tier takes them
+    }
+    auto tier = [&](int x) { return (cl_rows > 0 && n[x] >= cl_rows) ? 0 : (big_rows > 0 && n[x] >= big_rows) ? 1 : 2; };
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tier(x) < tier(y); });
+    b->nhuge = b->nbig = 0;
+    for (int s = 0; s < nsys; ++s) {
+        b->nhuge += tier(s) == 0 ? 1 : 0;
+        b->nbig += tier(s) == 1 ? 1 : 0;
+    }
+    b->ncl = std::min(b->nhuge, ncl_max);
     int per_sm = 0, per_sm_big = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel_ptr(mixed, b->o.precond, false), 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_big, batch_kernel_ptr(mixed, b->o.precond, true), 512, 0);
-    const int nsmall = nsys - b->nbig;
+    const int nsmall = nsys - b->nbig - b->nhuge;
     b->grid = std::max(1, std::min(std::max(nsmall, 1), std::max(1, per_sm) * sms));
     b->grid_big = std::max(1, std::min(std::max(b->nbig, 1), std::max(1, per_sm_big) * sms));
     bool ok = cudaMalloc(&b->sys, nsys * sizeof(BatchSys)) == cudaSuccess &&
               cudaMemcpy(b->sys, sys.data(), nsys * sizeof(BatchSys), cudaMemcpyHostToDevice) == cudaSuccess &&
-              upload(&b->order, order) && cudaMalloc(&b->queue, 2 * sizeof(int)) == cudaSuccess &&
+              upload(&b->order, order) && cudaMalloc(&b->queue, 3 * sizeof(int)) == cudaSuccess &&
               cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
+              cudaStreamCreateWithFlags(&b->side2, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess &&
+              cudaEventCreateWithFlags(&b->ev_join2, cudaEventDisableTiming) == cudaSuccess &&
               cudaMalloc(&b->indptr, po * 4) == cudaSuccess &&
               cudaMemcpy(b->indptr, indptr_host, po * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMalloc(&b->indices, zo * 4) == cudaSuccess &&
@@ -2078,6 +2189,11 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
               cudaMalloc(&b->dinv, ro * vsz) == cudaSuccess && cudaMalloc(&b->lev, 2 * nsys * sizeof(int)) == cudaSuccess &&
               cudaMalloc(&b->work, 9 * ro * vsz) == cudaSuccess;
     if (ok && mixed) ok = cudaMalloc(&b->vals32, zo * 4) == cudaSuccess && cudaMalloc(&b->r64, ro * 8) == cudaSuccess;
+    if (ok && b->ncl > 0)
+        ok = cudaMalloc(&b->cbar, b->ncl * sizeof(unsigned int)) == cudaSuccess &&
+             cudaMalloc(&b->cslot, b->ncl * sizeof(int)) == cudaSuccess &&
+             cudaMalloc(&b->cpart, (size_t)b->ncl * kSlots * kMaxK * b->csize * sizeof(double)) == cudaSuccess &&
+             cudaMalloc(&b->cerr, sizeof(int)) == cudaSuccess;
     if (!ok) {
         free_batch(b);
         set_error("kcfd_batch_create: device allocation failed (%lld rows, %lld entries)", ro, zo);
@@ -2095,6 +2211,16 @@ int kcfd_batch_info(const kcfd_batch* b, int64_t* info) {
     info[1] = b->n_total;
     info[2] = b->nnz_total;
     info[3] = b->grid;
+    return KCFD_OK;
+}
+
+int kcfd_batch_tiers(const kcfd_batch* b, int32_t* tiers) {
+    KCFD_REQUIRE(b && tiers, "kcfd_batch_tiers: NULL argument");
+    tiers[0] = b->nhuge;
+    tiers[1] = b->nbig;
+    tiers[2] = b->nsys - b->nhuge - b->nbig;
+    tiers[3] = b->ncl;
+    tiers[4] = b->csize;
     return KCFD_OK;
 }
 
@@ -2131,31 +2257,57 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
     B.iters = iters;
     B.relres = relres;
     B.status = status;
-    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, 2 * sizeof(int), st));
+    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, 3 * sizeof(int), st));
+    if (b->ncl > 0) {
+        KCFD_CUDA(cudaMemsetAsync(b->cbar, 0, b->ncl * sizeof(unsigned int), st));
+        KCFD_CUDA(cudaMemsetAsync(b->cerr, 0, sizeof(int), st));
+    }
     B.nq = b->nsys;
     void* args[] = {&B};
     const int pgrid = std::max(1, std::min(b->nsys, 4 * b->grid));
     KCFD_CUDA(cudaLaunchKernel(B.mixed ? (void*)batch_prep_kernel<1> : (void*)batch_prep_kernel<0>, dim3(pgrid),
                                dim3(256), args, 0, st));
-    // big tier on the side stream, forked from and joined back into the caller's
-    BatchArgs Bb = B, Bs = B;
+    // cluster tier and big tier on side streams, forked from and joined back into the
+    // caller's; the cluster tier is launched first so that its clusters find free SMs
+    BatchArgs Bh = B, Bb = B, Bs = B;
+    Bh.queue = b->queue + 2;
+    Bh.nq = b->nhuge;
+    Bb.order = b->order + b->nhuge;
     Bb.nq = b->nbig;
-    Bs.order = b->order + b->nbig;
+    Bs.order = b->order + b->nhuge + b->nbig;
     Bs.queue = b->queue + 1;
-    Bs.nq = b->nsys - b->nbig;
+    Bs.nq = b->nsys - b->nhuge - b->nbig;
     void* args_b[] = {&Bb};
     void* args_s[] = {&Bs};
-    if (b->nbig > 0) {
+    if (b->nhuge > 0 || b->nbig > 0) {
         KCFD_CUDA(cudaEventRecord(b->ev_fork, st));
         KCFD_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+        KCFD_CUDA(cudaStreamWaitEvent(b->side2, b->ev_fork, 0));
+    }
+    if (b->nhuge > 0) {
+        ClusterCtl C;
+        C.bar = b->cbar;
+        C.slot = b->cslot;
+        C.partials = b->cpart;
+        C.err = b->cerr;
+        C.budget = 4000000000LL;  // ~2 s at 2 GHz per barrier wait
+        void* args_h[] = {&Bh, &C};
+        cudaLaunchAttribute at[1];
+        const cudaLaunchConfig_t cfg = cluster_config(b->ncl, b->csize, b->side2, at);
+        KCFD_CUDA(cudaLaunchKernelExC(&cfg, batch_cluster_ptr(B.mixed, B.precond), args_h));
+    }
+    if (b->nbig > 0)
         KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond, true), dim3(b->grid_big), dim3(512), args_b, 0,
                                    b->side));
-    }
     if (Bs.nq > 0)
         KCFD_CUDA(cudaLaunchKernel(batch_kernel_ptr(B.mixed, B.precond, false), dim3(b->grid), dim3(256), args_s, 0, st));
     if (b->nbig > 0) {
         KCFD_CUDA(cudaEventRecord(b->ev_join, b->side));
         KCFD_CUDA(cudaStreamWaitEvent(st, b->ev_join, 0));
+    }
+    if (b->nhuge > 0) {
+        KCFD_CUDA(cudaEventRecord(b->ev_join2, b->side2));
+        KCFD_CUDA(cudaStreamWaitEvent(st, b->ev_join2, 0));
     }
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;

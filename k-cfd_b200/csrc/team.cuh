@@ -5,7 +5,10 @@
 //  * GridTeam -- every CTA of a cooperative launch owns a contiguous row range of one
 //                system; phases are separated by a software grid barrier whose wait
 //                is bounded by a clock64 budget (on expiry the kernel records
-//                KCFD_TIMEOUT and returns; nothing spins forever).
+//                KCFD_TIMEOUT and returns; nothing spins forever). The same team
+//                over the CTAs of one thread-block cluster (ranks from cluster_ids()) gives a
+//                group whose members the hardware schedules together, with its own
+//                barrier counter and partials.
 //
 // Reductions are fixed-order: a fixed xor-shuffle tree inside each warp, a fixed
 // tree over warps, and (GridTeam) a fixed strided sum over CTA partials followed by
@@ -78,6 +81,7 @@ struct GridTeam {
     int rank, size;
     TeamCtl ctl;
     __device__ GridTeam(const TeamCtl& c) : rank(blockIdx.x), size(gridDim.x), ctl(c) {}
+    __device__ GridTeam(const TeamCtl& c, int r, int n) : rank(r), size(n), ctl(c) {}
 
     // Grid barrier on one 32-bit counter (zeroed before the launch): CTA 0 adds
     // 2^31 - (size - 1), every other CTA adds 1, so the top bit flips exactly when the
@@ -142,5 +146,17 @@ struct GridTeam {
         return true;
     }
 };
+
+// This CTA's rank in its thread-block cluster, the cluster's CTA count and its index
+// in the grid.
+__device__ __forceinline__ void cluster_ids(int& rank, int& size, int& id) {
+    unsigned r, n, c;
+    asm volatile("mov.u32 %0, %%cluster_ctarank;" : "=r"(r));
+    asm volatile("mov.u32 %0, %%cluster_nctarank;" : "=r"(n));
+    asm volatile("mov.u32 %0, %%clusterid.x;" : "=r"(c));
+    rank = (int)r;
+    size = (int)n;
+    id = (int)c;
+}
 
 }  // namespace kcfd

@@ -23,15 +23,21 @@ from . import _lib
 class BatchOpts(C.Structure):
     _fields_ = [("precond", C.c_int32), ("stop", C.c_int32), ("mode", C.c_int32), ("maxiter", C.c_int32),
                 ("lanes", C.c_int32), ("max_refine", C.c_int32), ("inner_maxiter", C.c_int32), ("big_rows", C.c_int32),
+                ("cluster_rows", C.c_int32), ("cluster_size", C.c_int32),
                 ("rtol", C.c_double), ("atol", C.c_double), ("inner_rtol", C.c_double)]
 
 
 class BatchSolver:
-    """patterns: list of (indptr, indices) host arrays (one per system)."""
+    """patterns: list of (indptr, indices) host arrays (one per system).
+
+    Tiers by system size: at least cluster_rows rows (0: 131072, negative: none) are
+    solved by a thread-block cluster of cluster_size CTAs (0: 4); at least big_rows
+    rows (0: 16384, negative: none) by one 512-thread CTA; the rest by one 256-thread
+    CTA. tiers() reports the split."""
 
     def __init__(self, patterns, mode="mixed", precond="jacobi", rtol=1e-8, atol=0.0, maxiter=20000, lanes=1,
                  inner_rtol=1e-3, inner_maxiter=400, max_refine=60, stop=_lib.STOP_SCIPY, big_rows=0,
-                 device="cuda"):
+                 cluster_rows=0, cluster_size=0, device="cuda"):
         torch = _lib.require_cuda()
         self.nsys = len(patterns)
         self.n = np.array([len(ip) - 1 for ip, _ in patterns], dtype=np.int32)
@@ -47,6 +53,7 @@ class BatchSolver:
         o.maxiter, o.lanes, o.max_refine, o.inner_maxiter = int(maxiter), int(lanes), int(max_refine), int(inner_maxiter)
         o.rtol, o.atol, o.inner_rtol = float(rtol), float(atol), float(inner_rtol)
         o.big_rows = int(big_rows)
+        o.cluster_rows, o.cluster_size = int(cluster_rows), int(cluster_size)
         h = C.c_void_p()
         _lib.check(_lib.lib().kcfd_batch_create(self.nsys, self.n.ctypes.data, self.nnz.ctypes.data, ip.ctypes.data,
                                                 ix.ctypes.data, C.byref(o), C.byref(h)), "kcfd_batch_create")
@@ -58,6 +65,12 @@ class BatchSolver:
         self.iters = torch.zeros(self.nsys, dtype=torch.int32, device=dev)
         self.relres = torch.zeros(self.nsys, dtype=torch.float64, device=dev)
         self.status = torch.zeros(self.nsys, dtype=torch.int32, device=dev)
+
+    def tiers(self):
+        """dict(cluster, big, small, clusters, cluster_size): systems per tier, clusters launched."""
+        v = np.zeros(5, dtype=np.int32)
+        _lib.check(_lib.lib().kcfd_batch_tiers(self._h, v.ctypes.data_as(_lib.P_i32)), "kcfd_batch_tiers")
+        return dict(zip(("cluster", "big", "small", "clusters", "cluster_size"), (int(t) for t in v)))
 
     def __del__(self):
         h = getattr(self, "_h", None)

@@ -5,7 +5,9 @@ Per system: the true FP64 relative residual meets rtol (1e-8 scaled by 1.5 for t
 recursive-vs-true gap) and the solution is within 1e-6 relative L2 of spsolve. A
 system's result is bitwise the same alone and in the batch (its CTA computes it with
 the same fixed-order reductions whatever else runs), and the FP64 batch equals the
-single-CTA solver handle bitwise.
+single-CTA solver handle bitwise. The cluster tier (systems solved by the CTAs of one
+thread-block cluster) meets the same residual and spsolve bounds, and its results are
+bitwise the same alone and in the batch too.
 """
 import numpy as np
 import pytest
@@ -77,3 +79,44 @@ def test_fp64_batch_equals_single_cta_handle(batch):
         xk = torch.zeros(d.n, dtype=torch.float64, device="cuda")
         s.solve(d, torch.from_numpy(rhs[k]).cuda(), xk)
         np.testing.assert_array_equal(xk.cpu().numpy(), xs[k])
+
+
+@pytest.mark.parametrize("mode,csize", [("fp64", 8), ("mixed", 8), ("fp64", 2)])
+def test_cluster_tier_solutions(batch, mode, csize):
+    import torch
+    from kcfd.batch import BatchSolver
+    pats, vals, rhs, sizes = batch
+    bs = BatchSolver(pats, mode=mode, precond="jacobi", rtol=1e-8, cluster_rows=2000, cluster_size=csize)
+    t = bs.tiers()
+    assert t["cluster_size"] == csize
+    assert t["cluster"] == int((bs.n >= 2000).sum()) > 0 and t["clusters"] >= 1
+    assert t["cluster"] + t["big"] + t["small"] == bs.nsys
+    v = torch.cat(vals)
+    b = bs.pack(rhs)
+    x = torch.zeros_like(b)
+    it, rr, st = bs.solve(v, b, x)
+    assert list(st.cpu().numpy()) == [0] * bs.nsys
+    xs = bs.unpack(x)
+    for k in range(bs.nsys):
+        A = _csr(pats[k], vals[k])
+        assert np.linalg.norm(rhs[k] - A @ xs[k]) / np.linalg.norm(rhs[k]) < 1.5e-8
+        xd = spla.spsolve(A.tocsc(), rhs[k])
+        assert np.linalg.norm(xs[k] - xd) / np.linalg.norm(xd) < 1e-6
+
+
+def test_cluster_tier_same_result_alone_and_in_the_batch(batch):
+    import torch
+    from kcfd.batch import BatchSolver
+    pats, vals, rhs, sizes = batch
+    full = BatchSolver(pats, mode="fp64", cluster_rows=2000)
+    x = torch.zeros(full.n_total, dtype=torch.float64, device="cuda")
+    full.solve(torch.cat(vals), full.pack(rhs), x)
+    xs = full.unpack(x)
+    big = [k for k in range(len(pats)) if len(pats[k][0]) - 1 >= 2000][:3]
+    assert big
+    for k in big:
+        one = BatchSolver([pats[k]], mode="fp64", cluster_rows=2000)
+        assert one.tiers()["cluster"] == 1
+        x1 = torch.zeros(one.n_total, dtype=torch.float64, device="cuda")
+        one.solve(vals[k], one.pack([rhs[k]]), x1)
+        np.testing.assert_array_equal(x1.cpu().numpy(), xs[k])

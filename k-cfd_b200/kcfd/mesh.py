@@ -27,6 +27,7 @@ class Mesh:
         self.area = self.normal = self.fcenter = None
         self.ccenter = self.volume = None
         self.face_nodes = self.cell_faces = None
+        self.nodes = self.cell_ptr = self.cell_nodes = None
         self.boundary_patches = {}
         self.indptr = self.indices = self.slot_on = self.slot_no = self.diag_slot = None
         self.face_color = self.cell_color = self.level_natural = None
@@ -107,6 +108,7 @@ def build_mesh(node_coords, cell_node_list, boundary_faces_dict, ndim=2, cell_fa
         m.n_cells, m.n_faces, m.n_internal_faces, m.n_boundary_faces = n, F, Fi, F - Fi
         m.n_int_colors, m.n_bnd_colors, m.n_cell_colors, m.n_levels = (int(v) for v in info[5:9])
         m.nodes = nodes
+        m.cell_ptr, m.cell_nodes = cell_ptr, cell_nodes   # cell -> node lists (CSR), for export
         m.owner = np.empty(F, np.int64); m.neighbour = np.empty(F, np.int64)
         m.face_nodes = np.empty((F, kfn), np.int64); m.cell_faces = np.empty((n, kcf), np.int64)
         m.area = np.empty(F); m.normal = np.empty((F, D)); m.fcenter = np.empty((F, D))

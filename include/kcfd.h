@@ -152,13 +152,22 @@ typedef struct {
     double  inner_rtol;  /* MIXED: inner FP32 solve reduction per refinement   */
     int32_t max_refine;  /* MIXED: refinement steps                            */
     int32_t inner_maxiter; /* MIXED: inner iterations per refinement step (0: 400) */
+    int32_t fill_level;  /* KCFD_PREC_ILU0 only: 0 ILU(0); k > 0 ILU(k), the
+                            level-of-fill factorisation (core/preconditioner.py:
+                            56-61 offers 'iluk' through SuperLU's threshold ILU;
+                            this is the structural form)                        */
 } kcfd_solver_opts_t;
 
 /* ILU(0) ordering: level_of_row_host gives each row's level (e.g. the mesh's cell
  * colouring, or natural-order dependency levels); NULL -> natural-order levels.
  * Coupled rows must lie on different levels. With ILU(0) the handle solves the
  * level-permuted system P A P^T (rows grouped by level), so every level is a
- * contiguous row range that all CTAs share evenly.                               */
+ * contiguous row range that all CTAs share evenly.
+ * ILU(k), fill_level = k > 0: the rows are ordered by a greedy distance-(k+1)
+ * colouring of A's (symmetrised) graph, which keeps every fill entry between rows of
+ * different colours, so the colours are the levels (level_of_row_host is not used);
+ * the factor's pattern (A's plus the fill of level <= k) is the handle's permuted
+ * matrix, with zeros in the fill slots, so its products are A's.                  */
 int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts,
                        const int32_t* level_of_row_host, kcfd_solver** out);
 void kcfd_solver_destroy(kcfd_solver* s);

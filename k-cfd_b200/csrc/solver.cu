@@ -1094,7 +1094,8 @@ __global__ void cast_kernel(int64_t m, const double* __restrict__ s, V* __restri
 __global__ void permute_vals_kernel(int64_t nnz, const int* __restrict__ src, const double* __restrict__ v,
                                     double* __restrict__ p64, float* __restrict__ p32) {
     for (int64_t k = blockIdx.x * (int64_t)blockDim.x + threadIdx.x; k < nnz; k += (int64_t)gridDim.x * blockDim.x) {
-        const double x = v[src[k]];
+        const int j = src[k];
+        const double x = j >= 0 ? v[j] : 0.0;  // ILU(k) fill slots hold zeros
         p64[k] = x;
         if (p32) p32[k] = (float)x;
     }
@@ -1175,6 +1176,7 @@ using namespace kcfd;
 struct kcfd_solver {
     kcfd_solver_opts_t o;
     int n = 0, nnz = 0;
+    int pnnz = 0;  // entries of the permuted matrix (ILU(k): A's plus the fill)
     int grid = 0, block = 256, team = 1, lanes = 8;
     int sm_count = 0;
     void* work = nullptr;
@@ -1265,6 +1267,55 @@ int free_solver(kcfd_solver* s) {
         if (p) cudaFree(p);
     delete s;
     return KCFD_OK;
+}
+
+// Greedy distance-d colouring of A's symmetrised graph, rows in index order: each row
+// takes the smallest colour not used by any row within d edges of it. With d = k + 1
+// no ILU(k) fill entry joins two rows of one colour (a level-l fill entry (i, j)
+// closes a path of l + 1 edges from i to j through earlier rows).
+std::vector<int> distance_colouring(int n, const std::vector<int>& ip, const std::vector<int>& ix, int d) {
+    std::vector<int> deg(n + 1, 0);
+    for (int i = 0; i < n; ++i)
+        for (int k = ip[i]; k < ip[i + 1]; ++k)
+            if (ix[k] != i) {
+                deg[i + 1]++;
+                deg[ix[k] + 1]++;
+            }
+    for (int i = 0; i < n; ++i) deg[i + 1] += deg[i];
+    std::vector<int> adj(deg[n]), fill(deg.begin(), deg.end() - 1);
+    for (int i = 0; i < n; ++i)
+        for (int k = ip[i]; k < ip[i + 1]; ++k)
+            if (ix[k] != i) {
+                adj[fill[i]++] = ix[k];
+                adj[fill[ix[k]]++] = i;
+            }
+    std::vector<int> colour(n, -1), seen(n, -1), used;
+    std::vector<int> front, next;
+    for (int v = 0; v < n; ++v) {
+        seen[v] = v;
+        front.assign(1, v);
+        std::vector<int> near;
+        for (int depth = 0; depth < d && !front.empty(); ++depth) {
+            next.clear();
+            for (int u : front)
+                for (int e = deg[u]; e < deg[u + 1]; ++e) {
+                    const int w = adj[e];
+                    if (seen[w] == v) continue;
+                    seen[w] = v;
+                    next.push_back(w);
+                    if (colour[w] >= 0) near.push_back(colour[w]);
+                }
+            front.swap(next);
+        }
+        int c = 0;
+        std::sort(near.begin(), near.end());
+        for (int x : near) {
+            if (x == c) ++c;
+            else if (x > c) break;
+        }
+        colour[v] = c;
+    }
+    return colour;
 }
 
 SolveArgs make_args(const kcfd_solver* s, const kcfd_csr_t* A) {
@@ -1787,9 +1838,13 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     // levels
     std::vector<int> lptr;
     std::vector<int> pip, pix, psrc, pdiag;  // ILU: the level-permuted CSR (host copy)
+    const int K = opts->precond == KCFD_PREC_ILU0 ? std::max(0, opts->fill_level) : 0;
+    if (opts->fill_level < 0) return fail("kcfd_solver_create: fill_level < 0");
     if (opts->precond == KCFD_PREC_ILU0) {
         std::vector<int> lev(n, 0);
-        if (level_of_row_host) {
+        if (K > 0) {
+            lev = distance_colouring(n, ip, ix, K + 1);
+        } else if (level_of_row_host) {
             for (int i = 0; i < n; ++i) lev[i] = level_of_row_host[i];
         } else {
             for (int i = 0; i < n; ++i)
@@ -1811,35 +1866,73 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
             inv[i] = fill[lev[i]]++;
         }
         pip.assign(n + 1, 0);
-        pix.assign(nnz, 0);
-        psrc.assign(nnz, 0);
+        pix.clear();
+        psrc.clear();
         pdiag.assign(n, -1);
-        std::vector<std::pair<int, int>> row;
+        pix.reserve(nnz);
+        psrc.reserve(nnz);
+        std::vector<int> plev;                     // ILU(k): level of fill of each entry
+        std::vector<std::pair<int, int>> row;      // (permuted column, caller slot)
+        std::vector<int> cc, cl, cs;               // the row being built: column, level, slot
         for (int r = 0; r < n; ++r) {
             const int o = perm[r];
-            const int len = ip[o + 1] - ip[o];
-            if (len > kMaxIluRow) return fail("kcfd_solver_create: ILU(0) row %d has %d entries (max %d)", o, len, kMaxIluRow);
-            pip[r + 1] = pip[r] + len;
             row.clear();
             for (int k = ip[o]; k < ip[o + 1]; ++k) row.emplace_back(inv[ix[k]], k);
             std::sort(row.begin(), row.end());
+            cc.clear();
+            cl.clear();
+            cs.clear();
+            for (const auto& e : row) {
+                cc.push_back(e.first);
+                cl.push_back(0);
+                cs.push_back(e.second);
+            }
+            if (K > 0) {
+                // symbolic ILU(k): eliminate with every earlier row k of the factor
+                // pattern (in column order, fill included); entry j of row k's upper
+                // part gives fill level lev(r,k) + lev(k,j) + 1, kept when <= K
+                for (size_t q = 0; q < cc.size() && cc[q] < r; ++q) {
+                    const int kr = cc[q], lk = cl[q];
+                    for (int e = pdiag[kr] + 1; e < pip[kr + 1]; ++e) {
+                        const int nl = lk + plev[e] + 1;
+                        if (nl > K) continue;
+                        const int j = pix[e];
+                        const auto it = std::lower_bound(cc.begin(), cc.end(), j);
+                        const size_t at = it - cc.begin();
+                        if (it != cc.end() && *it == j) {
+                            cl[at] = std::min(cl[at], nl);
+                        } else {
+                            cc.insert(it, j);
+                            cl.insert(cl.begin() + at, nl);
+                            cs.insert(cs.begin() + at, -1);
+                        }
+                    }
+                }
+            }
+            const int len = (int)cc.size();
+            if (len > kMaxIluRow)
+                return fail("kcfd_solver_create: ILU row %d has %d entries (max %d)", o, len, kMaxIluRow);
+            pip[r + 1] = pip[r] + len;
             for (int q = 0; q < len; ++q) {
-                const int c = row[q].first;
-                pix[pip[r] + q] = c;
-                psrc[pip[r] + q] = row[q].second;
+                const int c = cc[q];
+                pix.push_back(c);
+                psrc.push_back(cs[q]);
+                plev.push_back(cl[q]);
                 if (c == r) pdiag[r] = pip[r] + q;
                 else if (lev[perm[c]] == lev[o]) return fail("kcfd_solver_create: coupled rows %d, %d share level %d", o, perm[c], lev[o]);
             }
-            if (pdiag[r] < 0) return fail("kcfd_solver_create: row %d has no diagonal entry (ILU(0) needs it)", o);
+            if (pdiag[r] < 0) return fail("kcfd_solver_create: row %d has no diagonal entry (ILU needs it)", o);
         }
+        s->pnnz = pip[n];
         s->nlev = nlev;
         bool ok = upload(&s->perm, perm) && upload(&s->p_indptr, pip) && upload(&s->p_indices, pix) &&
                   upload(&s->p_src, psrc) && upload(&s->p_diag, pdiag);
-        ok = ok && cudaMalloc(&s->p_vals64, (size_t)nnz * sizeof(double)) == cudaSuccess;
-        if (mixed) ok = ok && cudaMalloc(&s->p_vals32, (size_t)nnz * sizeof(float)) == cudaSuccess;
+        const size_t pn = (size_t)s->pnnz;
+        ok = ok && cudaMalloc(&s->p_vals64, pn * sizeof(double)) == cudaSuccess;
+        if (mixed) ok = ok && cudaMalloc(&s->p_vals32, pn * sizeof(float)) == cudaSuccess;
         ok = ok && cudaMalloc(&s->px, (size_t)n * nrhs * sizeof(double)) == cudaSuccess;
         ok = ok && cudaMalloc(&s->pb, (size_t)n * nrhs * sizeof(double)) == cudaSuccess;
-        ok = ok && cudaMalloc(&s->lu, (size_t)nnz * vsz) == cudaSuccess;
+        ok = ok && cudaMalloc(&s->lu, pn * vsz) == cudaSuccess;
         ok = ok && cudaMalloc(&s->ludinv, (size_t)n * vsz) == cudaSuccess;
         if (!ok) {
             free_solver(s);
@@ -1934,8 +2027,8 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
             jacobi_setup_kernel<double><<<blocks, threads, 0, st>>>(s->n, A->indptr, A->indices, A->vals64, (double*)s->dinv);
         KCFD_CUDA(cudaGetLastError());
     } else if (s->o.precond == KCFD_PREC_ILU0) {
-        const int blocks = (int)std::min<int64_t>(((int64_t)s->nnz + threads - 1) / threads, s->sm_count * 16);
-        permute_vals_kernel<<<blocks, threads, 0, st>>>(s->nnz, s->p_src, A->vals64, s->p_vals64, nullptr);
+        const int blocks = (int)std::min<int64_t>(((int64_t)s->pnnz + threads - 1) / threads, s->sm_count * 16);
+        permute_vals_kernel<<<blocks, threads, 0, st>>>(s->pnnz, s->p_src, A->vals64, s->p_vals64, nullptr);
         if (mixed) rowsum_f32_kernel<<<rblocks, threads, 0, st>>>(s->n, s->p_indptr, s->p_indices, s->p_vals64, s->p_vals32);
         KCFD_CUDA(cudaGetLastError());
         SolveArgs a = make_args(s, A);

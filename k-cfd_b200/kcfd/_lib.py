@@ -41,7 +41,7 @@ class Csr(C.Structure):
 class SolverOpts(C.Structure):
     _fields_ = [("precond", i32), ("stop", i32), ("mode", i32), ("nrhs", i32), ("maxiter", i32), ("team", i32),
                 ("lanes", i32), ("block", i32), ("rtol", f64), ("atol", f64), ("inner_rtol", f64),
-                ("max_refine", i32), ("inner_maxiter", i32)]
+                ("max_refine", i32), ("inner_maxiter", i32), ("fill_level", i32)]
 
 
 class TfParams(C.Structure):

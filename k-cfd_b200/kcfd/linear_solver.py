@@ -10,7 +10,10 @@ device failure raises instead of falling back to the CPU. Semantics kept:
     starts from zero; non-convergence prints and returns x (:60-61).
   * preconditioner: 'none' | 'jacobi' (1/d where |d| > 1e-30, :43-47) | 'ilu0'
     (structural, level-scheduled ILU(0); the reference's 'ilu0' is SuperLU spilu,
-    so agreement with it is at the solution level) | 'amg' (falls back to 'ilu0' as
+    so agreement with it is at the solution level) | 'iluk' (structural ILU(k),
+    fill_level=k, default 1, on a distance-(k+1) colouring; the reference's 'iluk'
+    is SuperLU's threshold ILU with fill_factor=3 (:56-61), so agreement is again at
+    the solution level and fill_factor is not used) | 'amg' (falls back to 'ilu0' as
     the reference does without pyamg, :63-66).
   * method='direct': the device has no sparse LU; BiCGSTAB + ILU(0) to a relative
     residual of 1e-12 stands in for spsolve (documented difference).
@@ -37,17 +40,20 @@ def create_preconditioner(A_csr, method="none", **kwargs):
     if method == "amg":
         print("  [Preconditioner] amg not built on the device path; using ILU(0).")
         return create_preconditioner(A_csr, "ilu0")
+    fill = 0
+    name = method
     if method == "iluk":
-        raise NotImplementedError("iluk is not on the kcfd device path (use 'ilu0')")
+        fill = int(kwargs.get("fill_level", 1))
+        method, name = "ilu0", f"iluk(level={fill})"
     if method not in _lib.PREC:
         raise ValueError(f"Unknown preconditioner: {method}")
     if method == "none":
         return None, {"method": "none", "setup_time": 0.0}
     d = DeviceCSR.from_scipy(A_csr) if not isinstance(A_csr, DeviceCSR) else A_csr
-    s = Solver(d, precond=method, levels=kwargs.get("levels"))
+    s = Solver(d, precond=method, levels=None if fill else kwargs.get("levels"), fill_level=fill)
     s.setup(d)
     _lib.require_cuda().cuda.synchronize()
-    return {"method": method, "solver": s, "csr": d}, {"method": method, "setup_time": time.time() - t0}
+    return {"method": name, "solver": s, "csr": d}, {"method": name, "setup_time": time.time() - t0}
 
 
 def _as_device(system):
@@ -68,6 +74,7 @@ def solve_linear_system(system, x0=None, method="direct", tol=1e-8, maxiter=1000
     rtol = precond_kwargs.pop("rtol", SCIPY_DEFAULT_RTOL)
     d, b, levels = _as_device(system)
     levels = precond_kwargs.pop("levels", levels)
+    fill = 0
     n = d.n
     if method == "direct":
         prec, atol, rtol_eff, its = "ilu0", 0.0, DIRECT_RTOL, max(maxiter, 20 * n)
@@ -76,14 +83,16 @@ def solve_linear_system(system, x0=None, method="direct", tol=1e-8, maxiter=1000
         if prec == "amg":
             prec = "ilu0"
         if prec == "iluk":
-            raise NotImplementedError("iluk is not on the kcfd device path (use 'ilu0')")
+            prec, fill, levels = "ilu0", int(precond_kwargs.pop("fill_level", 1)), None
+            precond_kwargs.pop("fill_factor", None)
     elif method == "gmres":
         raise NotImplementedError("gmres is not on the kcfd device path (use 'bicgstab')")
     else:
         raise ValueError(f"Unknown solver method: {method}")
     x = torch.zeros(n, dtype=torch.float64, device=b.device) if x0 is None else \
         torch.from_numpy(np.array(x0, dtype=np.float64)).to(b.device)
-    s = Solver(d, precond=prec, stop=_lib.STOP_SCIPY, maxiter=its, rtol=rtol_eff, atol=atol, levels=levels)
+    s = Solver(d, precond=prec, stop=_lib.STOP_SCIPY, maxiter=its, rtol=rtol_eff, atol=atol, levels=levels,
+               fill_level=fill)
     s.setup(d)
     it, rr, st = s.solve(d, b, x)
     status = int(st[0])

@@ -80,12 +80,13 @@ class Solver:
     mode: _lib.MODE_FP64 | _lib.MODE_MIXED; nrhs: 1 or 3; team: 0 auto, 1 one CTA,
     2 whole grid (persistent cooperative kernel), 3 graph engine (phase kernels in a
     CUDA graph with a device-side WHILE loop; FP64 only); levels: ILU(0) level of each row (e.g. mesh.cell_color), None for
-    natural-order levels.
+    natural-order levels. fill_level k > 0 with precond 'ilu0' gives ILU(k): rows ordered by a distance-(k+1)
+    colouring of the matrix graph (levels is then not used), the factor on A's pattern plus the fill of level <= k.
     """
 
     def __init__(self, csr, precond="jacobi", stop=_lib.STOP_SCIPY, mode=_lib.MODE_FP64, nrhs=1, maxiter=1000,
                  rtol=1e-8, atol=0.0, team=0, lanes=0, block=0, inner_rtol=1e-3, max_refine=60, levels=None,
-                 inner_maxiter=400):
+                 inner_maxiter=400, fill_level=0):
         torch = _lib.require_cuda()
         if precond not in _lib.PREC:
             raise ValueError(f"Unknown preconditioner: {precond}")
@@ -94,6 +95,7 @@ class Solver:
         o.team, o.lanes, o.block = team, lanes, block
         o.rtol, o.atol, o.inner_rtol, o.max_refine = float(rtol), float(atol), float(inner_rtol), int(max_refine)
         o.inner_maxiter = int(inner_maxiter)
+        o.fill_level = int(fill_level)
         self.opts = o
         self.n, self.nrhs, self.mode = csr.n, nrhs, mode
         self.precond = precond

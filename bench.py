@@ -235,15 +235,15 @@ def p_solve_roofline(s, peak, reps=3):
     sb = nnz * 12 + 4 * (n + 1) + 16 * n
     spmv = {"kernel": "spmv_row_kernel<double> (kcfd_spmv_f64, row per thread, entries loaded before the x gathers)", "bytes": int(sb), "launch_us": round(ts * 1e6, 2),
             "achieved": round(sb / ts / 1e9, 1), "frac": round(sb / ts / 1e9 / peak[0], 3)}
-    # bytes the engine actually moves: on ILU level 0 the SpMV phases copy q instead of
-    # multiplying (A M^-1 q = q there), so two SpMVs skip those rows' values, columns
-    # and row pointers
+    # bytes the engine actually moves: on ILU level 0 A M^-1 q = q, so two SpMVs skip
+    # those rows' values, columns and row pointers, and v = p, t = s there are neither
+    # stored nor read back (g_p, g_s and g_xr read p and s in their place)
     moved = None
     if info["team"] == 3 and info["levels"] >= 2:
         lev = np.asarray(s.mesh.cell_color)
         rl = np.diff(np.asarray(s.mesh.indptr))
         n0, nnz0 = int((lev == 0).sum()), int(rl[lev == 0].sum())
-        per_it = solver_bytes(n, nnz, 1, "ilu0", w) - 2 * (nnz0 * (w + 4) + 4 * n0)
+        per_it = solver_bytes(n, nnz, 1, "ilu0", w) - 2 * (nnz0 * (w + 4) + 4 * n0) - 4 * n0 * w
         moved = {"bytes_per_krylov_iter": int(per_it), "achieved": round(per_it * it / t / 1e9, 1),
                  "frac": round(per_it * it / t / 1e9 / peak[0], 3)}
     return {"bound": "hbm", "kernel": kern, "unit_of_work": "one p' solve (Krylov iterations x bytes/iteration)",

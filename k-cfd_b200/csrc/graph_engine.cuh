@@ -196,6 +196,38 @@ __device__ __forceinline__ void sell_gather(const Sell& m, int base, int w, cons
     }
 }
 
+// The forward sweep's gather: acc -= sum_k val y[col], where y = q on the level-0
+// rows (col < n0: the sweep's input, never copied) and z elsewhere; row order kept.
+template <int NRHS>
+__device__ __forceinline__ void sell_gather_fwd(const Sell& m, int base, int w, const double* z, const double* q,
+                                                int n0, double (&acc)[NRHS]) {
+    constexpr int B = NRHS == 1 ? 8 : 4;
+    for (int k0 = 0; k0 < w; k0 += B) {
+        int jj[B];
+        double vv[B];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const bool in = k0 + u < w;
+            const int slot = base + (k0 + u) * 32;
+            jj[u] = in ? __ldg(m.col + slot) : -1;
+            vv[u] = in ? __ldg(m.val + slot) : 0.0;
+        }
+        double xv[B][NRHS];
+#pragma unroll
+        for (int u = 0; u < B; ++u) {
+            const double* y = jj[u] < n0 ? q : z;
+#pragma unroll
+            for (int c = 0; c < NRHS; ++c) xv[u][c] = jj[u] >= 0 ? y[(size_t)jj[u] * NRHS + c] : 0.0;
+        }
+#pragma unroll
+        for (int u = 0; u < B; ++u)
+            if (jj[u] >= 0) {
+#pragma unroll
+                for (int c = 0; c < NRHS; ++c) acc[c] -= vv[u] * xv[u][c];
+            }
+    }
+}
+
 // SELL values from a source array: out[k] = in[src[k]], 0 for padding.
 __global__ void g_fill(int64_t m, const int* __restrict__ src, const double* __restrict__ in, double* __restrict__ out) {
     for (int64_t k = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; k < m; k += (int64_t)gridDim.x * blockDim.x) {
@@ -208,8 +240,10 @@ __global__ void g_fill(int64_t m, const int* __restrict__ src, const double* __r
 // entries, so their factor rows are A's rows (u_ij = a_ij, u_ii = a_ii), and the
 // backward sweep sets z_i = (q_i - sum_j a_ij z_j) / a_ii, so that
 // a_ii z_i + sum_j a_ij z_j = q_i whatever the other levels hold. The SpMV kernels
-// therefore copy q there and multiply only the rows of the later levels (read from
+// therefore take q there and multiply only the rows of the later levels (read from
 // the first slice boundary at or below the level-1 start, so warps stay on slices).
+// Nothing is stored for those rows: v = p and t = s there, so g_p and g_s read p and
+// g_xr reads s in their place (the same values, bit for bit).
 // Returns the first row the SpMV loop must treat (0 without the identity).
 template <int PREC>
 __device__ __forceinline__ int level0_rows(const Args& a) {
@@ -273,7 +307,8 @@ __global__ void __launch_bounds__(kBlock) g_init(Args a) {
 }
 
 // p = r + beta (p - omega v) (scipy / GPU-path forms); phat = M^-1 p for Jacobi, or
-// the level-0 rows of the ILU forward sweep (phat = p there).
+// phat = p for a single-level ILU (with more levels the sweeps read p itself on
+// level 0).
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_p(Args a) {
     pdl_enter();
@@ -283,8 +318,7 @@ __global__ void __launch_bounds__(kBlock) g_p(Args a) {
     constexpr int U = Ilp<NRHS>::U;
     const bool gpu = a.stop == KCFD_STOP_GPU;
     const int it = S.it;
-    int l0a = 0, l0b = a.n;
-    if (PREC == KCFD_PREC_ILU0) level_range(a, 0, l0a, l0b);
+    const int n0 = level0_rows<PREC>(a);
     double om[NRHS], be[NRHS];
     int dn[NRHS];
 #pragma unroll
@@ -306,7 +340,8 @@ __global__ void __launch_bounds__(kBlock) g_p(Args a) {
                     const size_t q = (size_t)i * NRHS + c;
                     R[u][c] = a.r[q];
                     P[u][c] = a.p[q];
-                    V[u][c] = a.v[q];
+                    // level-0 rows: v = A M^-1 p = p (never stored there)
+                    V[u][c] = (i < n0) ? P[u][c] : a.v[q];
                 }
             }
         }
@@ -324,7 +359,7 @@ __global__ void __launch_bounds__(kBlock) g_p(Args a) {
                 else pn = (P[u][c] - om[c] * V[u][c]) * be[c] + R[u][c];
                 a.p[q] = pn;
                 if (PREC == KCFD_PREC_JACOBI) a.ph[q] = D[u] * pn;
-                if (PREC == KCFD_PREC_ILU0 && i >= l0a && i < l0b) a.ph[q] = pn;
+                if (PREC == KCFD_PREC_ILU0 && a.nlev == 1) a.ph[q] = pn;  // more levels: the sweeps read p
             }
         }
     }
@@ -339,6 +374,7 @@ __global__ void __launch_bounds__(kBlock) g_fwd(Args a, int l, int which) {
     if (!S.active) return;
     const double* q = which ? a.r : a.p;
     double* z = which ? a.sh : a.ph;
+    const int n0 = level0_rows<KCFD_PREC_ILU0>(a);  // y = q there (not copied into z)
     int dn[NRHS];
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) dn[c] = which ? (S.done[c] || S.sconv[c]) : S.done[c];
@@ -354,7 +390,7 @@ __global__ void __launch_bounds__(kBlock) g_fwd(Args a, int l, int which) {
         for (int c = 0; c < NRHS; ++c) acc[c] = q[(size_t)i * NRHS + c];
         int base, w;
         sell_row(a.L, i, base, w);
-        sell_gather<NRHS, true>(a.L, base, w, z, acc);
+        sell_gather_fwd<NRHS>(a.L, base, w, z, q, n0, acc);
 #pragma unroll
         for (int c = 0; c < NRHS; ++c)
             if (!dn[c]) z[(size_t)i * NRHS + c] = acc[c] * di;
@@ -369,6 +405,8 @@ __global__ void __launch_bounds__(kBlock) g_bwd(Args a, int l, int which) {
     const St& S = *a.st;
     if (!S.active) return;
     double* z = which ? a.sh : a.ph;
+    // level 0 of a multi-level factor starts from q (y = q there, not copied into z)
+    const double* y = (l == 0 && a.nlev >= 2) ? (which ? a.r : a.p) : z;
     int dn[NRHS];
 #pragma unroll
     for (int c = 0; c < NRHS; ++c) dn[c] = which ? (S.done[c] || S.sconv[c]) : S.done[c];
@@ -379,7 +417,7 @@ __global__ void __launch_bounds__(kBlock) g_bwd(Args a, int l, int which) {
         const double di = __ldg(a.ldi + i);
         double acc[NRHS];
 #pragma unroll
-        for (int c = 0; c < NRHS; ++c) acc[c] = z[(size_t)i * NRHS + c];
+        for (int c = 0; c < NRHS; ++c) acc[c] = y[(size_t)i * NRHS + c];
         int base, w;
         sell_row(a.U, i, base, w);
         sell_gather<NRHS, true>(a.U, base, w, z, acc);
@@ -401,9 +439,8 @@ __global__ void __launch_bounds__(kBlock) g_spmv_v(Args a) {
     const int n0 = level0_rows<PREC>(a);
     const int stride = gridDim.x * blockDim.x;
     for (int q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < n0 * NRHS; q0 += stride) {
-        const double vv = a.p[q0];
-        a.v[q0] = vv;
-        red[q0 % NRHS] += a.rh[q0] * vv;
+        // v = p on level 0: only its dot with rhat; readers take p there
+        red[q0 % NRHS] += a.rh[q0] * a.p[q0];
     }
     for (int i = (n0 & ~31) + blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += stride) {
         if (i < n0) continue;
@@ -437,15 +474,15 @@ __global__ void __launch_bounds__(kBlock) g_spmv_v(Args a) {
     }
 }
 
-// s = r - alpha v (in r); shat = M^-1 s for Jacobi / level-0 copy for ILU; ||s||.
+// s = r - alpha v (in r); shat = M^-1 s for Jacobi, shat = s for a single-level ILU
+// (with more levels the sweeps read s itself on level 0); ||s||.
 template <int NRHS, int PREC>
 __global__ void __launch_bounds__(kBlock) g_s(Args a) {
     pdl_enter();
     St& S = *a.st;
     if (!S.active) return;
     constexpr int U = Ilp<NRHS>::U;
-    int l0a = 0, l0b = a.n;
-    if (PREC == KCFD_PREC_ILU0) level_range(a, 0, l0a, l0b);
+    const int n0 = level0_rows<PREC>(a);
     double al[NRHS];
     int dn[NRHS];
 #pragma unroll
@@ -468,7 +505,7 @@ __global__ void __launch_bounds__(kBlock) g_s(Args a) {
                 for (int c = 0; c < NRHS; ++c) {
                     const size_t q = (size_t)i * NRHS + c;
                     R[u][c] = a.r[q];
-                    V[u][c] = a.v[q];
+                    V[u][c] = (i < n0) ? a.p[q] : a.v[q];  // v = p on level 0
                 }
             }
         }
@@ -483,7 +520,7 @@ __global__ void __launch_bounds__(kBlock) g_s(Args a) {
                 const double sv = R[u][c] - al[c] * V[u][c];
                 a.r[q] = sv;
                 if (PREC == KCFD_PREC_JACOBI) a.sh[q] = D[u] * sv;
-                if (PREC == KCFD_PREC_ILU0 && i >= l0a && i < l0b) a.sh[q] = sv;
+                if (PREC == KCFD_PREC_ILU0 && a.nlev == 1) a.sh[q] = sv;  // more levels: the sweeps read s
                 red[c] += sv * sv;
             }
         }
@@ -549,8 +586,7 @@ __global__ void __launch_bounds__(kBlock) g_spmv_t(Args a) {
         for (int q0 = blockIdx.x * blockDim.x + threadIdx.x; q0 < n0 * NRHS; q0 += stride) {
             const int c = q0 % NRHS;
             if (dn[c]) continue;
-            const double tv = a.r[q0];  // t = s on level 0
-            a.t[q0] = tv;
+            const double tv = a.r[q0];  // t = s on level 0 (not stored; g_xr takes s there)
             red[c] += tv * tv;
             red[NRHS + c] += tv * tv;
         }
@@ -611,6 +647,7 @@ __global__ void __launch_bounds__(kBlock) g_xr(Args a) {
 #pragma unroll
     for (int k = 0; k < 2 * NRHS; ++k) red[k] = 0.0;
     const int stride = gridDim.x * blockDim.x;
+    const int n0 = level0_rows<PREC>(a);
     for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += U * stride) {
         double X[U][NRHS], HP[U][NRHS], HS[U][NRHS], R[U][NRHS], T[U][NRHS], RH[U][NRHS];
 #pragma unroll
@@ -624,7 +661,7 @@ __global__ void __launch_bounds__(kBlock) g_xr(Args a) {
                     HP[u][c] = ph[q];
                     HS[u][c] = sh[q];
                     R[u][c] = a.r[q];
-                    T[u][c] = a.t[q];
+                    T[u][c] = (i < n0) ? R[u][c] : a.t[q];  // t = s on level 0
                     RH[u][c] = a.rh[q];
                 }
             }

@@ -126,7 +126,7 @@ def measured_peak():
 # of one p' Krylov iteration on the 128^3 cavity, from one ncu capture of the graph
 # engine (profiles/graph_engine_p_solve_cavity128.md); the roofline's traffic is this
 # times the solve's Krylov count (the kernels and their sizes repeat every iteration).
-NCU_P_ITER_DRAM_BYTES_128 = 890082048
+NCU_P_ITER_DRAM_BYTES_128 = 857019136
 
 
 def solver_bytes(n, nnz, iters, precond, w, nrhs=1):

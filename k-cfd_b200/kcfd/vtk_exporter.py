@@ -66,17 +66,18 @@ def vtu_blocks(mesh):
     nodes, ptr, _ = _cell_lists(mesh)
     k = np.diff(ptr)
     nd = 2 if (getattr(mesh, "ndim", 2) == 2 or nodes.shape[1] == 2) else 3
-    names, codes = [], []
-    for kk in k:
-        nm, code = _cell_type(int(kk), nd)
-        names.append(nm)
-        codes.append(code)
-    first = {}
-    for i, nm in enumerate(names):
-        first.setdefault(nm, len(first))
-    rank = np.fromiter((first[nm] for nm in names), dtype=np.int64, count=len(names))
-    order = np.argsort(rank, kind="stable")
-    return order, np.asarray(codes, dtype=np.uint8)[order]
+    counts = np.unique(k)
+    code_of = {int(c): _cell_type(int(c), nd)[1] for c in counts}
+    codes = np.zeros(len(k), dtype=np.uint8)
+    for c, code in code_of.items():
+        codes[k == c] = code
+    # blocks in order of each type's first appearance (node counts sharing a type,
+    # such as 2D polygons, share a block)
+    uniq, first_idx = np.unique(codes, return_index=True)
+    rank_of = np.empty(256, dtype=np.int64)
+    rank_of[uniq[np.argsort(first_idx)]] = np.arange(len(uniq))
+    order = np.argsort(rank_of[codes], kind="stable")
+    return order, codes[order]
 
 
 def _encode(arr, ascii):
@@ -106,8 +107,12 @@ def export_mesh_to_vtu(mesh, filepath: str, cell_data: dict = None, ascii: bool 
     pts[:, : min(3, nodes.shape[1])] = nodes[:, :3]
     order, codes = vtu_blocks(mesh)
     lens = np.diff(ptr)[order]
-    conn = np.concatenate([cn[ptr[c]:ptr[c + 1]] for c in order]) if len(order) else np.zeros(0, np.int64)
     offsets = np.cumsum(lens).astype(np.int64)
+    # gather each written cell's node run: entry e of the output sits at
+    # ptr[order[c]] + (e - start of c in the output)
+    starts_out = offsets - lens
+    idx = np.repeat(ptr[:-1][order] - starts_out, lens) + np.arange(int(offsets[-1]) if len(offsets) else 0)
+    conn = cn[idx]
     n = len(ptr) - 1
     out = ['<?xml version="1.0"?>',
            '<VTKFile type="UnstructuredGrid" version="1.0" byte_order="LittleEndian" header_type="UInt64">',

@@ -336,18 +336,47 @@ def make_two_fluid(out, meshes):
     np.savez_compressed(os.path.join(out, "two_fluid.npz"), **d)
 
 
+def make_partitions(out, meshes):
+    """parallel/partitioning.py: RCB part ids and ghost maps of the fixture meshes for
+    2-5 parts (the cavity mesh's uniform centres exercise the median ties)."""
+    from parallel.partitioning import GeometricPartitioner, GhostCellLayer
+    for name, m in meshes.items():
+        d = {}
+        for n_parts in (2, 3, 4, 5):
+            part = GeometricPartitioner(m).partition(n_parts)
+            d[f"part{n_parts}"] = np.asarray(part, dtype=np.int64)
+            g = GhostCellLayer(m, part)
+            trip = [(r, q, c) for r in sorted(g.ghost_map) for q in sorted(g.ghost_map[r])
+                    for c in g.ghost_map[r][q]]
+            d[f"ghost{n_parts}"] = np.asarray(trip, dtype=np.int64).reshape(-1, 3)
+        np.savez_compressed(os.path.join(out, f"part_{name}.npz"), **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
     ap.add_argument("--out", default=HERE)
+    ap.add_argument("--only", default="", help="comma list of fixture groups to write (default: all)")
     a = ap.parse_args()
     _install_stubs()
     sys.path.insert(0, a.ref)
-    meshes = make_meshes(a.out)
-    make_operators(a.out, meshes)
-    make_solvers(a.out)
-    make_simple(a.out)
-    make_two_fluid(a.out, meshes)
+    only = set(x for x in a.only.split(",") if x)
+    want = lambda g: not only or g in only
+    if only and "meshes" not in only:
+        import tempfile
+        meshes = make_meshes(tempfile.mkdtemp())  # rebuilt for the other groups, not rewritten
+    else:
+        meshes = make_meshes(a.out)
+    if want("operators"):
+        make_operators(a.out, meshes)
+    if want("solvers"):
+        make_solvers(a.out)
+    if want("simple"):
+        make_simple(a.out)
+    if want("two_fluid"):
+        make_two_fluid(a.out, meshes)
+    if want("partitions"):
+        make_partitions(a.out, meshes)
     print("golden fixtures written to", a.out)
 
 

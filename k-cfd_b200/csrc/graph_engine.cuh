@@ -631,7 +631,9 @@ __global__ void __launch_bounds__(kBlock) g_xr(Args a) {
     // unconditional bound on the loop, whatever the state logic does
     if (!a.eager && blockIdx.x == 0 && threadIdx.x == 0 && S.trips > a.maxiter + 2) cudaGraphSetConditional(a.cond, 0u);
     if (!S.active) return;
-    constexpr int U = Ilp<NRHS>::U;
+    // two rows per thread for one right-hand side: 48 registers, 5 resident CTAs per SM
+    // (four rows: 77 registers, 3 CTAs; measured 194.5 against 191.2 us per p' iteration)
+    constexpr int U = NRHS == 1 ? 2 : Ilp<NRHS>::U;
     const bool gpu = a.stop == KCFD_STOP_GPU;
     const double* ph = (PREC == KCFD_PREC_NONE) ? a.p : a.ph;
     const double* sh = (PREC == KCFD_PREC_NONE) ? a.r : a.sh;

@@ -1406,7 +1406,7 @@ GeGrid ge_grids(int n, int sms, int gmax) {
     r.sv = g((const void*)ge::g_spmv_v<NRHS, PREC>, 1);
     r.s = g((const void*)ge::g_s<NRHS, PREC>, U);
     r.st = g((const void*)ge::g_spmv_t<NRHS, PREC>, 1);
-    r.xr = g((const void*)ge::g_xr<NRHS, PREC>, U);
+    r.xr = g((const void*)ge::g_xr<NRHS, PREC>, NRHS == 1 ? 2 : U);  // g_xr's rows per thread
     return r;
 }
 

@@ -152,6 +152,9 @@ class TwoFluidSolver:
         self._s1 = Solver(self._A, precond="ilu0", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels)
         self._sg = Solver(self._A, precond="ilu0", nrhs=nd, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels)
         self._params = _lib.TfParams()
+        # Krylov iterations of the one-rhs and the ndim-rhs solves since the last
+        # reset (device counters, read by the caller when it wants them)
+        self.krylov = torch.zeros(2, dtype=torch.int64, device=device)
 
     # ---- set-up (models/two_fluid.py:97-165) ----
     def initialize(self, alpha_g_init=0.05):
@@ -278,6 +281,7 @@ class TwoFluidSolver:
     def _solve(self, solver, x, rhs):
         solver.setup(self._A)
         solver.solve(self._A, rhs, x)
+        self.krylov[0 if solver is self._s1 else 1] += solver.iters.max().to(self.krylov.dtype)
 
     def _simple_iteration(self):
         self._sync_params()

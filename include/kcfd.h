@@ -48,6 +48,23 @@ int  kcfd_last_error(char* buf, int32_t len);
 /* Number of SMs and compute capability of the current device (probe, no allocation). */
 int  kcfd_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor);
 
+/* ------------------------------------------------------------ CUDA graphs ---- */
+/* Capture the device work of a sequence of kcfd_* calls issued on one stream as a
+ * CUDA graph and replay it (e.g. one SIMPLE outer iteration: assembly, solver set-up
+ * and solves, with fixed pointers and sizes). No counterpart in the reference, whose
+ * outer loop is host Python (models/single_phase.py:70-101).
+ * kcfd_graph_capture_begin starts a thread-local capture on a non-default stream;
+ * calls that allocate (kcfd_solver_create, kcfd_batch_create, kcfd_mesh_build) and a
+ * handle's first solve on the graph engine must come before it (inside a capture an
+ * engine handle solves on its persistent kernel). kcfd_graph_capture_end ends the
+ * capture and instantiates the graph into *out; kcfd_graph_launch replays it on a
+ * stream; kcfd_graph_destroy frees it.                                             */
+typedef struct kcfd_graph kcfd_graph;
+int  kcfd_graph_capture_begin(void* stream);
+int  kcfd_graph_capture_end(void* stream, kcfd_graph** out);
+int  kcfd_graph_launch(kcfd_graph* g, void* stream);
+void kcfd_graph_destroy(kcfd_graph* g);
+
 /* ------------------------------------------------------- host mesh build ---- */
 /* Face discovery, owner/neighbour, geometry, boundary tagging
  * (mesh/mesh_reader.py:141-323 build_fvmesh_from_arrays / _build_fvmesh_3d), plus

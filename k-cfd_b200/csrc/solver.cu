@@ -1747,6 +1747,50 @@ int kcfd_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor) {
     return KCFD_OK;
 }
 
+struct kcfd_graph {
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+};
+
+int kcfd_graph_capture_begin(void* stream) {
+    KCFD_REQUIRE(stream, "kcfd_graph_capture_begin: a non-default stream is required");
+    KCFD_CUDA(cudaStreamBeginCapture((cudaStream_t)stream, cudaStreamCaptureModeThreadLocal));
+    return KCFD_OK;
+}
+
+int kcfd_graph_capture_end(void* stream, kcfd_graph** out) {
+    KCFD_REQUIRE(stream && out, "kcfd_graph_capture_end: NULL argument");
+    *out = nullptr;
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture((cudaStream_t)stream, &g);
+    cudaGraphExec_t x = nullptr;
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&x, g, 0);
+    if (e != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        cudaGetLastError();
+        set_error("kcfd_graph_capture_end: %s", cudaGetErrorString(e));
+        return KCFD_CUDA_ERROR;
+    }
+    auto* h = new kcfd_graph();
+    h->graph = g;
+    h->exec = x;
+    *out = h;
+    return KCFD_OK;
+}
+
+int kcfd_graph_launch(kcfd_graph* g, void* stream) {
+    KCFD_REQUIRE(g && g->exec, "kcfd_graph_launch: NULL graph");
+    KCFD_CUDA(cudaGraphLaunch(g->exec, (cudaStream_t)stream));
+    return KCFD_OK;
+}
+
+void kcfd_graph_destroy(kcfd_graph* g) {
+    if (!g) return;
+    if (g->exec) cudaGraphExecDestroy(g->exec);
+    if (g->graph) cudaGraphDestroy(g->graph);
+    delete g;
+}
+
 int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, const int32_t* level_of_row_host,
                        kcfd_solver** out) {
     KCFD_REQUIRE(A && opts && out, "kcfd_solver_create: NULL argument");

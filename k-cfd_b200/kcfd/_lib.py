@@ -103,6 +103,10 @@ SIGNATURES = {
     "kcfd_batch_destroy": (None, [vp]),
     "kcfd_batch_info": (i32, [vp, P_i64]),
     "kcfd_batch_tiers": (i32, [vp, P_i32]),
+    "kcfd_graph_capture_begin": (i32, [vp]),
+    "kcfd_graph_capture_end": (i32, [vp, C.POINTER(vp)]),
+    "kcfd_graph_launch": (i32, [vp, vp]),
+    "kcfd_graph_destroy": (None, [vp]),
     "kcfd_batch_solve": (i32, [vp, vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_vec_norms2": (i32, [i32, i32, vp, vp, vp, vp]),
     "kcfd_record_norm": (i32, [vp, vp, vp, i32, vp]),

@@ -157,3 +157,39 @@ class Solver:
         e = C.c_int32(0)
         _lib.check(_lib.lib().kcfd_solver_error(self._h, C.byref(e), _lib.stream_handle(stream)), "kcfd_solver_error")
         return e.value
+
+
+class DeviceGraph:
+    """The device work of the kcfd calls issued on `stream` inside the with-block,
+    captured as a CUDA graph (kcfd_graph_*); launch() replays it. Allocate (handles,
+    tensors) before the block; issue the calls on `stream` (pass it, or make it
+    torch's current stream)."""
+
+    def __init__(self, stream):
+        self.stream = stream
+        self._h = C.c_void_p()
+
+    def __enter__(self):
+        _lib.check(_lib.lib().kcfd_graph_capture_begin(_lib.stream_handle(self.stream)), "kcfd_graph_capture_begin")
+        return self
+
+    def __exit__(self, et, ev, tb):
+        h = C.c_void_p()
+        st = _lib.lib().kcfd_graph_capture_end(_lib.stream_handle(self.stream), C.byref(h))
+        if et is None:
+            _lib.check(st, "kcfd_graph_capture_end")
+        self._h = h
+        return False
+
+    def launch(self, stream=None):
+        _lib.check(_lib.lib().kcfd_graph_launch(self._h, _lib.stream_handle(stream or self.stream)),
+                   "kcfd_graph_launch")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h is not None and h.value:
+            try:
+                _lib.lib().kcfd_graph_destroy(h)
+            except Exception:
+                pass
+            self._h = None

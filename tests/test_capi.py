@@ -40,3 +40,14 @@ def test_last_error_roundtrip():
                            ctypes.byref(ctypes.c_void_p()))
     assert rc == _lib.BAD_INPUT
     assert "ndim" in _lib.last_error()
+
+
+def test_graph_entry_points_reject_null_arguments():
+    """The graph entry points check their arguments before any CUDA call."""
+    from kcfd import _lib
+    L = _lib.lib()
+    assert L.kcfd_graph_capture_begin(None) == _lib.BAD_INPUT
+    assert L.kcfd_graph_launch(None, None) == _lib.BAD_INPUT
+    assert L.kcfd_graph_capture_end(None, None) == _lib.BAD_INPUT
+    L.kcfd_graph_destroy(None)
+    assert "kcfd_graph" in _lib.last_error()

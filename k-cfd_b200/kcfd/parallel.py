@@ -179,6 +179,8 @@ class HaloExchange:
         import torch.distributed as dist
         self.plan, self.group, self.dist = plan, group, dist
         R = plan.n_ranks
+        if dist.is_initialized() and dist.get_world_size(group) != R:
+            raise ValueError(f"HaloExchange: the group has {dist.get_world_size(group)} ranks, the partition {R} parts")
         self.send_counts = [len(plan.send.get(q, ())) for q in range(R)]
         self.recv_counts = [(plan.recv[q].stop - plan.recv[q].start) if q in plan.recv else 0 for q in range(R)]
         order = [plan.send[q] for q in range(R) if q in plan.send]

@@ -87,3 +87,13 @@ def tune(csr, b, x0, precond="jacobi", mode=_lib.MODE_FP64, nrhs=1, team=0, leve
     _CACHE[k] = out
     _save()
     return out
+
+
+def tuned_solver(csr, b, x0, precond="jacobi", mode=_lib.MODE_FP64, nrhs=1, team=0, levels=None, rtol=1e-8,
+                 maxiter=5000, **kw):
+    """A Solver with the launch shape tune() picks for this pattern (tuned once per
+    process, or read from the KCFD_TUNE_CACHE file)."""
+    shape = tune(csr, b, x0, precond=precond, mode=mode, nrhs=nrhs, team=team, levels=levels, rtol=rtol,
+                 maxiter=maxiter, **kw)
+    return Solver(csr, precond=precond, mode=mode, nrhs=nrhs, team=team, lanes=shape["lanes"], block=shape["block"],
+                  levels=levels, rtol=rtol, maxiter=maxiter)

@@ -59,6 +59,14 @@ int  kcfd_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor);
  * engine handle solves on its persistent kernel). kcfd_graph_capture_end ends the
  * capture and instantiates the graph into *out; kcfd_graph_launch replays it on a
  * stream; kcfd_graph_destroy frees it.                                             */
+/* Failure-detection self-test of the team barrier (no counterpart in the reference):
+ * `ctas` CTAs meet at one barrier of a team that expects `team_size` members, on the
+ * caller's zeroed counter `bar` (uint32) and error flag `err` (int32). With
+ * team_size > ctas the barrier cannot complete; every wait gives up after
+ * budget_cycles (clock64), records KCFD_TIMEOUT in *err and returns, as the solver's
+ * barriers do, and the context stays usable. With team_size == ctas *err stays 0.  */
+int  kcfd_selftest_barrier(int32_t ctas, int32_t team_size, int64_t budget_cycles, uint32_t* bar, int32_t* err,
+                           void* stream);
 typedef struct kcfd_graph kcfd_graph;
 int  kcfd_graph_capture_begin(void* stream);
 int  kcfd_graph_capture_end(void* stream, kcfd_graph** out);

@@ -1747,6 +1747,28 @@ int kcfd_device_info(int32_t* sm_count, int32_t* cc_major, int32_t* cc_minor) {
     return KCFD_OK;
 }
 
+// One barrier of a team of `size` members met by gridDim.x CTAs (ranks 0..gridDim.x-1).
+__global__ void selftest_barrier_kernel(TeamCtl ctl, int size) {
+    GridTeam tm(ctl, blockIdx.x, size);
+    tm.sync();
+}
+
+int kcfd_selftest_barrier(int32_t ctas, int32_t team_size, int64_t budget_cycles, uint32_t* bar, int32_t* err,
+                          void* stream) {
+    KCFD_REQUIRE(bar && err, "kcfd_selftest_barrier: NULL argument");
+    KCFD_REQUIRE(ctas >= 1 && ctas <= 64 && team_size >= ctas && team_size <= 65,
+                 "kcfd_selftest_barrier: need 1 <= ctas <= 64 and ctas <= team_size <= 65");
+    KCFD_REQUIRE(budget_cycles > 0 && budget_cycles <= 4000000000LL, "kcfd_selftest_barrier: budget out of range");
+    TeamCtl ctl;
+    ctl.bar = bar;
+    ctl.partials = nullptr;
+    ctl.err = err;
+    ctl.budget = budget_cycles;
+    selftest_barrier_kernel<<<ctas, 32, 0, (cudaStream_t)stream>>>(ctl, team_size);
+    KCFD_CUDA(cudaGetLastError());
+    return KCFD_OK;
+}
+
 struct kcfd_graph {
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;

@@ -103,6 +103,7 @@ SIGNATURES = {
     "kcfd_batch_destroy": (None, [vp]),
     "kcfd_batch_info": (i32, [vp, P_i64]),
     "kcfd_batch_tiers": (i32, [vp, P_i32]),
+    "kcfd_selftest_barrier": (i32, [i32, i32, i64, vp, vp, vp]),
     "kcfd_graph_capture_begin": (i32, [vp]),
     "kcfd_graph_capture_end": (i32, [vp, C.POINTER(vp)]),
     "kcfd_graph_launch": (i32, [vp, vp]),

@@ -240,14 +240,28 @@ class TwoFluidSolver:
     # ---- time loop (models/two_fluid.py:167-222) ----
     def solve_transient(self, t_end, dt=None, report_interval=100, adaptive_dt=False, cfl_target=0.5,
                         dt_min=1e-8, dt_max=None, monitor=None):
-        if adaptive_dt:
-            raise NotImplementedError("adaptive time control (core/time_control.py) is not on the kcfd device path")
+        """models/two_fluid.py:167-258. With adaptive_dt the step after each SIMPLE
+        solve comes from AdaptiveTimeControl on the liquid velocity (brought to the
+        host once per step) and nu_l = mu_l / rho_l, shrinking when the step's residual
+        is not below 10 tol; as in the reference, time advances by the new step."""
         if dt is not None:
             self.dt = dt
+        ctrl = None
+        if adaptive_dt:
+            from .time_control import AdaptiveTimeControl
+            ctrl = AdaptiveTimeControl(dt_init=self.dt, dt_min=dt_min, dt_max=dt_max if dt_max is not None else t_end,
+                                       cfl_target=cfl_target)
         t, step = 0.0, 0
         self.residuals = []
+        dt_history, cfl_history = [], []
         while t < t_end - 1e-15:
             max_res = self.step()
+            if ctrl is not None:
+                new_dt, info = ctrl.compute_dt(self.mesh, self.U_l.values, self.mu_l / self.rho_l,
+                                               converged=(max_res < 10 * self.tol))
+                self.dt = new_dt
+                dt_history.append(new_dt)
+                cfl_history.append(info["cfl_max"])
             t += self.dt
             step += 1
             self.residuals.append(max_res)
@@ -256,8 +270,8 @@ class TwoFluidSolver:
             if step % report_interval == 0:
                 print(f"  Step {step}, t={t:.4f}, residual={max_res:.2e}, "
                       f"alpha_g: [{self.alpha_g.min():.4f}, {self.alpha_g.max():.4f}]")
-        return {"time_steps": step, "final_time": t, "residuals": self.residuals, "dt_history": [],
-                "cfl_history": []}
+        return {"time_steps": step, "final_time": t, "residuals": self.residuals, "dt_history": dt_history,
+                "cfl_history": cfl_history}
 
     def step(self):
         """One time step: store the old fields, then the SIMPLE inner iterations."""

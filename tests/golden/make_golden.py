@@ -352,6 +352,36 @@ def make_partitions(out, meshes):
         np.savez_compressed(os.path.join(out, f"part_{name}.npz"), **d)
 
 
+def make_time_control(out, meshes):
+    """core/time_control.py: compute_dt sequences (CFL- and Fourier-limited steps, the
+    growth cap, a non-converged shrink, the clip) on two fixture meshes with seeded
+    velocities, plus compute_cfl / compute_fourier arrays."""
+    from core.time_control import AdaptiveTimeControl
+    d = {}
+    for name in ("quad", "hex"):
+        m = meshes[name]
+        n, nd = m.n_cells, getattr(m, "ndim", 2)
+        rng = np.random.default_rng(21)
+        ctrl = AdaptiveTimeControl(dt_init=1e-3, dt_min=1e-8, dt_max=0.05, cfl_target=0.5)
+        vels, rows = [], []
+        for step in range(8):
+            vel = rng.normal(size=(n, nd)) * (0.05 if step < 4 else 300.0)
+            alpha = 1e-6 if step % 2 == 0 else 50.0
+            conv = step != 5
+            dt, info = ctrl.compute_dt(m, vel, alpha if step != 7 else None, converged=conv)
+            vels.append(vel)
+            rows.append([alpha, float(conv), dt, info["cfl_max"], info["fourier_max"],
+                         ["cfl", "fourier", "divergence"].index(info["dt_limited_by"])])
+        d[f"{name}_vel"] = np.concatenate(vels)
+        d[f"{name}_rows"] = np.asarray(rows, dtype=np.float64)
+        cmax, carr = ctrl.compute_cfl(m, vels[0], 2e-3)
+        fmax, farr = ctrl.compute_fourier(m, 1e-3, 2e-3)
+        d[f"{name}_cfl"] = carr
+        d[f"{name}_fo"] = farr
+        d[f"{name}_cfl1d"] = ctrl.compute_cfl(m, vels[0][:, 0], 2e-3)[1]
+    np.savez_compressed(os.path.join(out, "time_control.npz"), **d)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--ref", default="/root/reference")
@@ -377,6 +407,8 @@ def main():
         make_two_fluid(a.out, meshes)
     if want("partitions"):
         make_partitions(a.out, meshes)
+    if want("time_control"):
+        make_time_control(a.out, meshes)
     print("golden fixtures written to", a.out)
 
 

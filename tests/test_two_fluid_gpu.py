@@ -55,3 +55,31 @@ def test_two_fluid_solve_transient_api():
     out = sv.solve_transient(3 * sv.dt, sv.dt, report_interval=100)
     assert out["time_steps"] == 3 and len(out["residuals"]) == 3
     assert _rel(sv.T_l.values, g["quad_2_T_l"]) < 1e-10
+
+
+def test_two_fluid_adaptive_dt_follows_the_reference_loop():
+    """solve_transient(adaptive_dt=True) equals the reference's loop (models/two_fluid.py:
+    207-233) stepped by hand with the time controller (pinned to the reference in
+    test_time_control.py): the same dt and CFL histories and fields, bit for bit. tol
+    is set so that the steps count as converged, which exercises the CFL / growth
+    limits instead of the shrink."""
+    from kcfd.time_control import AdaptiveTimeControl
+    t_end = 3.5e-3
+    sv = _device_solver("quad", 11)
+    sv.tol = 1e3
+    out = sv.solve_transient(t_end, 1e-3, report_interval=100, adaptive_dt=True, cfl_target=0.5)
+    ref = _device_solver("quad", 11)
+    ref.tol = 1e3
+    ctrl = AdaptiveTimeControl(dt_init=1e-3, dt_min=1e-8, dt_max=t_end, cfl_target=0.5)
+    t, dts = 0.0, []
+    while t < t_end - 1e-15:
+        res = ref.step()
+        dt, _ = ctrl.compute_dt(ref.mesh, ref.U_l.values, ref.mu_l / ref.rho_l, converged=res < 10 * ref.tol)
+        ref.dt = dt
+        dts.append(dt)
+        t += dt
+    assert out["time_steps"] == len(dts) >= 2
+    assert out["dt_history"] == dts and out["cfl_history"] == ctrl.cfl_history
+    assert dts[0] != 1e-3
+    for f in FIELDS:
+        np.testing.assert_array_equal(getattr(sv, f).values, getattr(ref, f).values)

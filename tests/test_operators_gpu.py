@@ -107,3 +107,50 @@ def test_device_system_solves_through_linear_solver():
     b = s.rhs.cpu().numpy()
     xd = spla.spsolve(A.tocsc(), b)
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-9
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_signature_operators(name):
+    """The module-level operators of kcfd.fvm_operators (the reference's signatures:
+    op(mesh, ..., system), host arrays, mass flux in reference face order, a
+    ScalarField-like phi with per-patch boundary values) give the reference's full
+    system on the host FVMSystem mirror and on a DeviceSystem."""
+    from types import SimpleNamespace
+    from scipy import sparse
+    from kcfd import fvm_operators as kf
+    from kcfd.assembly import DeviceSystem
+    m, dm, g, f, T = _setup(name)
+    names = list(m.boundary_patches)
+    bc = {}
+    for nm, kind, val in zip(names, g["bc_kind"], g["bc_value"]):
+        bc[nm] = {"type": str(kind), "value": float(val)} if str(kind) == "neumann" else {"type": str(kind)}
+    phib, k = {}, 0
+    for nm in names:
+        nf = len(m.boundary_patches[nm])
+        phib[nm] = g["phi_b"][k:k + nf]
+        k += nf
+    phi = SimpleNamespace(values=g["phi"], boundary_values=phib)
+    gamma = SimpleNamespace(values=g["gamma"])
+    ref = sparse.csr_matrix((g["full_data"], g["full_indices"], g["full_indptr"]))
+    for system in (kf.FVMSystem(m.n_cells), DeviceSystem(dm)):
+        kf.diffusion_operator(m, gamma, system)
+        kf.convection_operator_upwind(m, g["mf"], system)
+        kf.temporal_operator(m, 1.3, 0.01, g["phi_old"], system)
+        kf.apply_boundary_conditions(m, phi, gamma, g["mf"], system, bc)
+        kf.under_relax(system, phi, 0.7)
+        A = system.to_sparse()
+        A.sort_indices()
+        np.testing.assert_array_equal(A.indptr, g["full_indptr"])
+        np.testing.assert_array_equal(A.indices, g["full_indices"])
+        _close(A.data, ref.data)
+        rhs = system.rhs.cpu().numpy() if hasattr(system.rhs, "cpu") else system.rhs
+        diag = system.diag.cpu().numpy() if hasattr(system.diag, "cpu") else system.diag
+        _close(rhs, g["full_rhs"])
+        _close(diag, g["full_diag"])
+    s = kf.FVMSystem(m.n_cells)
+    kf.source_term(m, g["S"], s)
+    _close(s.rhs, g["src_rhs"])
+    s = kf.FVMSystem(m.n_cells)
+    kf.linearized_source(m, g["Sp"], g["Su"], s)
+    _close(s.rhs, g["lin_rhs"]) if np.abs(g["lin_rhs"]).max() > 0 else None
+    _close(s.diag, g["lin_diag"]) if np.abs(g["lin_diag"]).max() > 0 else None

@@ -154,3 +154,16 @@ def test_reference_signature_operators(name):
     kf.linearized_source(m, g["Sp"], g["Su"], s)
     _close(s.rhs, g["lin_rhs"]) if np.abs(g["lin_rhs"]).max() > 0 else None
     _close(s.diag, g["lin_diag"]) if np.abs(g["lin_diag"]).max() > 0 else None
+
+
+@pytest.mark.parametrize("name", NAMES)
+def test_reference_signature_muscl(name):
+    """kcfd.interpolation.muscl_deferred_correction with the reference's signature
+    (host arrays, mass flux in reference face order) equals the reference's output."""
+    from types import SimpleNamespace
+    from kcfd.interpolation import muscl_deferred_correction
+    m, dm, g, f, T = _setup(name)
+    phi = SimpleNamespace(values=g["phi"])
+    for lim in ("minmod", "superbee", "van_albada", "van_leer"):
+        c = muscl_deferred_correction(m, phi, g["mf"], g["gg"], lim)
+        _close(c, g["muscl_" + lim])

@@ -11,6 +11,12 @@ Synthetic generators for the workloads the reference has no generator for:
   * delaunay_tet_arrays  -- Delaunay tetrahedralisation of a jittered lattice
 Everything here is vectorised numpy; the meshes are built from these arrays by
 kcfd.mesh.build_mesh (native face discovery).
+
+The reference's named generators return a kcfd Mesh built from the same arrays:
+generate_channel_mesh, generate_cavity_mesh, generate_bubble_column_mesh,
+generate_triangle_channel_mesh (mesh/mesh_generator.py:96-128,232-325),
+generate_3d_channel_mesh, generate_3d_duct_mesh, generate_3d_cavity_mesh
+(mesh/mesh_generator_3d.py:12-206).
 """
 from __future__ import annotations
 
@@ -195,3 +201,56 @@ def delaunay_tet_arrays(box, n_target, rng, jitter=0.25):
     rest = ~((zc < 1e-9 * Lz + 1e-12) | (zc > Lz * (1 - 1e-9) - 1e-12))
     bd["wall"] = list(bf[rest])
     return pts, cells, cfaces, bd
+
+
+# ------------------------------------------------- the reference's named generators --
+def _build(nodes, cells, bd, cf=None):
+    from .mesh import build_mesh
+    return build_mesh(nodes, cells, bd, ndim=3 if cf is not None else 2, cell_face_node_list=cf)
+
+
+def generate_channel_mesh(length=1.0, height=0.1, nx=50, ny=20):
+    """mesh/mesh_generator.py:96-110: inlet (left), outlet (right), wall_bottom, wall_top."""
+    return _build(*quad_box_arrays(0.0, 0.0, length, height, nx, ny, CHANNEL_2D_NAMES))
+
+
+def generate_cavity_mesh(size=1.0, n=64):
+    """mesh/mesh_generator.py:113-126: lid (top), wall_bottom, wall_left, wall_right."""
+    return _build(*quad_box_arrays(0.0, 0.0, size, size, n, n, CAVITY_2D_NAMES))
+
+
+def generate_bubble_column_mesh(width=0.15, height=0.45, nx=30, ny=90):
+    """mesh/mesh_generator.py:232-263: the bottom split into inlet_gas (faces whose
+    centre x lies in [width/3, 2 width/3]) and wall_bottom, after outlet (top),
+    wall_left and wall_right."""
+    nodes, cells, bd = quad_box_arrays(0.0, 0.0, width, height, nx, ny,
+                                       {"bottom": "_bottom", "top": "outlet", "left": "wall_left",
+                                        "right": "wall_right"})
+    bottom = np.asarray(bd.pop("_bottom"))
+    xc = 0.5 * (nodes[bottom[:, 0], 0] + nodes[bottom[:, 1], 0])
+    inlet = (width / 3.0 <= xc) & (xc <= 2.0 * width / 3.0)
+    bd["inlet_gas"] = list(bottom[inlet])
+    bd["wall_bottom"] = list(bottom[~inlet])
+    return _build(nodes, cells, bd)
+
+
+def generate_triangle_channel_mesh(Lx=1.0, Ly=0.1, nx=20, ny=5):
+    """mesh/mesh_generator.py:266-325."""
+    return _build(*tri_channel_arrays(Lx, Ly, nx, ny))
+
+
+def generate_3d_channel_mesh(Lx=1.0, Ly=0.1, Lz=0.1, nx=20, ny=10, nz=10, boundary_names=None):
+    """mesh/mesh_generator_3d.py:12-159 (default names: inlet, outlet, wall_bottom,
+    wall_top, wall_front, wall_back)."""
+    nodes, cells, cf, bd = hex_box_arrays(Lx, Ly, Lz, nx, ny, nz, boundary_names or CHANNEL_3D_NAMES)
+    return _build(nodes, cells, bd, cf)
+
+
+def generate_3d_duct_mesh(Lx=2.0, Ly=0.1, Lz=0.1, nx=20, ny=10, nz=10):
+    """mesh/mesh_generator_3d.py:162-178."""
+    return generate_3d_channel_mesh(Lx, Ly, Lz, nx, ny, nz, CHANNEL_3D_NAMES)
+
+
+def generate_3d_cavity_mesh(Lx=1.0, Ly=1.0, Lz=1.0, nx=16, ny=16, nz=16):
+    """mesh/mesh_generator_3d.py:181-206: lid (y = Ly), walls elsewhere."""
+    return generate_3d_channel_mesh(Lx, Ly, Lz, nx, ny, nz, CAVITY_3D_NAMES)

@@ -352,6 +352,31 @@ def make_partitions(out, meshes):
         np.savez_compressed(os.path.join(out, f"part_{name}.npz"), **d)
 
 
+def make_generators(out):
+    """The reference's named generators with non-default arguments: their
+    build_fvmesh_from_arrays inputs and the built mesh (gen_<name>.npz)."""
+    import mesh.mesh_generator as mg
+    import mesh.mesh_generator_3d as mg3
+    rec = _Recorder(mg.build_fvmesh_from_arrays)
+    mg.build_fvmesh_from_arrays = rec
+    mg3.build_fvmesh_from_arrays = rec
+    cases = {
+        "channel": lambda: mg.generate_channel_mesh(1.2, 0.3, 7, 4),
+        "cavity": lambda: mg.generate_cavity_mesh(0.8, 6),
+        "tri_channel": lambda: mg.generate_triangle_channel_mesh(1.1, 0.4, 6, 3),
+        "bubble_column": lambda: mg.generate_bubble_column_mesh(0.15, 0.45, 9, 12),
+        "channel_3d": lambda: mg3.generate_3d_channel_mesh(1.0, 0.5, 0.4, 5, 3, 2),
+        "duct_3d": lambda: mg3.generate_3d_duct_mesh(2.0, 0.3, 0.2, 6, 3, 2),
+        "cavity_3d": lambda: mg3.generate_3d_cavity_mesh(1.0, 0.7, 0.6, 3, 4, 2),
+    }
+    for name, fn in cases.items():
+        rec.calls.clear()
+        m = fn()
+        d = _mesh_arrays(m)
+        d.update(_inputs_arrays(rec.calls[0]))
+        np.savez_compressed(os.path.join(out, f"gen_{name}.npz"), **d)
+
+
 def make_time_control(out, meshes):
     """core/time_control.py: compute_dt sequences (CFL- and Fourier-limited steps, the
     growth cap, a non-converged shrink, the clip) on two fixture meshes with seeded
@@ -409,6 +434,8 @@ def main():
         make_partitions(a.out, meshes)
     if want("time_control"):
         make_time_control(a.out, meshes)
+    if want("generators"):
+        make_generators(a.out)
     print("golden fixtures written to", a.out)
 
 

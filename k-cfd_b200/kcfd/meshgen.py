@@ -254,3 +254,96 @@ def generate_3d_duct_mesh(Lx=2.0, Ly=0.1, Lz=0.1, nx=20, ny=10, nz=10):
 def generate_3d_cavity_mesh(Lx=1.0, Ly=1.0, Lz=1.0, nx=16, ny=16, nz=16):
     """mesh/mesh_generator_3d.py:181-206: lid (y = Ly), walls elsewhere."""
     return generate_3d_channel_mesh(Lx, Ly, Lz, nx, ny, nz, CAVITY_3D_NAMES)
+
+
+def _split_quad(q):
+    """Two triangles of a quad (a, b, c, d), cut on the diagonal through its smallest
+    node id, so that the two cells sharing the quad cut it the same way."""
+    a, b, c, d = (int(v) for v in q)
+    if min(a, b, c, d) in (a, c):
+        return [(a, b, c), (a, c, d)]
+    return [(a, b, d), (b, c, d)]
+
+
+def _hex_quads(h):
+    """The six faces of a hex (n0..n7), outward, in the order z-, z+, y-, y+, x-, x+."""
+    n0, n1, n2, n3, n4, n5, n6, n7 = (int(v) for v in h)
+    return [(n0, n3, n2, n1), (n4, n5, n6, n7), (n0, n1, n5, n4), (n2, n3, n7, n6), (n0, n4, n7, n3),
+            (n1, n2, n6, n5)]
+
+
+def _tet_tris(t):
+    n0, n1, n2, n3 = (int(v) for v in t)
+    return [(n0, n2, n1), (n0, n1, n3), (n1, n2, n3), (n0, n3, n2)]
+
+
+def hybrid_hex_tet_arrays(Lx=2.0, Ly=0.1, Lz=0.1, nx=20, ny=8, nz=8, tet_fraction=0.5, boundary_names=None):
+    """mesh/hybrid_mesh_generator.py:93-260: hexes on the low-x side, and on the
+    high-x side every hex replaced by 12 tets around an added centre node (each hex
+    face cut by _split_quad, each triangle joined to the centre); the last hex column
+    carries its x+ face as the two triangles its tet neighbours see. Boundary faces
+    are the faces of one cell only (none through a centre node), each given to the
+    first box plane (x_min, x_max, y_min, y_max, z_min, z_max) holding all its
+    nodes, in the order the cells list them."""
+    names = boundary_names or CHANNEL_3D_NAMES
+    dx, dy, dz = Lx / nx, Ly / ny, Lz / nz
+    nx_hex = max(1, int(nx * (1.0 - tet_fraction)))
+    nx_tet = nx - nx_hex
+    base = (nx + 1) * (ny + 1) * (nz + 1)
+
+    def nid(i, j, k):
+        return k * (ny + 1) * (nx + 1) + j * (nx + 1) + i
+
+    k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
+    lattice = np.stack([i.reshape(-1) * dx, j.reshape(-1) * dy, k.reshape(-1) * dz], axis=1)
+    kc, jc, ic = (a.reshape(-1) for a in np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx_hex, nx),
+                                                      indexing="ij"))
+    centres = np.stack([(ic + 0.5) * dx, (jc + 0.5) * dy, (kc + 0.5) * dz], axis=1)
+    nodes = np.concatenate([lattice, centres]) if len(centres) else lattice
+    centre_of = {(int(a), int(b), int(c)): base + q for q, (a, b, c) in enumerate(zip(ic, jc, kc))}
+    tol = 1e-10
+    x, y, z = lattice[:, 0], lattice[:, 1], lattice[:, 2]
+    planes = [("x_min", np.abs(x) < tol), ("x_max", np.abs(x - Lx) < tol), ("y_min", np.abs(y) < tol),
+              ("y_max", np.abs(y - Ly) < tol), ("z_min", np.abs(z) < tol), ("z_max", np.abs(z - Lz) < tol)]
+    cells, cfaces = [], []
+    for kk in range(nz):
+        for jj in range(ny):
+            for ii in range(nx):
+                h = [nid(ii, jj, kk), nid(ii + 1, jj, kk), nid(ii + 1, jj + 1, kk), nid(ii, jj + 1, kk),
+                     nid(ii, jj, kk + 1), nid(ii + 1, jj, kk + 1), nid(ii + 1, jj + 1, kk + 1), nid(ii, jj + 1, kk + 1)]
+                quads = _hex_quads(h)
+                if ii < nx_hex:
+                    faces = quads[:5] + _split_quad(quads[5]) if (ii == nx_hex - 1 and nx_tet > 0) else quads
+                    cells.append(np.array(h))
+                    cfaces.append([np.array(f) for f in faces])
+                else:
+                    c = centre_of[(ii, jj, kk)]
+                    for q in quads:
+                        for tri in _split_quad(q):
+                            t = (*tri, c)
+                            cells.append(np.array(t))
+                            cfaces.append([np.array(f) for f in _tet_tris(t)])
+    count = {}
+    for fl in cfaces:
+        for f in fl:
+            key = tuple(sorted(int(v) for v in f))
+            count[key] = count.get(key, 0) + 1
+    bd = {names.get(p, p): [] for p, _ in planes}
+    seen = set()
+    for fl in cfaces:
+        for f in fl:
+            key = tuple(sorted(int(v) for v in f))
+            if key in seen or count[key] != 1 or max(key) >= base:
+                continue
+            seen.add(key)
+            for p, on in planes:
+                if on[list(key)].all():
+                    bd.setdefault(names.get(p, p), []).append(f)
+                    break
+    return nodes, cells, cfaces, bd
+
+
+def generate_hybrid_hex_tet_mesh(Lx=2.0, Ly=0.1, Lz=0.1, nx=20, ny=8, nz=8, tet_fraction=0.5, boundary_names=None):
+    """mesh/hybrid_mesh_generator.py:93-260 (the cell zone map is not kept)."""
+    nodes, cells, cf, bd = hybrid_hex_tet_arrays(Lx, Ly, Lz, nx, ny, nz, tet_fraction, boundary_names)
+    return _build(nodes, cells, bd, cf)

@@ -30,3 +30,21 @@ def test_named_generator_matches_reference(name):
         np.testing.assert_array_equal(m.boundary_patches[k], ref_p[k])
     for a, b in ((m.area, d["area"]), (m.normal, d["normal"]), (m.ccenter, d["ccenter"]), (m.volume, d["volume"])):
         np.testing.assert_allclose(a, b, rtol=1e-14, atol=1e-15)
+
+
+def test_hybrid_generator_matches_reference():
+    """generate_hybrid_hex_tet_mesh: the reference generator's recorded inputs (nodes,
+    cells, per-cell faces, boundary dict) bit for bit, and the built mesh."""
+    from conftest import golden_inputs
+    d = load_golden("mesh_hybrid")
+    nodes, cells, bd, cfl = golden_inputs(d)
+    n2, c2, f2, b2 = meshgen.hybrid_hex_tet_arrays(1.0, 0.5, 0.5, 4, 2, 2, 0.5)
+    np.testing.assert_array_equal(n2, nodes)
+    assert len(c2) == len(cells) and all(np.array_equal(a, b) for a, b in zip(c2, cells))
+    assert all(len(a) == len(b) and all(np.array_equal(x, y) for x, y in zip(a, b)) for a, b in zip(f2, cfl))
+    assert list(b2) == list(bd)
+    for k in bd:
+        assert len(b2[k]) == len(bd[k]) and all(np.array_equal(x, y) for x, y in zip(b2[k], bd[k]))
+    m = meshgen.generate_hybrid_hex_tet_mesh(1.0, 0.5, 0.5, 4, 2, 2, 0.5)
+    np.testing.assert_array_equal(m.owner, d["owner"])
+    np.testing.assert_array_equal(m.neighbour, d["neighbour"])

@@ -44,6 +44,15 @@ def _flat(lists):
     return lens, flat
 
 
+def build_fvmesh_from_arrays(node_coords, cell_node_list, boundary_faces_dict, cell_zone_map=None, ndim=2,
+                             cell_face_node_list=None):
+    """The reference's builder signature (mesh/mesh_reader.py:141-242); the cell zone
+    map is kept on the mesh (cell_zones) and not used by the solvers."""
+    m = build_mesh(node_coords, cell_node_list, boundary_faces_dict, ndim=ndim, cell_face_node_list=cell_face_node_list)
+    m.cell_zones = dict(cell_zone_map or {})
+    return m
+
+
 def build_mesh(node_coords, cell_node_list, boundary_faces_dict, ndim=2, cell_face_node_list=None):
     """Build a Mesh with the reference builder's face order, owner/neighbour and geometry."""
     L = _lib.lib()

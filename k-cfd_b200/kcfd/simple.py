@@ -240,6 +240,33 @@ class SIMPLESolver:
         self._graph = None
         return {"time_steps": steps, "final_time": t}
 
+    # ---- profiles (models/single_phase.py:390-425) ----
+    def _spacing(self, axis):
+        """Centre distance along `axis` across the first internal face (in face order)
+        where it exceeds 1e-10; 0.05 if there is none."""
+        m = self.mesh
+        cc = np.asarray(m.ccenter)
+        internal = np.flatnonzero(np.asarray(m.neighbour) >= 0)
+        d = np.abs(cc[np.asarray(m.owner)[internal], axis] - cc[np.asarray(m.neighbour)[internal], axis])
+        big = np.flatnonzero(d > 1e-10)
+        return float(d[big[0]]) if len(big) else 0.05
+
+    def _profile(self, axis, target):
+        cc = np.asarray(self.mesh.ccenter)
+        sel = np.flatnonzero(np.abs(cc[:, axis] - target) < self._spacing(axis) * 1.5)
+        pos = cc[sel, 1 - axis]
+        U = self.U.values
+        idx = np.argsort(pos)
+        return pos[idx], U[sel, 0][idx], U[sel, 1][idx]
+
+    def get_velocity_at_y(self, x_target, n_points=50):
+        """(y, u, v) of the cells within 1.5 cell widths of x = x_target, sorted by y."""
+        return self._profile(0, x_target)
+
+    def get_velocity_at_x(self, y_target):
+        """(x, u, v) of the cells within 1.5 cell heights of y = y_target, sorted by x."""
+        return self._profile(1, y_target)
+
     def face_mass_flux(self):
         """Current face mass flux in reference face order (host)."""
         return self.dm.to_reference_faces(self.mf_t)

@@ -377,6 +377,28 @@ def make_generators(out):
         np.savez_compressed(os.path.join(out, f"gen_{name}.npz"), **d)
 
 
+def make_profiles(out):
+    """models/single_phase.py:390-425: velocity profiles through the 8x8 cavity after
+    20 outer iterations (the 2d case of make_simple), with the U they were taken from."""
+    from mesh.mesh_generator import generate_cavity_mesh
+    from models.single_phase import SIMPLESolver
+    import contextlib
+    import io
+    m = generate_cavity_mesh(1.0, 8)
+    sv = SIMPLESolver(m, rho=1.0, mu=0.01)
+    for pname in m.boundary_patches:
+        sv.set_velocity_bc(pname, "dirichlet", [1.0, 0.0] if pname == "lid" else [0.0, 0.0])
+        sv.set_pressure_bc(pname, "zero_gradient")
+    sv.alpha_u, sv.alpha_p, sv.max_outer_iter, sv.tol = 0.7, 0.3, 20, 0.0
+    with contextlib.redirect_stdout(io.StringIO()):
+        sv.solve_steady()
+    d = {"U": sv.U.values.copy()}
+    for tag, (a, b, c) in (("y05", sv.get_velocity_at_y(0.5)), ("y03", sv.get_velocity_at_y(0.3)),
+                           ("x05", sv.get_velocity_at_x(0.5)), ("x09", sv.get_velocity_at_x(0.9))):
+        d[tag + "_pos"], d[tag + "_u"], d[tag + "_v"] = a, b, c
+    np.savez_compressed(os.path.join(out, "profiles.npz"), **d)
+
+
 def make_time_control(out, meshes):
     """core/time_control.py: compute_dt sequences (CFL- and Fourier-limited steps, the
     growth cap, a non-converged shrink, the clip) on two fixture meshes with seeded
@@ -436,6 +458,8 @@ def main():
         make_time_control(a.out, meshes)
     if want("generators"):
         make_generators(a.out)
+    if want("profiles"):
+        make_profiles(a.out)
     print("golden fixtures written to", a.out)
 
 

@@ -316,3 +316,13 @@ def test_spmv_matches_scipy(torch_cuda):
     np.testing.assert_allclose(y3, A @ x, rtol=1e-13, atol=1e-13)
     y32 = d.spmv(torch.from_numpy(x[:, 0].astype(np.float32)).cuda(), fp32=True).cpu().numpy()
     np.testing.assert_allclose(y32, A @ x[:, 0], rtol=1e-4, atol=1e-4)
+
+
+def test_benchmark_solvers_reports_the_reference_keys(torch_cuda):
+    from kcfd.gpu_solver import benchmark_solvers
+    A, b = convdiff_system(channel_mesh(20, 16))
+    r = benchmark_solvers(A.tocsr(), b, n_runs=2)
+    assert r["backend"] == "b200"
+    for k in ("cpu_direct", "cpu_bicgstab", "gpu_bicgstab"):
+        assert r[k] > 0.0
+    np.testing.assert_allclose(A @ r["x_direct"], b, rtol=0, atol=1e-10 * np.abs(b).max())

@@ -162,22 +162,32 @@ class Server:
         self.policy = policy
         self.builders = max(1, int(builders))
 
-    def run(self, requests, serial=False):
+    def run(self, requests, serial=False, case_factory=None):
         """Serve `requests` in real time (arrival times honoured). serial=True runs one
-        case at a time (the serial comparator). Returns a list of Result."""
-        torch = _lib.require_cuda()
+        case at a time (the serial comparator). Returns a list of Result; `last_stats`
+        then holds the peak admitted footprint and the peak number of resident cases.
+
+        case_factory(request) -> case replaces the device-resident `Case` (same members:
+        req, cells, done_iters, launch(k), ready(), continuity(), fields()); the default
+        builds a Case on the current GPU."""
         from concurrent.futures import ThreadPoolExecutor
+        if case_factory is None:
+            torch = _lib.require_cuda()
+            dev = torch.cuda.current_device()
+
+            def build(r):
+                torch.cuda.set_device(dev)
+                # alone, a case takes the library's fastest single-case solvers
+                return Case(r, self.precision, self.graph, self.precond_p, small_team=0 if serial else 1)
+
+            finish = torch.cuda.synchronize
+        else:
+            build, finish = case_factory, (lambda: None)
         reqs = sorted(requests, key=lambda r: r.arrival)
         pending = list(reqs)
         queue, building, active, results = [], [], [], []
-        used = 0
+        used = peak_used = peak_resident = 0
         max_active = 1 if serial else self.max_active
-        dev = torch.cuda.current_device()
-
-        def build(r):
-            torch.cuda.set_device(dev)
-            # alone, a case takes the library's fastest single-case solvers
-            return Case(r, self.precision, self.graph, self.precond_p, small_team=0 if serial else 1)
 
         t0 = time.perf_counter()
         with ThreadPoolExecutor(max_workers=self.builders) as pool:
@@ -199,6 +209,8 @@ class Server:
                     queue.pop(pick)
                     used += fp
                     building.append((r, fp, time.perf_counter() - t0, pool.submit(build, r)))
+                    peak_used = max(peak_used, used)
+                    peak_resident = max(peak_resident, len(active) + len(building))
                     progressed = True
                 # built cases start their first tick
                 still_b = []
@@ -237,7 +249,8 @@ class Server:
                 active = still
                 if not progressed:
                     time.sleep(0.0002)
-        torch.cuda.synchronize()
+        finish()
+        self.last_stats = {"peak_bytes": peak_used, "peak_resident": peak_resident}
         return results
 
 

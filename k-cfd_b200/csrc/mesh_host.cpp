@@ -9,13 +9,21 @@
 //    centres, Newell normals, divergence-theorem volumes), with the reference's
 //    operation order so results agree to the last bit;
 //  * boundary tagging :216-231 / :298-313 (last patch assignment of a key wins).
-// Face discovery uses an open-addressing hash of the sorted node tuple (<= 4 nodes,
-// node ids < 2^32), so the whole build is one pass over the cell faces.
+// Face discovery keys every face item by its sorted node tuple (<= 4 nodes, node ids
+// < 2^32), buckets the items by their smallest node and matches them inside each
+// bucket; face ids are then numbered in item order. The passes that are independent
+// per cell, item, face or row run on host threads over fixed chunks, so the result
+// is the same bit for bit whatever the thread count; the greedy colourings and the
+// neighbour assignment (the last later cell wins) stay sequential.
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <memory>
 #include <mutex>
+#include <thread>
+#include <type_traits>
+#include <utility>
 #include <vector>
 
 #include "kcfd_common.h"
@@ -102,6 +110,29 @@ class KeyTable {
     std::vector<int64_t> vals_;
 };
 
+// Allocator whose resize() leaves new elements default-initialised (no zero fill):
+// the builder writes every element of these arrays on its worker threads.
+template <class T>
+struct DefaultInitAlloc : std::allocator<T> {
+    template <class U>
+    struct rebind {
+        using other = DefaultInitAlloc<U>;
+    };
+    DefaultInitAlloc() = default;
+    template <class U>
+    DefaultInitAlloc(const DefaultInitAlloc<U>&) noexcept {}
+    template <class U>
+    void construct(U* p) noexcept(std::is_nothrow_default_constructible<U>::value) {
+        ::new ((void*)p) U;
+    }
+    template <class U, class... A>
+    void construct(U* p, A&&... a) {
+        ::new ((void*)p) U(std::forward<A>(a)...);
+    }
+};
+template <class T>
+using dvec = std::vector<T, DefaultInitAlloc<T>>;
+
 }  // namespace
 }  // namespace kcfd
 
@@ -110,17 +141,48 @@ struct kcfd_host_mesh {
     int64_t n_cells = 0, n_faces = 0, n_internal = 0, nnz = 0;
     int max_face_nodes = 2, max_cell_faces = 0;
     int n_int_colors = 0, n_bnd_colors = 0, n_cell_colors = 0, n_levels = 0;
-    std::vector<int64_t> owner, neighbour, face_nodes, cell_faces;
-    std::vector<double> area, normal, fcenter, ccenter, volume;
-    std::vector<int32_t> face_patch, indptr, indices, slot_on, slot_no, diag_slot;
-    std::vector<int32_t> face_color, cell_color, level_natural;
+    kcfd::dvec<int64_t> owner, neighbour, face_nodes, cell_faces;
+    kcfd::dvec<double> area, normal, fcenter, ccenter, volume;
+    kcfd::dvec<int32_t> face_patch, indptr, indices, slot_on, slot_no, diag_slot;
+    kcfd::dvec<int32_t> face_color, cell_color, level_natural;
 };
 
 using kcfd::Key;
 using kcfd::make_key;
 using kcfd::KeyTable;
+using kcfd::dvec;
 
 namespace {
+
+// Host threads for the builder's independent passes (per cell, item, face or row).
+int host_threads() {
+    static const int t = [] {
+        unsigned h = std::thread::hardware_concurrency();
+        return (int)std::min(16u, std::max(1u, h));
+    }();
+    return t;
+}
+
+// Chunks of at least 32768 elements, at most one per host thread.
+int n_chunks(int64_t n) { return (int)std::max<int64_t>(1, std::min<int64_t>(host_threads(), n / 32768)); }
+
+// Runs fn(chunk, begin, end) over `chunks` contiguous pieces of [0, n). The pieces
+// depend only on n and chunks, and each element is computed by the same arithmetic
+// whatever thread runs it, so results do not depend on the thread count or timing.
+// A piece whose thread cannot be started runs on the calling thread.
+template <class Fn>
+void parallel_chunks(int64_t n, int chunks, Fn&& fn) {
+    auto run = [&](int t) { fn(t, n * t / chunks, n * (t + 1) / chunks); };
+    std::vector<std::thread> pool;
+    int t = 1;
+    try {
+        for (; t < chunks; ++t) pool.emplace_back(run, t);
+    } catch (...) {
+    }
+    for (int u = t; u < chunks; ++u) run(u);
+    run(0);
+    for (auto& th : pool) th.join();
+}
 
 void build_pattern(kcfd_host_mesh* m) {
     const int64_t n = m->n_cells, F = m->n_faces;
@@ -132,7 +194,7 @@ void build_pattern(kcfd_host_mesh* m) {
             cnt[m->neighbour[f] + 1] += 1;
         }
     for (int64_t i = 0; i < n; ++i) cnt[i + 1] += cnt[i];
-    std::vector<int32_t> cols(cnt[n]);
+    dvec<int32_t> cols(cnt[n]);
     std::vector<int64_t> pos(cnt.begin(), cnt.end() - 1);
     for (int64_t i = 0; i < n; ++i) cols[pos[i]++] = (int32_t)i;
     for (int64_t f = 0; f < F; ++f)
@@ -141,31 +203,43 @@ void build_pattern(kcfd_host_mesh* m) {
             cols[pos[o]++] = (int32_t)nb;
             cols[pos[nb]++] = (int32_t)o;
         }
-    m->indptr.assign(n + 1, 0);
-    m->indices.clear();
-    m->indices.reserve(cols.size());
-    for (int64_t i = 0; i < n; ++i) {
-        auto b = cols.begin() + cnt[i], e = cols.begin() + cnt[i + 1];
-        std::sort(b, e);
-        auto u = std::unique(b, e);
-        m->indices.insert(m->indices.end(), b, u);
-        m->indptr[i + 1] = (int32_t)m->indices.size();
-    }
-    m->nnz = (int64_t)m->indices.size();
+    // each row sorted and deduplicated in place, then packed
+    dvec<int64_t> ulen(n);
+    const int RC = n_chunks(n);
+    parallel_chunks(n, RC, [&](int, int64_t r0, int64_t r1) {
+        for (int64_t i = r0; i < r1; ++i) {
+            auto b = cols.begin() + cnt[i], e = cols.begin() + cnt[i + 1];
+            std::sort(b, e);
+            ulen[i] = std::unique(b, e) - b;
+        }
+    });
+    m->indptr.resize(n + 1);
+    m->indptr[0] = 0;
+    for (int64_t i = 0; i < n; ++i) m->indptr[i + 1] = (int32_t)(m->indptr[i] + ulen[i]);
+    m->nnz = m->indptr[n];
+    m->indices.resize(m->nnz);
+    parallel_chunks(n, RC, [&](int, int64_t r0, int64_t r1) {
+        for (int64_t i = r0; i < r1; ++i)
+            std::copy(cols.begin() + cnt[i], cols.begin() + cnt[i] + ulen[i], m->indices.begin() + m->indptr[i]);
+    });
     auto slot = [&](int64_t r, int64_t c) -> int32_t {
         auto b = m->indices.begin() + m->indptr[r], e = m->indices.begin() + m->indptr[r + 1];
         auto it = std::lower_bound(b, e, (int32_t)c);
         return (int32_t)(it - m->indices.begin());
     };
     m->diag_slot.resize(n);
-    for (int64_t i = 0; i < n; ++i) m->diag_slot[i] = slot(i, i);
-    m->slot_on.assign(F, -1);
-    m->slot_no.assign(F, -1);
-    for (int64_t f = 0; f < F; ++f)
-        if (m->neighbour[f] >= 0) {
-            m->slot_on[f] = slot(m->owner[f], m->neighbour[f]);
-            m->slot_no[f] = slot(m->neighbour[f], m->owner[f]);
+    parallel_chunks(n, RC, [&](int, int64_t r0, int64_t r1) {
+        for (int64_t i = r0; i < r1; ++i) m->diag_slot[i] = slot(i, i);
+    });
+    m->slot_on.resize(F);
+    m->slot_no.resize(F);
+    parallel_chunks(F, n_chunks(F), [&](int, int64_t f0, int64_t f1) {
+        for (int64_t f = f0; f < f1; ++f) {
+            const bool in = m->neighbour[f] >= 0;
+            m->slot_on[f] = in ? slot(m->owner[f], m->neighbour[f]) : -1;
+            m->slot_no[f] = in ? slot(m->neighbour[f], m->owner[f]) : -1;
         }
+    });
 }
 
 // Greedy edge colouring of internal faces in face order (no two faces of a colour
@@ -241,6 +315,11 @@ int kcfd_mesh_build(int32_t ndim, int64_t n_nodes, const double* nodes, int64_t 
     KCFD_REQUIRE(nodes && cell_ptr && cell_nodes, "kcfd_mesh_build: NULL node/cell arrays");
     const bool is3d = (ndim == 3 && cface_ptr != nullptr);
     if (ndim == 3) KCFD_REQUIRE(cface_ptr && cface_len && cface_off && cface_nodes, "kcfd_mesh_build: 3D needs cell face lists");
+    KCFD_REQUIRE(cell_ptr[0] == 0 && (!is3d || cface_ptr[0] == 0), "kcfd_mesh_build: offsets must start at 0");
+    for (int64_t c = 0; c < n_cells; ++c) {
+        KCFD_REQUIRE(cell_ptr[c + 1] > cell_ptr[c], "kcfd_mesh_build: cell %lld has no nodes", (long long)c);
+        if (is3d) KCFD_REQUIRE(cface_ptr[c + 1] >= cface_ptr[c], "kcfd_mesh_build: cell face offsets decrease at cell %lld", (long long)c);
+    }
     for (int64_t k = 0; k < cell_ptr[n_cells]; ++k)
         KCFD_REQUIRE(cell_nodes[k] >= 0 && cell_nodes[k] < n_nodes, "kcfd_mesh_build: cell node %lld out of range", (long long)cell_nodes[k]);
 
@@ -249,37 +328,41 @@ int kcfd_mesh_build(int32_t ndim, int64_t n_nodes, const double* nodes, int64_t 
     m->n_cells = n_cells;
     const int64_t n = n_cells;
     const int D = ndim;
+    const int CC = n_chunks(n);
     // ---- cell centres (node mean, sequential sum) and 2D areas (shoelace) ----
-    m->ccenter.assign(n * D, 0.0);
-    m->volume.assign(n, 0.0);
-    for (int64_t c = 0; c < n; ++c) {
-        int64_t b = cell_ptr[c], e = cell_ptr[c + 1];
-        int k = (int)(e - b);
-        for (int d = 0; d < D; ++d) {
-            double s = nodes[cell_nodes[b] * D + d];
-            for (int i = 1; i < k; ++i) s = s + nodes[cell_nodes[b + i] * D + d];
-            m->ccenter[c * D + d] = s / (double)k;
-        }
-        if (!is3d) {
-            double a = 0.0;
-            for (int i = 0; i < k; ++i) {
-                const double* pi = nodes + cell_nodes[b + i] * D;
-                const double* pj = nodes + cell_nodes[b + (i + 1) % k] * D;
-                double t1 = pi[0] * pj[1];
-                double t2 = pj[0] * pi[1];
-                a = a + (t1 - t2);
+    m->ccenter.resize(n * D);
+    m->volume.resize(n);  // 2D: shoelace below; 3D: divergence theorem after the faces
+    parallel_chunks(n, CC, [&](int, int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; ++c) {
+            int64_t b = cell_ptr[c], e = cell_ptr[c + 1];
+            int k = (int)(e - b);
+            for (int d = 0; d < D; ++d) {
+                double s = nodes[cell_nodes[b] * D + d];
+                for (int i = 1; i < k; ++i) s = s + nodes[cell_nodes[b + i] * D + d];
+                m->ccenter[c * D + d] = s / (double)k;
             }
-            m->volume[c] = std::fabs(a) / 2.0;
+            if (!is3d) {
+                double a = 0.0;
+                for (int i = 0; i < k; ++i) {
+                    const double* pi = nodes + cell_nodes[b + i] * D;
+                    const double* pj = nodes + cell_nodes[b + (i + 1) % k] * D;
+                    double t1 = pi[0] * pj[1];
+                    double t2 = pj[0] * pi[1];
+                    a = a + (t1 - t2);
+                }
+                m->volume[c] = std::fabs(a) / 2.0;
+            }
         }
-    }
+    });
     // ---- face discovery ----
-    int64_t n_items = is3d ? cface_ptr[n] : cell_ptr[n];
-    KeyTable table((size_t)n_items);
-    std::vector<int64_t> first_item;  // per face: item index of first discovery
-    first_item.reserve(n_items / 2 + 16);
-    std::vector<int64_t> item_face(n_items);
-    int kmax_face = 2;
-    std::vector<int64_t> cells_nf(n, 0);
+    // Every face item (a 2D cell edge or a given 3D face list) gets the key of its
+    // sorted node tuple. Items are bucketed by their smallest node id, which keeps
+    // the matching local (neighbouring cells share nodes), and matched inside each
+    // bucket; an item whose key has no earlier item is the face's first discovery.
+    // Face ids then follow item order, which is the reference's visiting order
+    // (cells in order, items of a cell in order).
+    const int64_t* iptr = is3d ? cface_ptr : cell_ptr;
+    const int64_t n_items = iptr[n];
     auto item_nodes = [&](int64_t it, int64_t c, int64_t* buf) -> int {
         if (is3d) {
             int k = (int)cface_len[it];
@@ -292,142 +375,230 @@ int kcfd_mesh_build(int32_t ndim, int64_t n_nodes, const double* nodes, int64_t 
         buf[1] = cell_nodes[b + (pos + 1) % (e - b)];
         return 2;
     };
-    int64_t buf[8];
-    for (int64_t c = 0; c < n; ++c) {
-        int64_t b = is3d ? cface_ptr[c] : cell_ptr[c];
-        int64_t e = is3d ? cface_ptr[c + 1] : cell_ptr[c + 1];
-        cells_nf[c] = e - b;
-        for (int64_t it = b; it < e; ++it) {
-            int k = item_nodes(it, c, buf);
-            if (k < 2 || k > 4) {
-                delete m;
-                kcfd::set_error("kcfd_mesh_build: faces need 2..4 nodes (got %d)", k);
-                return KCFD_BAD_INPUT;
-            }
-            for (int i = 0; i < k; ++i)
-                if (buf[i] < 0 || buf[i] >= n_nodes) {
-                    delete m;
-                    kcfd::set_error("kcfd_mesh_build: face node out of range");
-                    return KCFD_BAD_INPUT;
+    dvec<Key> item_key(n_items);
+    dvec<int32_t> item_cell(n_items);
+    struct ItemError {
+        int64_t item = -1;
+        int kind = 0, k = 0;
+    };
+    std::vector<ItemError> err_c(CC);
+    std::vector<int> kmax_c(CC, 2);
+    parallel_chunks(n, CC, [&](int t, int64_t c0, int64_t c1) {
+        int64_t buf[4];
+        for (int64_t c = c0; c < c1; ++c)
+            for (int64_t it = iptr[c]; it < iptr[c + 1]; ++it) {
+                const int k = is3d ? (int)cface_len[it] : 2;
+                if (k < 2 || k > 4) {
+                    err_c[t] = {it, 1, k};
+                    return;
                 }
-            kmax_face = std::max(kmax_face, k);
-            Key key = make_key(buf, k);
-            bool found = false;
-            size_t s = table.find_or_insert(key, &found);
-            if (!found) {
-                table.val(s) = (int64_t)first_item.size();
-                first_item.push_back(it);
-                m->owner.push_back(c);
-                m->neighbour.push_back(-1);
-            } else {
-                m->neighbour[table.val(s)] = c;
+                item_nodes(it, c, buf);
+                for (int i = 0; i < k; ++i)
+                    if (buf[i] < 0 || buf[i] >= n_nodes) {
+                        err_c[t] = {it, 2, k};
+                        return;
+                    }
+                kmax_c[t] = std::max(kmax_c[t], k);
+                item_key[it] = make_key(buf, k);
+                item_cell[it] = (int32_t)c;
             }
-            item_face[it] = table.val(s);
+    });
+    int kmax_face = 2;
+    for (int t = 0; t < CC; ++t) {
+        if (err_c[t].item >= 0) {  // the chunks are in item order: this is the first bad item
+            delete m;
+            if (err_c[t].kind == 1)
+                kcfd::set_error("kcfd_mesh_build: faces need 2..4 nodes (got %d)", err_c[t].k);
+            else
+                kcfd::set_error("kcfd_mesh_build: face node out of range");
+            return KCFD_BAD_INPUT;
         }
+        kmax_face = std::max(kmax_face, kmax_c[t]);
     }
-    const int64_t F = (int64_t)first_item.size();
+    std::vector<int64_t> bucket_ptr(n_nodes + 1, 0);
+    for (int64_t it = 0; it < n_items; ++it) bucket_ptr[(item_key[it].hi >> 32) + 1] += 1;
+    for (int64_t v = 0; v < n_nodes; ++v) bucket_ptr[v + 1] += bucket_ptr[v];
+    dvec<int64_t> bucket(n_items);
+    {
+        std::vector<int64_t> fill(bucket_ptr.begin(), bucket_ptr.end() - 1);
+        for (int64_t it = 0; it < n_items; ++it) bucket[fill[item_key[it].hi >> 32]++] = it;
+    }
+    // rep[it]: the first item with the same key (itself for a first discovery)
+    dvec<int64_t> rep(n_items);
+    parallel_chunks(n_nodes, n_chunks(n_nodes), [&](int, int64_t v0, int64_t v1) {
+        std::vector<int64_t> order;
+        for (int64_t v = v0; v < v1; ++v) {
+            const int64_t b = bucket_ptr[v], e = bucket_ptr[v + 1];
+            if (e - b <= 32) {
+                for (int64_t j = b; j < e; ++j) {
+                    const int64_t it = bucket[j];
+                    int64_t r = it;
+                    for (int64_t q = b; q < j; ++q)
+                        if (item_key[bucket[q]] == item_key[it]) {
+                            r = rep[bucket[q]];
+                            break;
+                        }
+                    rep[it] = r;
+                }
+            } else {  // a node shared by many faces: sort the bucket by (key, item)
+                order.assign(bucket.begin() + b, bucket.begin() + e);
+                std::sort(order.begin(), order.end(), [&](int64_t x, int64_t y) {
+                    const Key& p = item_key[x];
+                    const Key& q = item_key[y];
+                    if (p.hi != q.hi) return p.hi < q.hi;
+                    if (p.lo != q.lo) return p.lo < q.lo;
+                    return x < y;
+                });
+                for (size_t j = 0; j < order.size(); ++j)
+                    rep[order[j]] =
+                        (j > 0 && item_key[order[j]] == item_key[order[j - 1]]) ? rep[order[j - 1]] : order[j];
+            }
+        }
+    });
+    dvec<Key>().swap(item_key);
+    dvec<int64_t>().swap(bucket);
+    // face ids: first discoveries numbered in item order
+    const int IC = n_chunks(n_items);
+    std::vector<int64_t> first_off(IC + 1, 0);
+    parallel_chunks(n_items, IC, [&](int t, int64_t i0, int64_t i1) {
+        int64_t k = 0;
+        for (int64_t it = i0; it < i1; ++it) k += (rep[it] == it);
+        first_off[t + 1] = k;
+    });
+    for (int t = 0; t < IC; ++t) first_off[t + 1] += first_off[t];
+    const int64_t F = first_off[IC];
+    dvec<int64_t> first_item(F);  // per face: item index of first discovery
+    dvec<int64_t> item_face(n_items);
+    m->owner.resize(F);
+    m->neighbour.resize(F);
+    parallel_chunks(n_items, IC, [&](int t, int64_t i0, int64_t i1) {
+        int64_t f = first_off[t];
+        for (int64_t it = i0; it < i1; ++it)
+            if (rep[it] == it) {
+                item_face[it] = f;
+                first_item[f] = it;
+                m->owner[f] = item_cell[it];
+                m->neighbour[f] = -1;
+                ++f;
+            }
+    });
+    parallel_chunks(n_items, IC, [&](int, int64_t i0, int64_t i1) {
+        for (int64_t it = i0; it < i1; ++it)
+            if (rep[it] != it) item_face[it] = item_face[rep[it]];
+    });
+    for (int64_t it = 0; it < n_items; ++it)  // in item order: the last later cell wins
+        if (rep[it] != it) m->neighbour[item_face[it]] = item_cell[it];
+    dvec<int64_t>().swap(rep);
     m->n_faces = F;
     m->max_face_nodes = kmax_face;
     int kc = 0;
-    for (int64_t c = 0; c < n; ++c) kc = std::max<int64_t>(kc, cells_nf[c]);
+    for (int64_t c = 0; c < n; ++c) kc = std::max<int64_t>(kc, iptr[c + 1] - iptr[c]);
     m->max_cell_faces = kc;
-    m->cell_faces.assign(n * kc, -1);
-    for (int64_t c = 0; c < n; ++c) {
-        int64_t b = is3d ? cface_ptr[c] : cell_ptr[c];
-        for (int64_t j = 0; j < cells_nf[c]; ++j) m->cell_faces[c * kc + j] = item_face[b + j];
-    }
-    m->face_nodes.assign(F * kmax_face, -1);
-    std::vector<int> fsize(F);
-    for (int64_t f = 0; f < F; ++f) {
-        int64_t it = first_item[f];
-        int k = item_nodes(it, m->owner[f], buf);
-        fsize[f] = k;
-        for (int i = 0; i < k; ++i) m->face_nodes[f * kmax_face + i] = buf[i];
-    }
+    m->cell_faces.resize(n * kc);
+    parallel_chunks(n, CC, [&](int, int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; ++c)
+            for (int64_t j = 0; j < kc; ++j)
+                m->cell_faces[c * kc + j] = (iptr[c] + j < iptr[c + 1]) ? item_face[iptr[c] + j] : -1;
+    });
+    const int FC = n_chunks(F);
+    m->face_nodes.resize(F * kmax_face);
+    dvec<int> fsize(F);
+    parallel_chunks(F, FC, [&](int, int64_t f0, int64_t f1) {
+        int64_t buf[4];
+        for (int64_t f = f0; f < f1; ++f) {
+            int k = item_nodes(first_item[f], m->owner[f], buf);
+            fsize[f] = k;
+            for (int i = 0; i < kmax_face; ++i) m->face_nodes[f * kmax_face + i] = i < k ? buf[i] : -1;
+        }
+    });
     int64_t ni = 0;
     for (int64_t f = 0; f < F; ++f) ni += (m->neighbour[f] >= 0);
     m->n_internal = ni;
     // ---- face geometry ----
-    m->area.assign(F, 0.0);
-    m->normal.assign(F * D, 0.0);
-    m->fcenter.assign(F * D, 0.0);
-    for (int64_t f = 0; f < F; ++f) {
-        const int64_t* fn = &m->face_nodes[f * kmax_face];
-        double* nr = &m->normal[f * D];
-        double* fc = &m->fcenter[f * D];
-        const double* cc = &m->ccenter[m->owner[f] * D];
-        if (D == 2) {
-            const double* p0 = nodes + fn[0] * 2;
-            const double* p1 = nodes + fn[1] * 2;
-            fc[0] = 0.5 * (p0[0] + p1[0]);
-            fc[1] = 0.5 * (p0[1] + p1[1]);
-            double dx = p1[0] - p0[0], dy = p1[1] - p0[1];
-            double len = std::sqrt(dx * dx + dy * dy);
-            nr[0] = dy;
-            nr[1] = -dx;
-            if (len > 1e-15) {
-                nr[0] = nr[0] / len;
-                nr[1] = nr[1] / len;
-            }
-            double t0 = fc[0] - cc[0], t1 = fc[1] - cc[1];
-            double dot = nr[0] * t0 + nr[1] * t1;
-            if (dot < 0) {
-                nr[0] = -nr[0];
-                nr[1] = -nr[1];
-            }
-            m->area[f] = len;
-        } else {
-            int k = fsize[f];
-            for (int d = 0; d < 3; ++d) {
-                double s = nodes[fn[0] * 3 + d];
-                for (int i = 1; i < k; ++i) s = s + nodes[fn[i] * 3 + d];
-                fc[d] = s / (double)k;
-            }
-            double nx = 0.0, ny = 0.0, nz = 0.0;
-            for (int i = 0; i < k; ++i) {
-                const double* pi = nodes + fn[i] * 3;
-                const double* pj = nodes + fn[(i + 1) % k] * 3;
-                nx = nx + (pi[1] - pj[1]) * (pi[2] + pj[2]);
-                ny = ny + (pi[2] - pj[2]) * (pi[0] + pj[0]);
-                nz = nz + (pi[0] - pj[0]) * (pi[1] + pj[1]);
-            }
-            double a = std::sqrt(nx * nx + ny * ny + nz * nz);
-            nr[0] = nx;
-            nr[1] = ny;
-            nr[2] = nz;
-            if (a > 1e-15) {
-                nr[0] = nr[0] / a;
-                nr[1] = nr[1] / a;
-                nr[2] = nr[2] / a;
-            }
-            m->area[f] = a * 0.5;
-            double dot = nr[0] * (fc[0] - cc[0]) + nr[1] * (fc[1] - cc[1]) + nr[2] * (fc[2] - cc[2]);
-            if (dot < 0) {
-                nr[0] = -nr[0];
-                nr[1] = -nr[1];
-                nr[2] = -nr[2];
+    m->area.resize(F);
+    m->normal.resize(F * D);
+    m->fcenter.resize(F * D);
+    parallel_chunks(F, FC, [&](int, int64_t f0, int64_t f1) {
+        for (int64_t f = f0; f < f1; ++f) {
+            const int64_t* fn = &m->face_nodes[f * kmax_face];
+            double* nr = &m->normal[f * D];
+            double* fc = &m->fcenter[f * D];
+            const double* cc = &m->ccenter[m->owner[f] * D];
+            if (D == 2) {
+                const double* p0 = nodes + fn[0] * 2;
+                const double* p1 = nodes + fn[1] * 2;
+                fc[0] = 0.5 * (p0[0] + p1[0]);
+                fc[1] = 0.5 * (p0[1] + p1[1]);
+                double dx = p1[0] - p0[0], dy = p1[1] - p0[1];
+                double len = std::sqrt(dx * dx + dy * dy);
+                nr[0] = dy;
+                nr[1] = -dx;
+                if (len > 1e-15) {
+                    nr[0] = nr[0] / len;
+                    nr[1] = nr[1] / len;
+                }
+                double t0 = fc[0] - cc[0], t1 = fc[1] - cc[1];
+                double dot = nr[0] * t0 + nr[1] * t1;
+                if (dot < 0) {
+                    nr[0] = -nr[0];
+                    nr[1] = -nr[1];
+                }
+                m->area[f] = len;
+            } else {
+                int k = fsize[f];
+                for (int d = 0; d < 3; ++d) {
+                    double s = nodes[fn[0] * 3 + d];
+                    for (int i = 1; i < k; ++i) s = s + nodes[fn[i] * 3 + d];
+                    fc[d] = s / (double)k;
+                }
+                double nx = 0.0, ny = 0.0, nz = 0.0;
+                for (int i = 0; i < k; ++i) {
+                    const double* pi = nodes + fn[i] * 3;
+                    const double* pj = nodes + fn[(i + 1) % k] * 3;
+                    nx = nx + (pi[1] - pj[1]) * (pi[2] + pj[2]);
+                    ny = ny + (pi[2] - pj[2]) * (pi[0] + pj[0]);
+                    nz = nz + (pi[0] - pj[0]) * (pi[1] + pj[1]);
+                }
+                double a = std::sqrt(nx * nx + ny * ny + nz * nz);
+                nr[0] = nx;
+                nr[1] = ny;
+                nr[2] = nz;
+                if (a > 1e-15) {
+                    nr[0] = nr[0] / a;
+                    nr[1] = nr[1] / a;
+                    nr[2] = nr[2] / a;
+                }
+                m->area[f] = a * 0.5;
+                double dot = nr[0] * (fc[0] - cc[0]) + nr[1] * (fc[1] - cc[1]) + nr[2] * (fc[2] - cc[2]);
+                if (dot < 0) {
+                    nr[0] = -nr[0];
+                    nr[1] = -nr[1];
+                    nr[2] = -nr[2];
+                }
             }
         }
-    }
+    });
     if (is3d) {
-        for (int64_t c = 0; c < n; ++c) {
-            double vol = 0.0;
-            const double* cc = &m->ccenter[c * 3];
-            for (int j = 0; j < kc; ++j) {
-                int64_t f = m->cell_faces[c * kc + j];
-                if (f < 0) continue;
-                const double* fc = &m->fcenter[f * 3];
-                const double* nr = &m->normal[f * 3];
-                double sgn = 1.0;
-                double tdot = nr[0] * (fc[0] - cc[0]) + nr[1] * (fc[1] - cc[1]) + nr[2] * (fc[2] - cc[2]);
-                if (tdot < 0) sgn = -1.0;
-                double d = fc[0] * nr[0] + fc[1] * nr[1] + fc[2] * nr[2];
-                vol = vol + sgn * d * m->area[f];
+        parallel_chunks(n, CC, [&](int, int64_t c0, int64_t c1) {
+            for (int64_t c = c0; c < c1; ++c) {
+                double vol = 0.0;
+                const double* cc = &m->ccenter[c * 3];
+                for (int j = 0; j < kc; ++j) {
+                    int64_t f = m->cell_faces[c * kc + j];
+                    if (f < 0) continue;
+                    const double* fc = &m->fcenter[f * 3];
+                    const double* nr = &m->normal[f * 3];
+                    double sgn = 1.0;
+                    double tdot = nr[0] * (fc[0] - cc[0]) + nr[1] * (fc[1] - cc[1]) + nr[2] * (fc[2] - cc[2]);
+                    if (tdot < 0) sgn = -1.0;
+                    double d = fc[0] * nr[0] + fc[1] * nr[1] + fc[2] * nr[2];
+                    vol = vol + sgn * d * m->area[f];
+                }
+                vol = std::fabs(vol) / 3.0;
+                if (vol < 1e-30) vol = 1e-30;
+                m->volume[c] = vol;
             }
-            vol = std::fabs(vol) / 3.0;
-            if (vol < 1e-30) vol = 1e-30;
-            m->volume[c] = vol;
-        }
+        });
     }
     // ---- boundary tagging ----
     m->face_patch.assign(F, -1);
@@ -480,7 +651,11 @@ int kcfd_mesh_info(const kcfd_host_mesh* m, int64_t* info) {
 int kcfd_mesh_export(const kcfd_host_mesh* m, kcfd_mesh_export_t* o) {
     KCFD_REQUIRE(m && o, "kcfd_mesh_export: NULL argument");
     auto cp = [](auto* dst, const auto& v) {
-        if (dst) std::memcpy(dst, v.data(), v.size() * sizeof(v[0]));
+        if (!dst) return;
+        const int64_t bytes = (int64_t)(v.size() * sizeof(v[0]));
+        char* d = reinterpret_cast<char*>(dst);
+        const char* s = reinterpret_cast<const char*>(v.data());
+        parallel_chunks(bytes, n_chunks(bytes / 64), [&](int, int64_t b, int64_t e) { std::memcpy(d + b, s + b, e - b); });
     };
     cp(o->owner, m->owner);
     cp(o->neighbour, m->neighbour);

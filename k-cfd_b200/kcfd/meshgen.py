@@ -70,6 +70,10 @@ def tri_channel_arrays(Lx, Ly, nx, ny):
     return nodes, cells, bd
 
 
+# corners of each hex face, in the reference's face order and node order
+HEX_FACE_CORNERS = np.array([[0, 3, 2, 1], [4, 5, 6, 7], [0, 1, 5, 4], [2, 3, 7, 6], [0, 4, 7, 3], [1, 2, 6, 5]])
+
+
 def hex_box_arrays(Lx, Ly, Lz, nx, ny, nz, names=None):
     """Structured hexes (k, j, i order), six faces per cell in the reference order."""
     names = names or CHANNEL_3D_NAMES
@@ -80,13 +84,13 @@ def hex_box_arrays(Lx, Ly, Lz, nx, ny, nz, names=None):
 
     k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
     nodes = np.stack([i.reshape(-1) * dx, j.reshape(-1) * dy, k.reshape(-1) * dz], axis=1)
-    kk, jj, ii = (a.reshape(-1) for a in np.meshgrid(np.arange(nz), np.arange(ny), np.arange(nx), indexing="ij"))
-    n0, n1, n2, n3 = nid(ii, jj, kk), nid(ii + 1, jj, kk), nid(ii + 1, jj + 1, kk), nid(ii, jj + 1, kk)
-    n4, n5, n6, n7 = nid(ii, jj, kk + 1), nid(ii + 1, jj, kk + 1), nid(ii + 1, jj + 1, kk + 1), nid(ii, jj + 1, kk + 1)
-    cells = np.stack([n0, n1, n2, n3, n4, n5, n6, n7], axis=1)
-    cfaces = np.stack([np.stack([n0, n3, n2, n1], 1), np.stack([n4, n5, n6, n7], 1),
-                       np.stack([n0, n1, n5, n4], 1), np.stack([n2, n3, n7, n6], 1),
-                       np.stack([n0, n4, n7, n3], 1), np.stack([n1, n2, n6, n5], 1)], axis=1)
+    # cell (i, j, k) -> its corner n0 = nid(i, j, k); corners n0..n7 are fixed offsets from it
+    base = nid(*np.meshgrid(np.arange(nx), np.arange(ny), np.arange(nz), indexing="ij")).transpose(2, 1, 0).reshape(-1)
+    row, plane = nx + 1, (nx + 1) * (ny + 1)
+    corner = np.array([0, 1, 1 + row, row, plane, plane + 1, plane + 1 + row, plane + row], dtype=np.int64)
+    cells = base[:, None] + corner[None, :]
+    # faces in the reference's order: z-, z+, y-, y+, x-, x+ (node lists as above)
+    cfaces = base[:, None, None] + corner[HEX_FACE_CORNERS][None, :, :]
     bd = {}
     K, J = (a.reshape(-1) for a in np.meshgrid(np.arange(nz), np.arange(ny), indexing="ij"))
     bd[names.get("x_min", "inlet")] = np.stack([nid(0, J, K), nid(0, J, K + 1), nid(0, J + 1, K + 1), nid(0, J + 1, K)], 1)

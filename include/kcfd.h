@@ -125,6 +125,39 @@ typedef struct {
 int  kcfd_mesh_export(const kcfd_host_mesh* m, kcfd_mesh_export_t* out);
 void kcfd_mesh_free(kcfd_host_mesh* m);
 
+/* Device face layout of a built mesh (host arrays in, host arrays out; no device
+ * call). Faces are ordered colour by colour (internal colours first), by reference
+ * face id inside a colour; per face, the geometric factors of the SIMPLE kernels with
+ * the reference's formulas: gc = dN / (dO + dN) (0.5 when dO + dN <= 1e-30;
+ * models/single_phase.py:380-388), dlen = |d_PN| on internal faces and |x_f - x_P| on
+ * boundary faces (:197), dorth = max(|d_PN . n|, 0.1 |d_PN|) (:166-175); and the faces
+ * of every cell in ascending reference id as device face indices. Row norms and dots
+ * sum their components left to right. Inputs are the kcfd_mesh_export arrays in
+ * reference face order; n_colors = internal + boundary face colours.               */
+typedef struct {
+    int64_t* order;      /* [F] reference face id of each device face                 */
+    int32_t* color_ptr;  /* [n_colors + 1] device face range of each colour           */
+    int32_t* owner;      /* [F]                                                       */
+    int32_t* neigh;      /* [Fi]                                                      */
+    double*  area;       /* [F]                                                       */
+    double*  normal;     /* [F * ndim]                                                */
+    double*  fcenter;    /* [F * ndim]                                                */
+    double*  gc;         /* [Fi]                                                      */
+    double*  dlen;       /* [F]                                                       */
+    double*  dorth;      /* [Fi]                                                      */
+    int32_t* slot_on;    /* [Fi]                                                      */
+    int32_t* slot_no;    /* [Fi]                                                      */
+    int32_t* cf_ptr;     /* [n + 1]                                                   */
+    int32_t* cf_face;    /* [n * max_cell_faces]; the first cf_ptr[n] entries are set */
+} kcfd_face_layout_t;
+
+int kcfd_mesh_device_layout(int32_t ndim, int64_t n_cells, int64_t n_faces, int64_t n_internal,
+                            int32_t n_colors, int32_t max_cell_faces, const int64_t* owner,
+                            const int64_t* neighbour, const int32_t* face_color, const double* ccenter,
+                            const double* fcenter, const double* normal, const double* area,
+                            const int32_t* slot_on, const int32_t* slot_no, const int64_t* cell_faces,
+                            kcfd_face_layout_t* out);
+
 /* ------------------------------------------------------------- CSR / SpMV ---- */
 /* Device CSR (int32 indices). vals64 and/or vals32 may be set; kernels read the
  * precision they are asked for.                                                   */

@@ -633,6 +633,150 @@ int kcfd_mesh_build(int32_t ndim, int64_t n_nodes, const double* nodes, int64_t 
     return KCFD_OK;
 }
 
+int kcfd_mesh_device_layout(int32_t ndim, int64_t n_cells, int64_t n_faces, int64_t n_internal,
+                            int32_t n_colors, int32_t max_cell_faces, const int64_t* owner,
+                            const int64_t* neighbour, const int32_t* face_color, const double* ccenter,
+                            const double* fcenter, const double* normal, const double* area,
+                            const int32_t* slot_on, const int32_t* slot_no, const int64_t* cell_faces,
+                            kcfd_face_layout_t* o) {
+    KCFD_REQUIRE(o && owner && neighbour && face_color && ccenter && fcenter && normal && area && slot_on &&
+                     slot_no && cell_faces,
+                 "kcfd_mesh_device_layout: NULL argument");
+    KCFD_REQUIRE(o->order && o->color_ptr && o->owner && o->neigh && o->area && o->normal && o->fcenter && o->gc &&
+                     o->dlen && o->dorth && o->slot_on && o->slot_no && o->cf_ptr && o->cf_face,
+                 "kcfd_mesh_device_layout: NULL output array");
+    KCFD_REQUIRE(ndim == 2 || ndim == 3, "kcfd_mesh_device_layout: ndim must be 2 or 3 (got %d)", ndim);
+    KCFD_REQUIRE(n_cells > 0 && n_cells < 0x7fffffffLL && n_faces > 0 && n_faces < 0x7fffffffLL && n_internal >= 0 &&
+                     n_internal <= n_faces && n_colors > 0 && max_cell_faces >= 0,
+                 "kcfd_mesh_device_layout: bad sizes");
+    const int64_t F = n_faces, Fi = n_internal, n = n_cells;
+    const int D = ndim, NC = n_colors;
+    // ---- faces ordered by colour, by reference id inside a colour (stable counting sort) ----
+    const int FC = n_chunks(F);
+    std::vector<char> bad(FC, 0);
+    std::vector<int64_t> cnt((size_t)FC * NC, 0);
+    parallel_chunks(F, FC, [&](int t, int64_t f0, int64_t f1) {
+        int64_t* c = &cnt[(size_t)t * NC];
+        for (int64_t f = f0; f < f1; ++f) {
+            const int32_t k = face_color[f];
+            if (k < 0 || k >= NC || owner[f] < 0 || owner[f] >= n || neighbour[f] < -1 || neighbour[f] >= n) {
+                bad[t] = 1;
+                return;
+            }
+            ++c[k];
+        }
+    });
+    for (int t = 0; t < FC; ++t)
+        KCFD_REQUIRE(!bad[t], "kcfd_mesh_device_layout: face colour, owner or neighbour out of range");
+    std::vector<int64_t> start((size_t)FC * NC);
+    int64_t run = 0;
+    for (int k = 0; k < NC; ++k) {
+        o->color_ptr[k] = (int32_t)run;
+        for (int t = 0; t < FC; ++t) {
+            start[(size_t)t * NC + k] = run;
+            run += cnt[(size_t)t * NC + k];
+        }
+    }
+    o->color_ptr[NC] = (int32_t)run;
+    parallel_chunks(F, FC, [&](int t, int64_t f0, int64_t f1) {
+        int64_t* s = &start[(size_t)t * NC];
+        for (int64_t f = f0; f < f1; ++f) o->order[s[face_color[f]]++] = f;
+    });
+    // ---- per device face: gathers and geometric factors ----
+    auto norm = [D](const double* v) {
+        double s = v[0] * v[0];
+        for (int k = 1; k < D; ++k) s = s + v[k] * v[k];
+        return std::sqrt(s);
+    };
+    std::fill(bad.begin(), bad.end(), 0);
+    parallel_chunks(F, FC, [&](int t, int64_t d0, int64_t d1) {
+        for (int64_t d = d0; d < d1; ++d) {
+            const int64_t f = o->order[d];
+            const int64_t ow = owner[f], nb = neighbour[f];
+            if ((d < Fi) != (nb >= 0)) {  // internal colours must come first
+                bad[t] = 1;
+                return;
+            }
+            o->owner[d] = (int32_t)ow;
+            o->area[d] = area[f];
+            const double* cp = ccenter + ow * D;
+            const double* fc = fcenter + f * D;
+            const double* nr = normal + f * D;
+            double eO[3];
+            for (int k = 0; k < D; ++k) {
+                o->normal[d * D + k] = nr[k];
+                o->fcenter[d * D + k] = fc[k];
+                eO[k] = fc[k] - cp[k];
+            }
+            const double dO = norm(eO);
+            if (d >= Fi) {
+                o->dlen[d] = dO;
+                continue;
+            }
+            o->neigh[d] = (int32_t)nb;
+            o->slot_on[d] = slot_on[f];
+            o->slot_no[d] = slot_no[f];
+            const double* cn = ccenter + nb * D;
+            double dv[3], eN[3];
+            for (int k = 0; k < D; ++k) {
+                dv[k] = cn[k] - cp[k];
+                eN[k] = fc[k] - cn[k];
+            }
+            const double dint = norm(dv);
+            double dn = dv[0] * nr[0];
+            for (int k = 1; k < D; ++k) dn = dn + dv[k] * nr[k];
+            const double a = std::fabs(dn), b = 0.1 * dint;
+            o->dorth[d] = (a != a) ? a : (b != b) ? b : (a >= b ? a : b);  // NaN-propagating max
+            o->dlen[d] = dint;
+            const double dN = norm(eN), sum = dO + dN;
+            o->gc[d] = (sum > 1e-30) ? dN / sum : 0.5;
+        }
+    });
+    for (int t = 0; t < FC; ++t)
+        KCFD_REQUIRE(!bad[t], "kcfd_mesh_device_layout: internal faces must take the first colours");
+    // ---- faces of each cell, ascending reference id, as device indices ----
+    std::vector<int32_t> dev_of_ref(F);
+    parallel_chunks(F, FC, [&](int, int64_t d0, int64_t d1) {
+        for (int64_t d = d0; d < d1; ++d) dev_of_ref[o->order[d]] = (int32_t)d;
+    });
+    const int kc = max_cell_faces, CC = n_chunks(n);
+    std::vector<int32_t> nvalid(n);
+    std::vector<char> badc(CC, 0);
+    parallel_chunks(n, CC, [&](int t, int64_t c0, int64_t c1) {
+        for (int64_t c = c0; c < c1; ++c) {
+            int k = 0;
+            for (int j = 0; j < kc; ++j) {
+                const int64_t v = cell_faces[c * kc + j];
+                if (v >= F) {
+                    badc[t] = 1;
+                    return;
+                }
+                k += (v >= 0);
+            }
+            nvalid[c] = k;
+        }
+    });
+    for (int t = 0; t < CC; ++t) KCFD_REQUIRE(!badc[t], "kcfd_mesh_device_layout: cell face id out of range");
+    int64_t total = 0;
+    o->cf_ptr[0] = 0;
+    for (int64_t c = 0; c < n; ++c) {
+        total += nvalid[c];
+        KCFD_REQUIRE(total < 0x7fffffffLL, "kcfd_mesh_device_layout: too many cell faces");
+        o->cf_ptr[c + 1] = (int32_t)total;
+    }
+    parallel_chunks(n, CC, [&](int, int64_t c0, int64_t c1) {
+        std::vector<int64_t> tmp(kc > 0 ? kc : 1);
+        for (int64_t c = c0; c < c1; ++c) {
+            int m = 0;
+            for (int j = 0; j < kc; ++j)
+                if (cell_faces[c * kc + j] >= 0) tmp[m++] = cell_faces[c * kc + j];
+            std::sort(tmp.begin(), tmp.begin() + m);
+            for (int i = 0; i < m; ++i) o->cf_face[o->cf_ptr[c] + i] = dev_of_ref[tmp[i]];
+        }
+    });
+    return KCFD_OK;
+}
+
 int kcfd_mesh_info(const kcfd_host_mesh* m, int64_t* info) {
     KCFD_REQUIRE(m && info, "kcfd_mesh_info: NULL argument");
     info[0] = m->n_faces;

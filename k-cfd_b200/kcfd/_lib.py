@@ -34,6 +34,12 @@ class MeshExport(C.Structure):
                                   "diag_slot", "face_color", "cell_color", "level_natural")]
 
 
+class FaceLayout(C.Structure):
+    """kcfd_face_layout_t: output arrays of kcfd_mesh_device_layout."""
+    _fields_ = [(n, vp) for n in ("order", "color_ptr", "owner", "neigh", "area", "normal", "fcenter", "gc", "dlen",
+                                  "dorth", "slot_on", "slot_no", "cf_ptr", "cf_face")]
+
+
 class Csr(C.Structure):
     _fields_ = [("n", i32), ("nnz", i32), ("indptr", vp), ("indices", vp), ("vals64", vp), ("vals32", vp)]
 
@@ -59,6 +65,8 @@ SIGNATURES = {
     "kcfd_mesh_info": (i32, [vp, P_i64]),
     "kcfd_mesh_export": (i32, [vp, C.POINTER(MeshExport)]),
     "kcfd_mesh_free": (None, [vp]),
+    "kcfd_mesh_device_layout": (i32, [i32, i64, i64, i64, i32, i32, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp,
+                                      C.POINTER(FaceLayout)]),
     "kcfd_cast_f64_f32": (i32, [i64, vp, vp, vp]),
     "kcfd_spmv_f64": (i32, [C.POINTER(Csr), vp, vp, i32, vp]),
     "kcfd_spmv_f32": (i32, [C.POINTER(Csr), vp, vp, i32, vp]),

@@ -34,8 +34,35 @@ class BCDesc(C.Structure):
                 ("has_p_dirichlet", C.c_int32), ("pad", C.c_int32)]
 
 
-def _norm_rows(v):
-    return np.sqrt((v * v).sum(axis=1))
+def device_layout(mesh):
+    """Host arrays of the device face layout (kcfd_mesh_device_layout, no device call):
+    faces colour by colour, internal colours first, by reference face id inside a
+    colour; owner / neighbour / geometry gathered in that order; gc, dlen, dorth; the
+    faces of each cell in ascending reference id as device face indices."""
+    L = _lib.lib()
+    D, n, F, Fi = mesh.ndim, mesh.n_cells, mesh.n_faces, mesh.n_internal_faces
+    nc = mesh.n_int_colors + mesh.n_bnd_colors
+    kcf = mesh.cell_faces.shape[1]
+    out = {"order": np.empty(F, np.int64), "color_ptr": np.empty(nc + 1, np.int32), "owner": np.empty(F, np.int32),
+           "neigh": np.empty(Fi, np.int32), "area": np.empty(F), "normal": np.empty((F, D)),
+           "fcenter": np.empty((F, D)), "gc": np.empty(Fi), "dlen": np.empty(F), "dorth": np.empty(Fi),
+           "slot_on": np.empty(Fi, np.int32), "slot_no": np.empty(Fi, np.int32), "cf_ptr": np.empty(n + 1, np.int32),
+           "cf_face": np.empty(max(n * kcf, 1), np.int32)}
+    lay = _lib.FaceLayout(**{k: v.ctypes.data for k, v in out.items()})
+
+    def arg(a, dt):
+        a = np.ascontiguousarray(a, dtype=dt)
+        keep.append(a)
+        return a.ctypes.data
+
+    keep = []
+    _lib.check(L.kcfd_mesh_device_layout(
+        D, n, F, Fi, nc, kcf, arg(mesh.owner, np.int64), arg(mesh.neighbour, np.int64),
+        arg(mesh.face_color, np.int32), arg(mesh.ccenter, np.float64), arg(mesh.fcenter, np.float64),
+        arg(mesh.normal, np.float64), arg(mesh.area, np.float64), arg(mesh.slot_on, np.int32),
+        arg(mesh.slot_no, np.int32), arg(mesh.cell_faces, np.int64), C.byref(lay)), "kcfd_mesh_device_layout")
+    out["cf_face"] = out["cf_face"][:int(out["cf_ptr"][n])]
+    return out
 
 
 class DeviceMesh:
@@ -46,28 +73,12 @@ class DeviceMesh:
         self.n_cells = n = mesh.n_cells
         F, Fi = mesh.n_faces, mesh.n_internal_faces
         self.n_faces, self.n_internal, self.n_boundary = F, Fi, F - Fi
-        col = mesh.face_color.astype(np.int64)
-        order = np.lexsort((np.arange(F), col))
+        lay = device_layout(mesh)
+        order, color_ptr = lay["order"], lay["color_ptr"]
         nci, ncb = mesh.n_int_colors, mesh.n_bnd_colors
-        color_ptr = np.searchsorted(col[order], np.arange(nci + ncb + 1)).astype(np.int32)
         assert color_ptr[nci] == Fi and color_ptr[-1] == F
         self.face_ref = order
         self.color_ptr = color_ptr
-        o = mesh.owner[order]
-        nb = mesh.neighbour[order][:Fi]
-        cc = mesh.ccenter
-        fc = mesh.fcenter[order]
-        nrm = mesh.normal[order]
-        nb_full = np.concatenate([nb, o[Fi:]])
-        dvec = cc[nb_full] - cc[o]
-        d_int = _norm_rows(dvec[:Fi])
-        d_bnd = _norm_rows(fc[Fi:] - cc[o[Fi:]])
-        dn = (dvec[:Fi] * nrm[:Fi]).sum(axis=1)
-        dorth = np.maximum(np.abs(dn), 0.1 * d_int)
-        dO = _norm_rows(fc[:Fi] - cc[o[:Fi]])
-        dN = _norm_rows(fc[:Fi] - cc[nb])
-        t = dO + dN
-        gc = np.where(t > 1e-30, dN / np.where(t > 1e-30, t, 1.0), 0.5)
         # boundary face bookkeeping: device boundary slot of each (patch, local index)
         bref = order[Fi:]
         pos_of_ref = np.full(F, -1, dtype=np.int64)
@@ -79,22 +90,15 @@ class DeviceMesh:
 
         i32, f64 = np.int32, np.float64
         self.t = {
-            "owner": dev(o, i32), "neigh": dev(nb, i32), "area": dev(mesh.area[order], f64),
-            "normal": dev(nrm, f64), "fcenter": dev(fc, f64), "ccenter": dev(cc, f64),
-            "volume": dev(mesh.volume, f64), "gc": dev(gc, f64),
-            "dlen": dev(np.concatenate([d_int, d_bnd]), f64), "dorth": dev(dorth, f64),
-            "slot_on": dev(mesh.slot_on[order][:Fi], i32), "slot_no": dev(mesh.slot_no[order][:Fi], i32),
+            "owner": dev(lay["owner"], i32), "neigh": dev(lay["neigh"], i32), "area": dev(lay["area"], f64),
+            "normal": dev(lay["normal"], f64), "fcenter": dev(lay["fcenter"], f64), "ccenter": dev(mesh.ccenter, f64),
+            "volume": dev(mesh.volume, f64), "gc": dev(lay["gc"], f64), "dlen": dev(lay["dlen"], f64),
+            "dorth": dev(lay["dorth"], f64), "slot_on": dev(lay["slot_on"], i32), "slot_no": dev(lay["slot_no"], i32),
             "diag_slot": dev(mesh.diag_slot, i32), "indptr": dev(mesh.indptr, i32),
             "indices": dev(mesh.indices, i32), "face_ref": dev(order, i32),
+            # faces of each cell, ascending reference face id, as device face indices
+            "cf_ptr": dev(lay["cf_ptr"], i32), "cf_face": dev(lay["cf_face"], i32),
         }
-        # faces of each cell, ascending reference face id, as device face indices
-        dev_of_ref = np.empty(F, dtype=np.int64)
-        dev_of_ref[order] = np.arange(F)
-        cf = np.sort(np.where(mesh.cell_faces >= 0, mesh.cell_faces, np.iinfo(np.int64).max), axis=1)
-        valid = cf != np.iinfo(np.int64).max
-        cf_ptr = np.concatenate([[0], np.cumsum(valid.sum(axis=1))])
-        self.t["cf_ptr"] = dev(cf_ptr, i32)
-        self.t["cf_face"] = dev(dev_of_ref[cf[valid]], i32)
         self._color_ptr_np = np.ascontiguousarray(color_ptr, dtype=np.int32)
         d = DMeshDesc()
         d.ndim, d.n_cells, d.n_faces, d.n_internal = D, n, F, Fi

@@ -416,7 +416,7 @@ def run_c4(args):
     collective."""
     import torch
     import torch.distributed as dist
-    from kcfd.batch import BatchSolver, lpt_shards, p_prime_batch, p_prime_host, p_prime_sizes
+    from kcfd.batch import BatchSolver, lpt_shards, p_prime_batch, p_prime_sizes
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     if world > 1:

@@ -3,7 +3,6 @@ worked sizes of the 128^3 cavity (host only): one FP64 SpMV of the p' matrix is
 nnz (8 + 4) + 4 (n + 1) + 2 n 8 = 216.9 MB; one BiCGSTAB + ILU(0) iteration is
 2 SpMV + 2 ILU applies + 19 vectors = 1,270.3 MB; the whole outer iteration adds the
 mass flux, gradient, MUSCL and assembly terms to the two solves."""
-import numpy as np
 
 import bench
 

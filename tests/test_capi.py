@@ -34,7 +34,6 @@ def test_library_exports_every_declared_symbol():
 
 def test_last_error_roundtrip():
     from kcfd import _lib
-    import numpy as np
     L = _lib.lib()
     rc = L.kcfd_mesh_build(5, 0, None, 0, None, None, None, None, None, None, 0, None, None, None,
                            ctypes.byref(ctypes.c_void_p()))

@@ -1,6 +1,5 @@
 """The case-16 helper reproduces the reference's own case-16 matrix (golden)."""
 import numpy as np
-from scipy import sparse
 
 from conftest import load_golden
 from case16 import channel_mesh, convdiff_system

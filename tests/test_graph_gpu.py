@@ -1,7 +1,6 @@
 """CUDA-graph capture of kcfd calls through the C ABI (kcfd_graph_*, kcfd.solver.DeviceGraph):
 a captured pair of SpMVs and a captured solver set-up + solve (persistent grid kernel),
 replayed, give bitwise the results of the same calls issued directly."""
-import numpy as np
 import pytest
 
 from case16 import channel_mesh, convdiff_system

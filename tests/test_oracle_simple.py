@@ -1,6 +1,5 @@
 """Oracle SIMPLE and linear solvers vs the reference's own outputs (golden fixtures)."""
 import numpy as np
-import pytest
 from scipy import sparse
 import scipy.sparse.linalg as spla
 

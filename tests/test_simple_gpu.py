@@ -9,7 +9,7 @@ against the FP64 form with the same 1e-6 bar.
 import numpy as np
 import pytest
 
-from conftest import load_golden, golden_inputs
+from conftest import load_golden
 
 pytestmark = pytest.mark.gpu
 

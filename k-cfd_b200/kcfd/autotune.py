@@ -27,16 +27,22 @@ def _load():
     p = os.environ.get("KCFD_TUNE_CACHE")
     if p and os.path.exists(p):
         try:
-            _CACHE.update(json.load(open(p)))
+            with open(p) as f:
+                _CACHE.update(json.load(f))
         except (OSError, ValueError):
             pass
 
 
 def _save():
+    """Write the cache next to its final name, then rename it into place, so that a
+    reader (another process tuning the same shapes) never sees a partial file."""
     p = os.environ.get("KCFD_TUNE_CACHE")
     if p:
+        tmp = f"{p}.{os.getpid()}.tmp"
         try:
-            json.dump(_CACHE, open(p, "w"))
+            with open(tmp, "w") as f:
+                json.dump(_CACHE, f)
+            os.replace(tmp, p)
         except OSError:
             pass
 

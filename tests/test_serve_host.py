@@ -143,3 +143,4 @@ def test_requests_and_footprints():
         assert footprint_bytes(nd, hi, "mixed") != footprint_bytes(nd, hi, "fp64")
     with pytest.raises(ValueError):
         Server(policy="lifo")
+

@@ -117,7 +117,8 @@ class ClockSampler:
 def measured_peak():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
-        d = json.load(open(p))
+        with open(p) as f:
+            d = json.load(f)
         return float(d["hbm_gbs"]), "measured"
     return 6650.0, "fallback"
 

@@ -279,6 +279,56 @@ def make_simple(out):
     np.savez_compressed(os.path.join(out, "simple.npz"), **d)
 
 
+CHANNEL_MU, CHANNEL_DPDX = 0.01, -1.0
+
+
+def channel_setup(sv, mesh, H):
+    """Poiseuille channel of verification/case1_poiseuille.py:67-99 (and case7): parabolic
+    inlet profile per inlet face, zero-gradient velocity and p = 0 at the outlet, no-slip
+    walls, u started at half the analytical maximum."""
+    ndim = mesh.ndim
+    fids = mesh.boundary_patches["inlet"]
+    y = np.array([mesh.faces[f].center[1] for f in fids])
+    u = np.zeros((len(fids), ndim))
+    u[:, 0] = -CHANNEL_DPDX / (2.0 * CHANNEL_MU) * y * (H - y)
+    sv.U.boundary_values["inlet"] = u
+    sv.set_velocity_bc("inlet", "dirichlet")
+    sv.set_velocity_bc("outlet", "zero_gradient")
+    for w in ("wall_bottom", "wall_top"):
+        sv.set_velocity_bc(w, "dirichlet", [0.0] * ndim)
+        sv.set_pressure_bc(w, "zero_gradient")
+    sv.set_pressure_bc("inlet", "zero_gradient")
+    sv.set_pressure_bc("outlet", "dirichlet", 0.0)
+    sv.U.values[:, 0] = -CHANNEL_DPDX * H ** 2 / (8.0 * CHANNEL_MU) * 0.5
+    sv.U.values[:, 1] = 0.0
+
+
+def make_channel(out):
+    """SIMPLESolver on the channel set-up of the reference's Poiseuille cases: quads
+    (generate_channel_mesh(1.0, 0.1, 20, 8), alpha 0.7 / 0.3) and split-quad triangles
+    (generate_triangle_channel_mesh(0.2, 0.1, 8, 4), alpha 0.2 / 0.05), a fixed number of
+    outer iterations each (tol 0)."""
+    from mesh.mesh_generator import generate_channel_mesh, generate_triangle_channel_mesh
+    from models.single_phase import SIMPLESolver
+    import contextlib
+    import io
+    d = {}
+    for tag, mk, H, au, ap, iters in (("quad", lambda: generate_channel_mesh(1.0, 0.1, 20, 8), 0.1, 0.7, 0.3, 15),
+                                      ("tri", lambda: generate_triangle_channel_mesh(0.2, 0.1, 8, 4), 0.1, 0.2, 0.05,
+                                       15)):
+        m = mk()
+        sv = SIMPLESolver(m, rho=1.0, mu=CHANNEL_MU)
+        channel_setup(sv, m, H)
+        sv.alpha_u, sv.alpha_p, sv.max_outer_iter, sv.tol = au, ap, iters, 0.0
+        with contextlib.redirect_stdout(io.StringIO()):
+            r = sv.solve_steady()
+        d[tag + "_U"] = sv.U.values.copy()
+        d[tag + "_p"] = sv.p.values.copy()
+        d[tag + "_res"] = np.array(r["residuals"])
+        d[tag + "_iters"] = np.int64(iters)
+    np.savez_compressed(os.path.join(out, "channel.npz"), **d)
+
+
 def two_fluid_setup(sv, mesh, seed):
     """Shared set-up of the two-fluid fixtures (also restated by the oracle and the
     device tests): inlet / outlet / heated bottom wall / adiabatic walls, seeded
@@ -450,6 +500,8 @@ def main():
         make_solvers(a.out)
     if want("simple"):
         make_simple(a.out)
+    if want("channel"):
+        make_channel(a.out)
     if want("two_fluid"):
         make_two_fluid(a.out, meshes)
     if want("partitions"):

@@ -1,0 +1,87 @@
+"""The oracle's SIMPLE restatement against the reference's own verification criteria.
+Host only.
+
+Poiseuille flow between plates, u(y) = -dpdx / (2 mu) y (H - y), with a parabolic inlet,
+outlet p = 0, no-slip walls, started from u = u_max / 2:
+
+- case 1 (verification/case1_poiseuille.py:47-99,119): 50 x 20 quads, L = 1, H = 0.1,
+  alpha_u 0.7, alpha_p 0.3, at most 500 outer iterations to 1e-5. The profile is
+  SIMPLESolver.get_velocity_at_y(0.8) (models/single_phase.py:390-405). Passes when
+  the relative L2 error is below 1 %.
+- case 7 (verification/case7_unstructured.py:38-112): 20 x 10 split quads (400
+  triangles), Lx = 0.2, Ly = 0.1, alpha_u 0.2, alpha_p 0.05, at most 3000 iterations
+  to 1e-4. The profile is every cell within 2 dx of x = 0.8 Lx. Passes below 10 %.
+
+The relative L2 is sqrt(mean((u - u_exact)^2)) / max|u_exact|, as in both cases."""
+import numpy as np
+
+from kcfd import meshgen
+from oracle import mesh as om, simple as osim
+
+MU, DPDX = 0.01, -1.0
+
+
+def exact(y, H):
+    return -DPDX / (2.0 * MU) * y * (H - y)
+
+
+def poiseuille(nodes, cells, bd, H, alpha_u, alpha_p, max_iter, tol):
+    m = om.build_2d(nodes, cells, bd)
+    o = osim.Simple(m, rho=1.0, mu=MU)
+    y_in = m.fcenter[m.boundary_patches["inlet"], 1]
+    o.set_velocity_bc("inlet", "dirichlet", np.c_[exact(y_in, H), np.zeros_like(y_in)])
+    o.set_velocity_bc("outlet", "zero_gradient")
+    for w in ("wall_bottom", "wall_top"):
+        o.set_velocity_bc(w, "dirichlet", [0.0, 0.0])
+        o.set_pressure_bc(w, "zero_gradient")
+    o.set_pressure_bc("inlet", "zero_gradient")
+    o.set_pressure_bc("outlet", "dirichlet", 0.0)
+    o.U[:, 0] = -DPDX * H ** 2 / (8.0 * MU) * 0.5
+    o.U[:, 1] = 0.0
+    o.alpha_u, o.alpha_p, o.max_outer_iter, o.tol = alpha_u, alpha_p, max_iter, tol
+    return m, o, o.solve_steady()
+
+
+def rel_l2(u, y, H):
+    ue = exact(y, H)
+    return np.sqrt(np.mean((u - ue) ** 2)) / max(np.max(np.abs(ue)), 1e-15)
+
+
+def test_case1_poiseuille_quads():
+    H = 0.1
+    nodes, cells, bd = meshgen.quad_box_arrays(0.0, 0.0, 1.0, H, 50, 20, meshgen.CHANNEL_2D_NAMES)
+    m, o, res = poiseuille(nodes, cells, bd, H, 0.7, 0.3, 500, 1e-5)
+    # get_velocity_at_y(0.8): dx from the first internal face with a nonzero x offset
+    it = np.nonzero(m.neighbour >= 0)[0]
+    dxs = np.abs(m.ccenter[m.owner[it], 0] - m.ccenter[m.neighbour[it], 0])
+    dx = dxs[np.nonzero(dxs > 1e-10)[0][0]]
+    sel = np.abs(m.ccenter[:, 0] - 0.8) < 1.5 * dx
+    assert sel.sum() == 40  # the two columns either side of x = 0.8
+    err = rel_l2(o.U[sel, 0], m.ccenter[sel, 1], H)
+    assert err < 0.01, (err, res["iterations"])
+
+
+def test_case7_poiseuille_triangles():
+    Lx, Ly, nx = 0.2, 0.1, 20
+    nodes, cells, bd = meshgen.tri_channel_arrays(Lx, Ly, nx, 10)
+    m, o, res = poiseuille(nodes, cells, bd, Ly, 0.2, 0.05, 3000, 1e-4)
+    sel = np.abs(m.ccenter[:, 0] - 0.8 * Lx) < Lx / nx * 2.0
+    assert sel.sum() > 0
+    err = rel_l2(o.U[sel, 0], m.ccenter[sel, 1], Ly)
+    assert err < 0.10, (err, res["iterations"])
+
+
+def test_channel_matches_reference_run():
+    """The same channel set-up against the reference's own SIMPLESolver run
+    (tests/golden/channel.npz, written by tests/golden/make_golden.py --only channel):
+    outlet p = 0, zero-gradient outlet velocity and a per-face inlet profile, paths the
+    cavity fixtures do not reach."""
+    from conftest import load_golden
+    g = load_golden("channel")
+    for tag, arrays, H, au, ap in (("quad", meshgen.quad_box_arrays(0.0, 0.0, 1.0, 0.1, 20, 8, meshgen.CHANNEL_2D_NAMES),
+                                    0.1, 0.7, 0.3),
+                                   ("tri", meshgen.tri_channel_arrays(0.2, 0.1, 8, 4), 0.1, 0.2, 0.05)):
+        m, o, res = poiseuille(*arrays, H, au, ap, int(g[tag + "_iters"]), 0.0)
+        for mine, ref in ((o.U, g[tag + "_U"]), (o.p, g[tag + "_p"])):
+            assert np.linalg.norm(mine - ref) <= 1e-10 * np.linalg.norm(ref), tag
+        np.testing.assert_allclose(res["residuals"], g[tag + "_res"], rtol=1e-8)

@@ -329,6 +329,40 @@ def make_channel(out):
     np.savez_compressed(os.path.join(out, "channel.npz"), **d)
 
 
+def make_muscl_case(out):
+    """The reference's MUSCL verification (verification/case6_muscl.py:136-205): a step
+    phi = [x < 0.3] advected at u = 1 on generate_channel_mesh(1.0, 0.02, 100, 1) to
+    T = 0.4 at CFL 0.4, once with backward-Euler upwind and once with the van Leer
+    deferred correction (2 inner passes per step), each step clipped to [0, 1], by the
+    case's own step functions. Stores both final fields and the step count."""
+    import contextlib
+    import io
+    import verification.case6_muscl as c6
+    from core.fields import VectorField
+    from core.interpolation import compute_mass_flux
+    from mesh.mesh_generator import generate_channel_mesh
+    mesh = generate_channel_mesh(1.0, 0.02, 100, 1)
+    U = VectorField(mesh, name="U")
+    U.values[:, 0], U.values[:, 1] = 1.0, 0.0
+    for bname, fids in mesh.boundary_patches.items():
+        U.boundary_values[bname] = np.zeros((len(fids), 2))
+        U.boundary_values[bname][:, 0] = 1.0
+    mf = compute_mass_flux(U, 1.0, mesh)
+    xc = np.array([c.center[0] for c in mesh.cells])
+    phi0 = np.where(xc < 0.3, 1.0, 0.0).astype(np.float64)
+    dt = 0.4 * (1.0 / 100) / 1.0
+    n_steps = int(np.ceil(0.4 / dt))
+    dt = 0.4 / n_steps
+    uw, mu = phi0.copy(), phi0.copy()
+    with contextlib.redirect_stdout(io.StringIO()):
+        for _ in range(n_steps):
+            uw = np.clip(c6._solve_upwind_step(mesh, uw, mf, 1.0, dt, 1.0), 0.0, 1.0)
+            mu = np.clip(c6._solve_muscl_step(mesh, mu, mf, 1.0, dt, 1.0, n_inner=2), 0.0, 1.0)
+    np.savez_compressed(os.path.join(out, "muscl_case.npz"), phi_upwind=uw, phi_muscl=mu, n_steps=np.int64(n_steps),
+                        dt=np.float64(dt), width_upwind=np.float64(c6._compute_diffusion_width(xc, uw)),
+                        width_muscl=np.float64(c6._compute_diffusion_width(xc, mu)))
+
+
 def two_fluid_setup(sv, mesh, seed):
     """Shared set-up of the two-fluid fixtures (also restated by the oracle and the
     device tests): inlet / outlet / heated bottom wall / adiabatic walls, seeded
@@ -502,6 +536,8 @@ def main():
         make_simple(a.out)
     if want("channel"):
         make_channel(a.out)
+    if want("muscl_case"):
+        make_muscl_case(a.out)
     if want("two_fluid"):
         make_two_fluid(a.out, meshes)
     if want("partitions"):

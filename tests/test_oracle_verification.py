@@ -85,3 +85,58 @@ def test_channel_matches_reference_run():
         for mine, ref in ((o.U, g[tag + "_U"]), (o.p, g[tag + "_p"])):
             assert np.linalg.norm(mine - ref) <= 1e-10 * np.linalg.norm(ref), tag
         np.testing.assert_allclose(res["residuals"], g[tag + "_res"], rtol=1e-8)
+
+
+def test_case6_muscl_step_advection():
+    """verification/case6_muscl.py:136-223 on the oracle's operators: a step phi = [x < 0.3]
+    advected at u = 1 on a 100 x 1 channel to T = 0.4 (CFL 0.4), backward Euler with upwind,
+    and with the van Leer deferred correction (2 inner passes per step), each step clipped
+    to [0, 1]. Both final fields equal the reference's own run (tests/golden/muscl_case.npz),
+    and MUSCL's 10-90 % front is no wider than upwind's, the case's pass criterion."""
+    import scipy.sparse.linalg as spla
+    from conftest import load_golden
+    from oracle import fvm as of
+    g = load_golden("muscl_case")
+    nodes, cells, bd = meshgen.quad_box_arrays(0.0, 0.0, 1.0, 0.02, 100, 1, meshgen.CHANNEL_2D_NAMES)
+    m = om.build_2d(nodes, cells, bd)
+    n = m.n_cells
+    U = np.c_[np.ones(n), np.zeros(n)]
+    Ub = np.zeros((m.n_faces, 2))
+    Ub[:, 0] = 1.0
+    mf = of.compute_mass_flux(m, U, Ub, 1.0)
+    phi0 = np.where(m.ccenter[:, 0] < 0.3, 1.0, 0.0)
+    dt, n_steps = float(g["dt"]), int(g["n_steps"])
+    inlet = m.boundary_patches["inlet"]
+    phi_b = {nm: (1.0 if nm == "inlet" else 0.0) for nm in m.boundary_patches}
+
+    def system_for(phi_old):
+        s = of.System(n)
+        of.temporal_operator(m, 1.0, dt, phi_old, s)
+        of.convection_operator_upwind(m, mf, s)
+        F = mf[inlet]
+        neg = F < 0  # inflow through the inlet: the case adds -F phi_b to the rhs
+        s.add_source(m.owner[inlet][neg], -F[neg] * 1.0)
+        return s
+
+    def solve(s):
+        return np.clip(spla.spsolve(s.to_sparse(), s.rhs), 0.0, 1.0)
+
+    uw, mu = phi0.copy(), phi0.copy()
+    for _ in range(n_steps):
+        uw = solve(system_for(uw))
+        cur = mu.copy()
+        for _ in range(2):
+            grad = of.green_gauss_gradient(m, cur, of.face_patch_values(m, phi_b, cur))
+            s = system_for(mu)
+            s.rhs += of.muscl_deferred_correction(m, cur, mf, grad, "van_leer")
+            cur = solve(s)
+        mu = cur
+    np.testing.assert_allclose(uw, g["phi_upwind"], rtol=0, atol=1e-12)
+    np.testing.assert_allclose(mu, g["phi_muscl"], rtol=0, atol=1e-12)
+
+    def width(phi):
+        x = m.ccenter[(phi >= 0.1) & (phi <= 0.9), 0]
+        return float(x[-1] - x[0]) if len(x) > 1 else 0.0
+
+    assert width(mu) <= width(uw)
+    assert abs(width(uw) - float(g["width_upwind"])) < 1e-12 and abs(width(mu) - float(g["width_muscl"])) < 1e-12

@@ -326,6 +326,35 @@ def make_channel(out):
         d[tag + "_p"] = sv.p.values.copy()
         d[tag + "_res"] = np.array(r["residuals"])
         d[tag + "_iters"] = np.int64(iters)
+    # the 3D duct of verification/case5_3d_duct.py:75-112 at 8 x 4 x 4, inlet from the
+    # case's own series profile
+    from mesh.mesh_generator_3d import generate_3d_duct_mesh
+    from verification.case5_3d_duct import analytical_3d_duct
+    m = generate_3d_duct_mesh(2.0, 0.1, 0.1, 8, 4, 4)
+    sv = SIMPLESolver(m, rho=1.0, mu=CHANNEL_MU)
+    fids = m.boundary_patches["inlet"]
+    yz = np.array([m.faces[f].center for f in fids])
+    u = np.zeros((len(fids), 3))
+    u[:, 0] = analytical_3d_duct(yz[:, 1], yz[:, 2], 0.1, 0.1, CHANNEL_DPDX, CHANNEL_MU)
+    sv.U.boundary_values["inlet"] = u
+    sv.set_velocity_bc("inlet", "dirichlet")
+    sv.set_velocity_bc("outlet", "zero_gradient")
+    for w in ("wall_bottom", "wall_top", "wall_front", "wall_back"):
+        sv.set_velocity_bc(w, "dirichlet", [0.0, 0.0, 0.0])
+        sv.set_pressure_bc(w, "zero_gradient")
+    sv.set_pressure_bc("inlet", "zero_gradient")
+    sv.set_pressure_bc("outlet", "dirichlet", 0.0)
+    sv.U.values[:, 0] = -CHANNEL_DPDX * 0.1 ** 2 / (8.0 * CHANNEL_MU) * 0.3
+    sv.U.values[:, 1] = 0.0
+    sv.U.values[:, 2] = 0.0
+    sv.alpha_u, sv.alpha_p, sv.max_outer_iter, sv.tol = 0.7, 0.3, 10, 0.0
+    with contextlib.redirect_stdout(io.StringIO()):
+        r = sv.solve_steady()
+    d["duct_inlet_u"] = u[:, 0].copy()
+    d["duct_U"] = sv.U.values.copy()
+    d["duct_p"] = sv.p.values.copy()
+    d["duct_res"] = np.array(r["residuals"])
+    d["duct_iters"] = np.int64(10)
     np.savez_compressed(os.path.join(out, "channel.npz"), **d)
 
 

@@ -12,7 +12,11 @@ outlet p = 0, no-slip walls, started from u = u_max / 2:
   triangles), Lx = 0.2, Ly = 0.1, alpha_u 0.2, alpha_p 0.05, at most 3000 iterations
   to 1e-4. The profile is every cell within 2 dx of x = 0.8 Lx. Passes below 10 %.
 
-The relative L2 is sqrt(mean((u - u_exact)^2)) / max|u_exact|, as in both cases."""
+- case 5 (verification/case5_3d_duct.py:21-63,75-131): a 2 x 0.1 x 0.1 duct of 20 x 8 x 8
+  hexes with the case's series profile at the inlet, alpha_u 0.7, alpha_p 0.3, at most
+  500 iterations to 1e-4, cells within 1.5 dx of x = 0.8 Lx. Passes below 5 %.
+
+The relative L2 is sqrt(mean((u - u_exact)^2)) / max|u_exact|, as in every case."""
 import numpy as np
 
 from kcfd import meshgen
@@ -40,6 +44,41 @@ def poiseuille(nodes, cells, bd, H, alpha_u, alpha_p, max_iter, tol):
     o.U[:, 1] = 0.0
     o.alpha_u, o.alpha_p, o.max_outer_iter, o.tol = alpha_u, alpha_p, max_iter, tol
     return m, o, o.solve_steady()
+
+
+def duct_exact(y, z, H, W, terms=20):
+    """The series profile of verification/case5_3d_duct.py:21-63 on [0, H] x [0, W]: the
+    rectangular-duct Poiseuille series in the centred coordinates, scaled as that case
+    scales it (4 G a^2 / (mu pi^3), a = H / 2) and floored at 0."""
+    a, b = H / 2.0, W / 2.0
+    yc, zc = y - a, z - b
+    s = np.zeros_like(y)
+    for k in range(terms):
+        m = 2 * k + 1
+        lam = m * np.pi / (2 * a)
+        den = np.cosh(lam * b)
+        ratio = np.where(den > 1e200, 0.0, np.cosh(lam * zc) / np.maximum(den, 1e-30))
+        s += (-1) ** k / m ** 3 * (1.0 - ratio) * np.cos(m * np.pi * yc / (2 * a))
+    return np.maximum(s * 4.0 * (-DPDX) * a ** 2 / (MU * np.pi ** 3), 0.0)
+
+
+def duct(nx, ny, nz, max_iter, tol, Lx=2.0, H=0.1, W=0.1):
+    nodes, cells, cf, bd = meshgen.hex_box_arrays(Lx, H, W, nx, ny, nz, meshgen.CHANNEL_3D_NAMES)
+    m = om.build_3d(nodes, cells, cf, bd)
+    o = osim.Simple(m, rho=1.0, mu=MU)
+    fi = m.boundary_patches["inlet"]
+    u_in = duct_exact(m.fcenter[fi, 1], m.fcenter[fi, 2], H, W)
+    z = np.zeros_like(u_in)
+    o.set_velocity_bc("inlet", "dirichlet", np.c_[u_in, z, z])
+    o.set_velocity_bc("outlet", "zero_gradient")
+    for w in ("wall_bottom", "wall_top", "wall_front", "wall_back"):
+        o.set_velocity_bc(w, "dirichlet", [0.0, 0.0, 0.0])
+        o.set_pressure_bc(w, "zero_gradient")
+    o.set_pressure_bc("inlet", "zero_gradient")
+    o.set_pressure_bc("outlet", "dirichlet", 0.0)
+    o.U[:, 0] = -DPDX * H ** 2 / (8.0 * MU) * 0.3
+    o.alpha_u, o.alpha_p, o.max_outer_iter, o.tol = 0.7, 0.3, max_iter, tol
+    return m, o, u_in, o.solve_steady()
 
 
 def rel_l2(u, y, H):
@@ -140,3 +179,25 @@ def test_case6_muscl_step_advection():
 
     assert width(mu) <= width(uw)
     assert abs(width(uw) - float(g["width_upwind"])) < 1e-12 and abs(width(mu) - float(g["width_muscl"])) < 1e-12
+
+
+def test_case5_duct():
+    Lx, H, W = 2.0, 0.1, 0.1
+    m, o, _, res = duct(20, 8, 8, 500, 1e-4)
+    sel = np.abs(m.ccenter[:, 0] - 0.8 * Lx) < Lx / 20 * 1.5
+    ue = duct_exact(m.ccenter[sel, 1], m.ccenter[sel, 2], H, W)
+    err = np.sqrt(np.mean((o.U[sel, 0] - ue) ** 2)) / max(np.max(np.abs(ue)), 1e-15)
+    assert err < 0.05, (err, res["iterations"])
+
+
+def test_duct_matches_reference_run():
+    """8 x 4 x 4 duct, 10 outer iterations, against the reference's own run
+    (tests/golden/channel.npz): the inlet series equals the case's function and the
+    fields agree to 1e-10 (3D outlet p = 0 and zero-gradient velocity)."""
+    from conftest import load_golden
+    g = load_golden("channel")
+    m, o, u_in, res = duct(8, 4, 4, int(g["duct_iters"]), 0.0)
+    np.testing.assert_allclose(u_in, g["duct_inlet_u"], rtol=1e-13, atol=1e-16)
+    for mine, ref in ((o.U, g["duct_U"]), (o.p, g["duct_p"])):
+        assert np.linalg.norm(mine - ref) <= 1e-10 * np.linalg.norm(ref)
+    np.testing.assert_allclose(res["residuals"], g["duct_res"], rtol=1e-8)

@@ -12,6 +12,9 @@ outlet p = 0, no-slip walls, started from u = u_max / 2:
   triangles), Lx = 0.2, Ly = 0.1, alpha_u 0.2, alpha_p 0.05, at most 3000 iterations
   to 1e-4. The profile is every cell within 2 dx of x = 0.8 Lx. Passes below 10 %.
 
+- case 22 (verification/case22_hybrid_mesh.py:64-131): the same duct on 16 x 4 x 4
+  columns, hexes on the low-x half and 12 tets per column cell on the high-x half,
+  at most 300 iterations to 1e-3. Passes below 10 %.
 - case 5 (verification/case5_3d_duct.py:21-63,75-131): a 2 x 0.1 x 0.1 duct of 20 x 8 x 8
   hexes with the case's series profile at the inlet, alpha_u 0.7, alpha_p 0.3, at most
   500 iterations to 1e-4, cells within 1.5 dx of x = 0.8 Lx. Passes below 5 %.
@@ -62,8 +65,8 @@ def duct_exact(y, z, H, W, terms=20):
     return np.maximum(s * 4.0 * (-DPDX) * a ** 2 / (MU * np.pi ** 3), 0.0)
 
 
-def duct(nx, ny, nz, max_iter, tol, Lx=2.0, H=0.1, W=0.1):
-    nodes, cells, cf, bd = meshgen.hex_box_arrays(Lx, H, W, nx, ny, nz, meshgen.CHANNEL_3D_NAMES)
+def duct(nx, ny, nz, max_iter, tol, Lx=2.0, H=0.1, W=0.1, arrays=None):
+    nodes, cells, cf, bd = arrays or meshgen.hex_box_arrays(Lx, H, W, nx, ny, nz, meshgen.CHANNEL_3D_NAMES)
     m = om.build_3d(nodes, cells, cf, bd)
     o = osim.Simple(m, rho=1.0, mu=MU)
     fi = m.boundary_patches["inlet"]
@@ -201,3 +204,13 @@ def test_duct_matches_reference_run():
     for mine, ref in ((o.U, g["duct_U"]), (o.p, g["duct_p"])):
         assert np.linalg.norm(mine - ref) <= 1e-10 * np.linalg.norm(ref)
     np.testing.assert_allclose(res["residuals"], g["duct_res"], rtol=1e-8)
+
+
+def test_case22_hybrid_duct():
+    Lx, H, W = 2.0, 0.1, 0.1
+    arrays = meshgen.hybrid_hex_tet_arrays(Lx, H, W, 16, 4, 4, tet_fraction=0.5)
+    m, o, _, res = duct(16, 4, 4, 300, 1e-3, arrays=arrays)
+    sel = np.abs(m.ccenter[:, 0] - 0.8 * Lx) < Lx / 16 * 1.5
+    ue = duct_exact(m.ccenter[sel, 1], m.ccenter[sel, 2], H, W)
+    err = np.sqrt(np.mean((o.U[sel, 0] - ue) ** 2)) / np.max(np.abs(ue))
+    assert err < 0.10, (err, res["iterations"])

@@ -15,6 +15,10 @@ outlet p = 0, no-slip walls, started from u = u_max / 2:
 - case 22 (verification/case22_hybrid_mesh.py:64-131): the same duct on 16 x 4 x 4
   columns, hexes on the low-x half and 12 tets per column cell on the high-x half,
   at most 300 iterations to 1e-3. Passes below 10 %.
+- case 14 (verification/case14_3d_cavity.py:38-110,180-186): the 12^3 lid-driven
+  cavity at Re 100, alpha_u 0.5, alpha_p 0.2, at most 500 iterations to 1e-3. The
+  vertical centreline (cells within 1.5 dx of x = z = 0.5) must recirculate: mean u
+  above y = 0.7 positive, between y = 0.3 and 0.6 negative.
 - case 5 (verification/case5_3d_duct.py:21-63,75-131): a 2 x 0.1 x 0.1 duct of 20 x 8 x 8
   hexes with the case's series profile at the inlet, alpha_u 0.7, alpha_p 0.3, at most
   500 iterations to 1e-4, cells within 1.5 dx of x = 0.8 Lx. Passes below 5 %.
@@ -214,3 +218,16 @@ def test_case22_hybrid_duct():
     ue = duct_exact(m.ccenter[sel, 1], m.ccenter[sel, 2], H, W)
     err = np.sqrt(np.mean((o.U[sel, 0] - ue) ** 2)) / np.max(np.abs(ue))
     assert err < 0.10, (err, res["iterations"])
+
+
+def test_case14_cavity_recirculates():
+    nodes, cells, cf, bd = meshgen.hex_box_arrays(1.0, 1.0, 1.0, 12, 12, 12, meshgen.CAVITY_3D_NAMES)
+    m = om.build_3d(nodes, cells, cf, bd)
+    o = osim.Simple(m, rho=1.0, mu=0.01)
+    osim.cavity_setup(o)
+    o.alpha_u, o.alpha_p, o.max_outer_iter, o.tol = 0.5, 0.2, 500, 1e-3
+    o.solve_steady()
+    c = m.ccenter
+    sel = (np.abs(c[:, 0] - 0.5) < 1.5 / 12) & (np.abs(c[:, 2] - 0.5) < 1.5 / 12)
+    y, u = c[sel, 1], o.U[sel, 0]
+    assert np.mean(u[y > 0.7]) > 0 and np.mean(u[(y > 0.3) & (y < 0.6)]) < 0

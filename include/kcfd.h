@@ -85,6 +85,9 @@ void kcfd_graph_destroy(kcfd_graph* g);
  *     nodes starting at cface_off[q] in cface_nodes.
  * Boundary faces: n_bfaces node lists (bface_len, flattened bface_nodes), each with
  *     the index of its patch in the caller's patch-dict order (bface_patch).      */
+/* The build runs its independent passes on up to 16 host threads (KCFD_HOST_THREADS in
+ * the environment, read once per process, caps the count); the result does not depend
+ * on the thread count. */
 typedef struct kcfd_host_mesh kcfd_host_mesh;
 
 int kcfd_mesh_build(int32_t ndim, int64_t n_nodes, const double* nodes,

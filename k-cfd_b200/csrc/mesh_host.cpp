@@ -18,6 +18,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdint>
+#include <cstdlib>
 #include <cstring>
 #include <memory>
 #include <mutex>
@@ -154,10 +155,16 @@ using kcfd::dvec;
 
 namespace {
 
-// Host threads for the builder's independent passes (per cell, item, face or row).
+// Host threads for the builder's independent passes (per cell, item, face or row):
+// KCFD_HOST_THREADS when set (a positive count), else the hardware's, at most 16.
+// Read once per process.
 int host_threads() {
     static const int t = [] {
         unsigned h = std::thread::hardware_concurrency();
+        if (const char* e = std::getenv("KCFD_HOST_THREADS")) {
+            const long v = std::strtol(e, nullptr, 10);
+            if (v > 0) h = (unsigned)std::min(v, 1024L);
+        }
         return (int)std::min(16u, std::max(1u, h));
     }();
     return t;

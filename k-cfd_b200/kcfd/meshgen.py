@@ -227,6 +227,11 @@ def generate_bubble_column_mesh(width=0.15, height=0.45, nx=30, ny=90):
     """mesh/mesh_generator.py:232-263: the bottom split into inlet_gas (faces whose
     centre x lies in [width/3, 2 width/3]) and wall_bottom, after outlet (top),
     wall_left and wall_right."""
+    return _build(*bubble_column_arrays(width, height, nx, ny))
+
+
+def bubble_column_arrays(width=0.15, height=0.45, nx=30, ny=90):
+    """Nodes, cells and boundary dict of generate_bubble_column_mesh."""
     nodes, cells, bd = quad_box_arrays(0.0, 0.0, width, height, nx, ny,
                                        {"bottom": "_bottom", "top": "outlet", "left": "wall_left",
                                         "right": "wall_right"})
@@ -235,7 +240,7 @@ def generate_bubble_column_mesh(width=0.15, height=0.45, nx=30, ny=90):
     inlet = (width / 3.0 <= xc) & (xc <= 2.0 * width / 3.0)
     bd["inlet_gas"] = list(bottom[inlet])
     bd["wall_bottom"] = list(bottom[~inlet])
-    return _build(nodes, cells, bd)
+    return nodes, cells, bd
 
 
 def generate_triangle_channel_mesh(Lx=1.0, Ly=0.1, nx=20, ny=5):

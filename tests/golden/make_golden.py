@@ -392,6 +392,45 @@ def make_muscl_case(out):
                         width_muscl=np.float64(c6._compute_diffusion_width(xc, mu)))
 
 
+def bubble_setup(sv):
+    """verification/case4_bubble_column.py:40-69: water-air properties, d_b 5 mm, gravity
+    -9.81 along y, alpha_g 0.001 at rest, 300 K, inlet alpha_g 0.04 at U_g = 0.1 m/s up,
+    outlet p = 0, walls; relaxation 0.3 / 0.2 / 0.3."""
+    sv.rho_l, sv.rho_g, sv.mu_l, sv.mu_g, sv.d_b = 998.2, 1.225, 1.003e-3, 1.789e-5, 0.005
+    sv.g = np.array([0.0, -9.81])
+    sv.initialize(alpha_g_init=0.001)
+    sv.set_inlet_bc("inlet_gas", 0.04, U_l=[0.0, 0.0], U_g=[0.0, 0.1])
+    sv.set_outlet_bc("outlet", p_val=0.0)
+    for w in ("wall_bottom", "wall_left", "wall_right"):
+        sv.set_wall_bc(w)
+    sv.alpha_u, sv.alpha_p, sv.alpha_alpha = 0.3, 0.2, 0.3
+
+
+def make_bubble(out):
+    """The bubble column of verification/case4_bubble_column.py on its 8 x 20 mesh: the
+    first 5 steps of dt = 0.02 of its solve_transient run, one solve_transient(dt, dt)
+    call per step, fields after every step."""
+    import contextlib
+    import io
+    from mesh.mesh_generator import generate_bubble_column_mesh
+    from models.two_fluid import TwoFluidSolver
+    mesh = generate_bubble_column_mesh(0.15, 0.45, 8, 20)
+    sv = TwoFluidSolver(mesh)
+    bubble_setup(sv)
+    sv.T_l.set_uniform(300.0)
+    sv.T_g.set_uniform(300.0)
+    sv.dt = 0.02
+    d = {}
+    for step in range(5):
+        with contextlib.redirect_stdout(io.StringIO()):
+            r = sv.solve_transient(sv.dt, sv.dt)
+        assert r["time_steps"] == 1
+        for f in ("alpha_g", "U_l", "U_g", "p"):
+            d[f"{step}_{f}"] = getattr(sv, f).values.copy()
+        d[f"{step}_res"] = np.array(r["residuals"])
+    np.savez_compressed(os.path.join(out, "bubble.npz"), **d)
+
+
 def two_fluid_setup(sv, mesh, seed):
     """Shared set-up of the two-fluid fixtures (also restated by the oracle and the
     device tests): inlet / outlet / heated bottom wall / adiabatic walls, seeded
@@ -567,6 +606,8 @@ def main():
         make_channel(a.out)
     if want("muscl_case"):
         make_muscl_case(a.out)
+    if want("bubble"):
+        make_bubble(a.out)
     if want("two_fluid"):
         make_two_fluid(a.out, meshes)
     if want("partitions"):

@@ -231,3 +231,34 @@ def test_case14_cavity_recirculates():
     sel = (np.abs(c[:, 0] - 0.5) < 1.5 / 12) & (np.abs(c[:, 2] - 0.5) < 1.5 / 12)
     y, u = c[sel, 1], o.U[sel, 0]
     assert np.mean(u[y > 0.7]) > 0 and np.mean(u[(y > 0.3) & (y < 0.6)]) < 0
+
+
+def test_case4_bubble_column_matches_reference_run():
+    """verification/case4_bubble_column.py:40-114 on the oracle's two-fluid model: the
+    8 x 20 bubble column (inlet alpha_g 0.04 at 0.1 m/s through the middle third of the
+    bottom, outlet p = 0, walls), its first 5 steps of dt = 0.02 against the reference's
+    own run (tests/golden/bubble.npz, one solve_transient(dt, dt) per step) to 1e-10, and
+    the case's physical-validity check on the result (alpha_g <= 1, mean alpha_g < 0.5)."""
+    from conftest import load_golden
+    from oracle.two_fluid import TwoFluid
+    g = load_golden("bubble")
+    nodes, cells, bd = meshgen.bubble_column_arrays(0.15, 0.45, 8, 20)
+    o = TwoFluid(om.build_2d(nodes, cells, bd))
+    o.rho_l, o.rho_g, o.mu_l, o.mu_g, o.d_b = 998.2, 1.225, 1.003e-3, 1.789e-5, 0.005
+    o.g = np.array([0.0, -9.81])
+    o.initialize(alpha_g_init=0.001)
+    o.set_inlet_bc("inlet_gas", 0.04, U_l=[0.0, 0.0], U_g=[0.0, 0.1])
+    o.set_outlet_bc("outlet", p_val=0.0)
+    for w in ("wall_bottom", "wall_left", "wall_right"):
+        o.set_wall_bc(w)
+    o.alpha_u, o.alpha_p, o.alpha_alpha = 0.3, 0.2, 0.3
+    o._set_uniform("T_l", 300.0)
+    o._set_uniform("T_g", 300.0)
+    for step in range(5):
+        res = o.step(0.02)
+        assert abs(res - g[f"{step}_res"][0]) <= 1e-6 * abs(g[f"{step}_res"][0])
+        for f in ("alpha_g", "U_l", "U_g", "p"):
+            ref = g[f"{step}_{f}"]
+            assert np.linalg.norm(o.v[f] - ref) <= 1e-10 * max(np.linalg.norm(ref), 1e-300), (step, f)
+    a = o.v["alpha_g"]
+    assert a.max() <= 1.0 and a.mean() < 0.5

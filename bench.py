@@ -125,7 +125,7 @@ def measured_peak():
 
 # DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the nine phase kernels
 # of one p' Krylov iteration on the 128^3 cavity, from one ncu capture of the graph
-# engine (profiles/graph_engine_p_solve_cavity128.md); the roofline's traffic is this
+# engine (KCFD_ENGINE_EAGER=1, one Krylov iteration captured); the roofline's traffic is this
 # times the solve's Krylov count (the kernels and their sizes repeat every iteration).
 NCU_P_ITER_DRAM_BYTES_128 = 857019136
 

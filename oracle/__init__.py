@@ -20,7 +20,9 @@ K-CFD reference (senily0/K-CFD) that the CUDA path in ``k-cfd_b200`` replaces:
                      no reference counterpart and their parity is unpinned.
 
 Parity pins: tests/golden/make_golden.py imports the reference itself and writes
-golden fixtures; tests/test_oracle_golden.py checks this package against them.
+golden fixtures; tests/test_oracle_mesh.py, test_oracle_ops.py, test_oracle_simple.py,
+test_oracle_two_fluid.py, test_oracle_iluk.py and test_oracle_verification.py check
+this package against them.
 
 Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may import
 this package, and only as the checker or the timed CPU baseline. The product

@@ -2,14 +2,15 @@
 
 Run in a container that holds the reference checkout (it is read, never modified):
 
-    python tests/golden/make_golden.py [--ref /root/reference]
+    python tests/golden/make_golden.py --ref <reference checkout>   (or KCFD_REFERENCE=<checkout>)
 
 The reference is pure Python. Its mesh package imports ``gmsh`` at module level
 without using it (mesh/mesh_generator.py:8), and its verification cases import
 matplotlib for plotting only, so both are replaced by empty stub modules before
 the import. Every fixture is small (kilobytes) and is written with
-numpy.savez_compressed; tests/test_oracle_golden.py checks the oracle against
-them and the GPU tests reuse the generator inputs recorded here.
+numpy.savez_compressed; the tests/test_oracle_*.py files check the oracle against
+them and the GPU tests compare the device path with them and reuse the generator
+inputs recorded here.
 """
 from __future__ import annotations
 
@@ -277,6 +278,28 @@ def make_simple(out):
         d[tag + "_res"] = np.array(r["residuals"])
         d[tag + "_iters"] = np.int64(iters)
     np.savez_compressed(os.path.join(out, "simple.npz"), **d)
+
+
+def make_c1(out):
+    """The reference's own CPU-runnable configuration, exactly: SIMPLESolver on
+    generate_cavity_mesh(1.0, 64) (4,096 quads), rho 1, mu 0.01, lid u = 1, no-slip
+    walls, zero-gradient pressure, upwind, alpha_u 0.7, alpha_p 0.3, 500 outer
+    iterations (tol 0), every system solved by the reference's spsolve
+    (models/single_phase.py:265,351). About 3 minutes on one host core."""
+    from mesh.mesh_generator import generate_cavity_mesh
+    from models.single_phase import SIMPLESolver
+    import contextlib
+    import io
+    m = generate_cavity_mesh(1.0, 64)
+    sv = SIMPLESolver(m, rho=1.0, mu=0.01)
+    for pname in m.boundary_patches:
+        sv.set_velocity_bc(pname, "dirichlet", [1.0, 0.0] if pname == "lid" else [0.0, 0.0])
+        sv.set_pressure_bc(pname, "zero_gradient")
+    sv.alpha_u, sv.alpha_p, sv.max_outer_iter, sv.tol = 0.7, 0.3, 500, 0.0
+    with contextlib.redirect_stdout(io.StringIO()):
+        r = sv.solve_steady()
+    np.savez_compressed(os.path.join(out, "c1_cavity64.npz"), U=sv.U.values.copy(), p=sv.p.values.copy(),
+                        res=np.array(r["residuals"]), iters=np.int64(500))
 
 
 CHANNEL_MU, CHANNEL_DPDX = 0.01, -1.0
@@ -583,10 +606,13 @@ def make_time_control(out, meshes):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=os.environ.get("KCFD_REFERENCE"),
+                    help="path of the K-CFD reference checkout (default: $KCFD_REFERENCE)")
     ap.add_argument("--out", default=HERE)
     ap.add_argument("--only", default="", help="comma list of fixture groups to write (default: all)")
     a = ap.parse_args()
+    if not a.ref:
+        ap.error("--ref (or KCFD_REFERENCE) must name the reference checkout")
     _install_stubs()
     sys.path.insert(0, a.ref)
     only = set(x for x in a.only.split(",") if x)
@@ -604,6 +630,8 @@ def main():
         make_simple(a.out)
     if want("channel"):
         make_channel(a.out)
+    if want("c1"):
+        make_c1(a.out)
     if want("muscl_case"):
         make_muscl_case(a.out)
     if want("bubble"):

@@ -75,3 +75,22 @@ def test_structural_ilu0_is_exact_on_pattern():
     mask = A.copy(); mask.data[:] = 1.0
     diff = (LU - A).multiply(mask)
     assert abs(diff).max() < 1e-12 * abs(A).max()
+
+
+def test_c1_500_iterations_match_reference():
+    """The benchmark's C1 configuration exactly (64^2 cavity, Re 100, upwind, alpha
+    0.7 / 0.3, 500 outer iterations): the oracle with BiCGSTAB + Jacobi at 1e-12 against
+    the reference's own spsolve run (tests/golden/c1_cavity64.npz), u, v and p each
+    within 1e-10 relative L2, and the residual history."""
+    from kcfd import meshgen
+    g = load_golden("c1_cavity64")
+    nodes, cells, bd = meshgen.quad_box_arrays(0, 0, 1, 1, 64, 64, meshgen.CAVITY_2D_NAMES)
+    s = simple.Simple(om.build_2d(nodes, cells, bd), rho=1.0, mu=0.01)
+    simple.cavity_setup(s)
+    s.solver, s.rtol, s.precond_u, s.precond_p = "bicgstab", 1e-12, "jacobi", "jacobi"
+    s.alpha_u, s.alpha_p, s.max_outer_iter, s.tol = 0.7, 0.3, int(g["iters"]), 0.0
+    r = s.solve_steady()
+    for k in range(2):
+        assert np.linalg.norm(s.U[:, k] - g["U"][:, k]) <= 1e-10 * np.linalg.norm(g["U"][:, k])
+    assert np.linalg.norm(s.p - g["p"]) <= 1e-10 * np.linalg.norm(g["p"])
+    np.testing.assert_allclose(r["residuals"], g["res"], rtol=1e-6)

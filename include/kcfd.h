@@ -31,6 +31,7 @@ extern "C" {
 #define KCFD_PREC_NONE   0
 #define KCFD_PREC_JACOBI 1
 #define KCFD_PREC_ILU0   2
+#define KCFD_PREC_AMG    3  /* smoothed-aggregation multigrid, one V(1,1) cycle per apply */
 
 /* stopping rules */
 #define KCFD_STOP_SCIPY  0  /* scipy bicgstab: ||r|| < max(atol, rtol ||b||), eps^2 breakdown
@@ -187,6 +188,7 @@ int kcfd_spmv_f32(const kcfd_csr_t* A, const float* x, float* y, int32_t nrhs, v
  * solve_linear_system (core/linear_solver.py:50-62) with create_preconditioner
  * (core/preconditioner.py:18-76, methods 'none' / 'jacobi' / 'ilu0').            */
 typedef struct kcfd_solver kcfd_solver;
+typedef struct kcfd_amg kcfd_amg;
 
 typedef struct {
     int32_t precond;     /* KCFD_PREC_*                                        */
@@ -217,7 +219,16 @@ typedef struct {
                             level-of-fill factorisation (core/preconditioner.py:
                             56-61 offers 'iluk' through SuperLU's threshold ILU;
                             this is the structural form)                        */
+    int32_t amg_max_levels; /* KCFD_PREC_AMG: kcfd_amg_opts_t.max_levels (0: 12)    */
+    int32_t amg_coarse_max; /* KCFD_PREC_AMG: kcfd_amg_opts_t.coarse_max (0: 128)   */
 } kcfd_solver_opts_t;
+/* KCFD_PREC_AMG: one right-hand side, graph engine only (team 0 or 3). The handle
+ * builds a kcfd_amg hierarchy on the pattern at creation and refreshes it in
+ * kcfd_solver_setup; each preconditioner apply inside the engine's loop is one V-cycle
+ * (its kernels are nodes of the engine's loop body). mode KCFD_MODE_MIXED keeps the
+ * Krylov iteration FP64 and stores the multigrid hierarchy and cycle vectors in FP32
+ * (FP64 arithmetic). Inside a stream capture an AMG handle does not solve (the
+ * engine's graph is not nested): the call returns KCFD_BAD_INPUT.                 */
 
 /* ILU(0) ordering: level_of_row_host gives each row's level (e.g. the mesh's cell
  * colouring, or natural-order dependency levels); NULL -> natural-order levels.
@@ -243,6 +254,53 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream);
 int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, double* x,
                       int32_t* iters, double* relres, int32_t* status, void* stream);
 
+/* z = M^-1 r with the handle's set-up preconditioner (one right-hand side, FP64
+ * handles): Jacobi, ILU(0) / ILU(k) (both sweeps on the level-permuted factors), one
+ * AMG V-cycle, or a copy for KCFD_PREC_NONE. Device vectors, no host sync. This is
+ * M.matvec of the LinearOperator that create_preconditioner returns
+ * (core/preconditioner.py:18-76).                                                   */
+int kcfd_solver_apply_precond(kcfd_solver* s, const kcfd_csr_t* A, const double* r, double* z, void* stream);
+/* The multigrid hierarchy of a KCFD_PREC_AMG handle (owned by the handle; NULL for
+ * other preconditioners), for kcfd_amg_info / kcfd_amg_export.                    */
+int kcfd_solver_amg(const kcfd_solver* s, kcfd_amg** out);
+
+
+/* ------------------------------------------------ algebraic multigrid ------ */
+/* Smoothed-aggregation AMG (Vanek, Mandel and Brezina 1996), the device counterpart of
+ * create_preconditioner(A, 'amg') (core/preconditioner.py:63-74: pyamg's
+ * smoothed_aggregation_solver(A).aspreconditioner()). Aggregates from three greedy
+ * passes over A's graph; P = (I - omega D^-1 A) T; A_c = P^T A P; omega = 4 / (3 rho)
+ * with rho a Gershgorin bound on level 0 and a power-iteration estimate below; a
+ * V(1,1) cycle with damped Jacobi; the coarsest level (<= 256 rows) by its dense
+ * inverse. kcfd_amg_create builds every pattern and product map on the host from A's
+ * pattern (device pointers; every row needs its diagonal entry); kcfd_amg_setup
+ * refreshes all values from A's current values on the device (no host sync);
+ * kcfd_amg_apply computes x = M^-1 b (one cycle) on the device.                   */
+typedef struct {
+    int32_t mode;         /* KCFD_MODE_FP64, or KCFD_MODE_MIXED: hierarchy values and cycle
+                             vectors stored in FP32, arithmetic in FP64            */
+    int32_t coarse_max;   /* stop coarsening at or below this many rows (0: 128, <= 256) */
+    int32_t max_levels;   /* 0: 12 (at most 16)                                     */
+    int32_t power_iters;  /* power iterations for rho(D^-1 A) below level 0 (0: 4)   */
+} kcfd_amg_opts_t;
+int  kcfd_amg_create(const kcfd_csr_t* A, const kcfd_amg_opts_t* opts, kcfd_amg** out);
+int  kcfd_amg_setup(kcfd_amg* h, const kcfd_csr_t* A, void* stream);
+int  kcfd_amg_apply(kcfd_amg* h, const double* b, double* x, void* stream);
+/* nlevels; rows_nnz[2 l], rows_nnz[2 l + 1] = rows and entries of level l (room for 16
+ * levels); device_bytes = memory the handle holds.                                */
+int  kcfd_amg_info(const kcfd_amg* h, int32_t* nlevels, int64_t* rows_nnz, int64_t* device_bytes);
+/* Copies one item of a level to host memory (synchronises the device), for tests:  */
+#define KCFD_AMG_AGGREGATES     0  /* int32[n_l] aggregate of each row (not the coarsest) */
+#define KCFD_AMG_INDPTR         1  /* int32[n_l + 1] A_l row pointers                     */
+#define KCFD_AMG_INDICES        2  /* int32[nnz_l] A_l columns                            */
+#define KCFD_AMG_VALUES         3  /* double[nnz_l] A_l values (levels >= 1)              */
+#define KCFD_AMG_P_INDPTR       4  /* int32[n_l + 1] prolongator row pointers             */
+#define KCFD_AMG_P_INDICES      5  /* int32[nnz(P_l)] prolongator columns                 */
+#define KCFD_AMG_P_VALUES       6  /* double[nnz(P_l)] prolongator values                 */
+#define KCFD_AMG_OMEGA          7  /* double[1] the level's omega                         */
+#define KCFD_AMG_COARSE_INVERSE 8  /* double[n_l * n_l] dense inverse (coarsest level)    */
+int  kcfd_amg_export(const kcfd_amg* h, int32_t level, int32_t what, void* out_host);
+void kcfd_amg_destroy(kcfd_amg* h);
 
 /* ------------------------------------------------------ batched systems ---- */
 /* Many independent systems (e.g. the pressure-correction systems of many meshes) of

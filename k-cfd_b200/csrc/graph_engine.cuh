@@ -69,6 +69,7 @@ struct Args {
     int* out_status;
     cudaGraphConditionalHandle cond;
     int eager;          // 1: launched from a host loop (no graph, no condition to set)
+    const void* amg;    // KCFD_PREC_AMG: the multigrid handle (host-side, for the cycle's launches)
 };
 
 // Programmatic dependent launch: the phase kernels of one iteration are launched so
@@ -708,15 +709,16 @@ __global__ void __launch_bounds__(kBlock) g_xr(Args a) {
     }
 }
 
-// Results; x = 0 for right-hand sides with b == 0 (scipy returns b).
+// Results; x = 0 for right-hand sides with b == 0 (scipy returns b), over the grid.
 template <int NRHS>
 __global__ void g_final(Args a) {
     const St& S = *a.st;
     for (int c = 0; c < NRHS; ++c) {
         if (!S.zero_x[c]) continue;
-        for (int i = threadIdx.x; i < a.n; i += blockDim.x) a.x[(size_t)i * NRHS + c] = 0.0;
+        for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x)
+            a.x[(size_t)i * NRHS + c] = 0.0;
     }
-    if (threadIdx.x == 0) {
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
         for (int c = 0; c < NRHS; ++c) {
             int st = S.status[c], its = S.iters[c];
             if (!S.done[c]) {

@@ -45,6 +45,7 @@
 
 #include "kcfd_common.h"
 #include "team.cuh"
+#include "amg.h"
 #include "graph_engine.cuh"
 
 namespace kcfd {
@@ -901,6 +902,35 @@ __global__ void __launch_bounds__(MAXB, 1) solve_cta_kernel(SolveArgs a) {
     else solve_fp64<NRHS, PREC>(tm, a, smem);
 }
 
+// z = M^-1 r with the handle's ILU factors (one right-hand side, FP64): r into the
+// level-permuted order, the two sweeps, and back.
+template <class Team>
+__device__ void ilu_precond_apply(Team& tm, const SolveArgs& a) {
+    for_my_rows(tm, a, [&](int s0, int s1) {
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) a.pb[i] = a.b[a.perm[i]];
+    });
+    if (!tm.sync()) return;
+    if (!ilu_apply<double, 1>(tm, a, a.pb, a.px)) return;
+    if (!tm.sync()) return;
+    for_my_rows(tm, a, [&](int s0, int s1) {
+        for (int i = s0 + threadIdx.x; i < s1; i += blockDim.x) a.x[a.perm[i]] = a.px[i];
+    });
+}
+
+__global__ void __launch_bounds__(512, 1) ilu_apply_grid_kernel(SolveArgs a) {
+    GridTeam tm(a.ctl);
+    ilu_precond_apply(tm, a);
+}
+
+__global__ void __launch_bounds__(1024, 1) ilu_apply_cta_kernel(SolveArgs a) {
+    CtaTeam tm;
+    ilu_precond_apply(tm, a);
+}
+
+__global__ void jacobi_apply_kernel(int n, const double* __restrict__ dinv, const double* r, double* z) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) z[i] = dinv[i] * r[i];
+}
+
 // ------------------------------------------------------------- batched systems --
 // Many independent systems of uneven size in ONE persistent launch: each CTA takes
 // the next system from a queue (largest first), builds its Jacobi inverse diagonal and
@@ -1197,6 +1227,8 @@ struct kcfd_solver {
     double* pb = nullptr;
     void* lu = nullptr;
     void* ludinv = nullptr;
+    // KCFD_PREC_AMG: the multigrid hierarchy (graph engine only)
+    kcfd_amg* amg = nullptr;
     // team control
     unsigned int* bar = nullptr;
     double* partials = nullptr;
@@ -1248,6 +1280,7 @@ void* solve_kernel_ptr(int mixed, int nrhs, int prec, bool grid, int block) {
 
 int free_solver(kcfd_solver* s) {
     if (!s) return KCFD_OK;
+    if (s->amg) kcfd_amg_destroy(s->amg);
     if (s->g.exec) cudaGraphExecDestroy(s->g.exec);
     if (s->g.graph) cudaGraphDestroy(s->g.graph);
     {
@@ -1431,6 +1464,11 @@ template <int NRHS, int PREC>
 void ge_body(const ge::Args& a, const GeGrid& G, cudaStream_t cs, bool pdl) {
     ge_launch(ge::g_p<NRHS, PREC>, G.p, cs, pdl, a);
     auto sweeps = [&](int which) {
+        if (PREC == KCFD_PREC_AMG) {
+            // phat = M^-1 p, shat = M^-1 s: one V-cycle each, skipped once the loop flag drops
+            amg::vcycle((const kcfd_amg*)a.amg, which ? a.r : a.p, which ? a.sh : a.ph, &a.st->active, cs, pdl);
+            return;
+        }
         if (PREC != KCFD_PREC_ILU0) return;
         if (a.nlev == 1) {
             ge_launch(ge::g_bwd<NRHS>, G.bwd, cs, pdl, a, 0, which);
@@ -1464,7 +1502,7 @@ int ge_eager(kcfd_solver* s, cudaStream_t st) {
         for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC>(a, G, st, s->g.pdl);
         KCFD_CUDA(cudaGetLastError());
     }
-    ge::g_final<NRHS><<<1, 256, 0, st>>>(a);
+    ge::g_final<NRHS><<<ge_fill_grid(s, s->n), 256, 0, st>>>(a);
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }
@@ -1501,6 +1539,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     a.out_status = g.res_i + 3;
     a.out_relres = g.res_d;
     a.eager = g.eager;
+    a.amg = s->amg;
     if (g.exec) cudaGraphExecDestroy(g.exec);
     if (g.graph) cudaGraphDestroy(g.graph);
     g.exec = nullptr;
@@ -1564,7 +1603,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     KCFD_CUDA(e3);
     if (e == cudaSuccess) {
         kp.func = (void*)ge::g_final<NRHS>;
-        kp.gridDim = dim3(1);
+        kp.gridDim = dim3(ge_fill_grid(s, n));
         kp.blockDim = dim3(256);
         e = cudaGraphAddKernelNode(&n_fin, g.graph, &n_cond, 1, &kp);
     }
@@ -1592,7 +1631,7 @@ int ge_dispatch(const kcfd_solver* s, Ts... args) {
 #define GE_CASE(R, P) \
     if (r == R && p == P) return F<R, P>::run(args...);
     GE_CASE(1, 0) GE_CASE(1, 1) GE_CASE(1, 2) GE_CASE(2, 0) GE_CASE(2, 1) GE_CASE(2, 2)
-    GE_CASE(3, 0) GE_CASE(3, 1) GE_CASE(3, 2)
+    GE_CASE(3, 0) GE_CASE(3, 1) GE_CASE(3, 2) GE_CASE(1, 3)
 #undef GE_CASE
     set_error("graph engine: unsupported configuration (nrhs %d, precond %d)", r, p);
     return KCFD_BAD_INPUT;
@@ -1820,7 +1859,11 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     KCFD_REQUIRE(A->n > 0 && A->nnz >= A->n && A->indptr && A->indices, "kcfd_solver_create: bad CSR (n=%d nnz=%d)",
                  A->n, A->nnz);
     KCFD_REQUIRE(opts->nrhs >= 1 && opts->nrhs <= 3, "kcfd_solver_create: nrhs must be 1, 2 or 3");
-    KCFD_REQUIRE(opts->precond >= 0 && opts->precond <= 2, "kcfd_solver_create: bad precond");
+    KCFD_REQUIRE(opts->precond >= 0 && opts->precond <= 3, "kcfd_solver_create: bad precond");
+    const bool amg = opts->precond == KCFD_PREC_AMG;
+    KCFD_REQUIRE(!amg || opts->nrhs == 1, "kcfd_solver_create: the AMG preconditioner takes one right-hand side");
+    KCFD_REQUIRE(!amg || opts->team == 0 || opts->team == 3,
+                 "kcfd_solver_create: the AMG preconditioner runs on the graph engine (team 0 or 3)");
     KCFD_REQUIRE(opts->mode == KCFD_MODE_FP64 || opts->mode == KCFD_MODE_MIXED, "kcfd_solver_create: bad mode");
     KCFD_REQUIRE(opts->stop == KCFD_STOP_SCIPY || opts->stop == KCFD_STOP_GPU, "kcfd_solver_create: bad stop rule");
     KCFD_REQUIRE(!(opts->mode == KCFD_MODE_MIXED && opts->stop == KCFD_STOP_GPU),
@@ -1828,6 +1871,10 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     KCFD_REQUIRE(opts->maxiter >= 0, "kcfd_solver_create: maxiter < 0");
     auto* s = new kcfd_solver();
     s->o = *opts;
+    // AMG: the Krylov iteration is FP64 on the graph engine; MIXED selects an FP32
+    // multigrid hierarchy (below), so the handle itself runs in FP64
+    const int amg_mode = opts->mode;
+    if (amg) s->o.mode = KCFD_MODE_FP64;
     if (s->o.mode == KCFD_MODE_MIXED) {
         if (s->o.inner_rtol <= 0) s->o.inner_rtol = 1e-3;
         if (s->o.max_refine <= 0) s->o.max_refine = 60;
@@ -1844,7 +1891,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     }
     s->sm_count = prop.multiProcessorCount;
     const int nrhs = opts->nrhs;
-    const bool mixed = opts->mode == KCFD_MODE_MIXED;
+    const bool mixed = s->o.mode == KCFD_MODE_MIXED;
     const size_t vsz = mixed ? sizeof(float) : sizeof(double);
     const int n = A->n, nnz = A->nnz;
     std::vector<int> ip(n + 1), ix(nnz);
@@ -1870,7 +1917,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     // a 4,096-row p' system: one CTA 35 us per Krylov iteration, the grid kernel 18 us,
     // the graph engine 25 us. A caller that runs many small solves concurrently (the
     // served loop) asks for one CTA explicitly, so that they overlap.
-    int team = opts->team;
+    int team = amg ? 3 : opts->team;
     if (team == 0) {
         const int64_t unk = (int64_t)n * nrhs;
         team = (unk <= 1024) ? 1 : ((mixed || unk <= 40000) ? 2 : 3);
@@ -2011,8 +2058,10 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     }
     // team 3 keeps the grid kernel's launch shape too: it factors ILU(0) with the
     // grid factor kernel and solves on the grid kernel inside stream captures
-    void* kern = solve_kernel_ptr(mixed, nrhs, opts->precond, team >= 2, s->block);
-    if (team >= 2) {
+    void* kern = amg ? nullptr : solve_kernel_ptr(mixed, nrhs, opts->precond, team >= 2, s->block);
+    if (amg) {
+        s->grid = 1;  // no persistent kernel: AMG solves run only on the graph engine
+    } else if (team >= 2) {
         int per_sm = 0;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, s->block, 0) != cudaSuccess || per_sm < 1) {
             free_solver(s);
@@ -2048,6 +2097,17 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         free_solver(s);
         set_error("kcfd_solver_create: device allocation failed");
         return KCFD_CUDA_ERROR;
+    }
+    if (amg) {
+        kcfd_amg_opts_t ao;
+        std::memset(&ao, 0, sizeof(ao));
+        ao.mode = amg_mode;
+        ao.max_levels = opts->amg_max_levels;
+        ao.coarse_max = opts->amg_coarse_max;
+        if (int e = kcfd_amg_create(A, &ao, &s->amg)) {
+            free_solver(s);
+            return e;
+        }
     }
     if (team == 3) {
         int e = ge_alloc(s);
@@ -2085,6 +2145,7 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
         rowsum_f32_kernel<<<rblocks, threads, 0, st>>>(s->n, A->indptr, A->indices, A->vals64, s->v32own);
         KCFD_CUDA(cudaGetLastError());
     }
+    if (s->o.precond == KCFD_PREC_AMG) return amg::setup(s->amg, A->vals64, st);
     if (s->o.precond == KCFD_PREC_JACOBI) {
         const int blocks = std::min((s->n + threads - 1) / threads, s->sm_count * 8);
         if (mixed)
@@ -2132,6 +2193,8 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
         KCFD_CUDA(cudaStreamIsCapturing((cudaStream_t)stream, &cap));
         if (cap == cudaStreamCaptureStatusNone)
             return ge_solve(s, A, b, x, iters, relres, status, (cudaStream_t)stream);
+        KCFD_REQUIRE(s->o.precond != KCFD_PREC_AMG,
+                     "kcfd_solver_solve: an AMG solve runs as its own graph; issue it outside stream capture");
     }
     void* kern = solve_kernel_ptr(mixed, s->o.nrhs, s->o.precond, s->team >= 2, s->block);
     KCFD_REQUIRE(kern != nullptr, "kcfd_solver_solve: no kernel for this configuration");
@@ -2139,12 +2202,49 @@ int kcfd_solver_solve(kcfd_solver* s, const kcfd_csr_t* A, const double* b, doub
     return launch_team(s, kern, args, (cudaStream_t)stream);
 }
 
+int kcfd_solver_apply_precond(kcfd_solver* s, const kcfd_csr_t* A, const double* r, double* z, void* stream) {
+    KCFD_REQUIRE(s && A && r && z, "kcfd_solver_apply_precond: NULL argument");
+    KCFD_REQUIRE(s->o.nrhs == 1, "kcfd_solver_apply_precond: one right-hand side only");
+    KCFD_REQUIRE(s->o.mode == KCFD_MODE_FP64, "kcfd_solver_apply_precond: FP64 handles only");
+    KCFD_REQUIRE(A->n == s->n && A->nnz == s->nnz, "kcfd_solver_apply_precond: matrix size differs from the bound pattern");
+    cudaStream_t st = (cudaStream_t)stream;
+    switch (s->o.precond) {
+        case KCFD_PREC_NONE:
+            KCFD_CUDA(cudaMemcpyAsync(z, r, (size_t)s->n * sizeof(double), cudaMemcpyDeviceToDevice, st));
+            return KCFD_OK;
+        case KCFD_PREC_JACOBI: {
+            const int blocks = std::max(1, std::min((s->n + 255) / 256, s->sm_count * 8));
+            jacobi_apply_kernel<<<blocks, 256, 0, st>>>(s->n, (const double*)s->dinv, r, z);
+            KCFD_CUDA(cudaGetLastError());
+            return KCFD_OK;
+        }
+        case KCFD_PREC_ILU0: {
+            SolveArgs a = make_args(s, A);
+            a.b = r;
+            a.x = z;
+            void* args[] = {&a};
+            void* k = s->team >= 2 ? (void*)ilu_apply_grid_kernel : (void*)ilu_apply_cta_kernel;
+            return launch_team(s, k, args, st);
+        }
+        case KCFD_PREC_AMG: return amg::vcycle(s->amg, r, z, nullptr, st, false);
+        default: break;
+    }
+    set_error("kcfd_solver_apply_precond: unknown preconditioner");
+    return KCFD_BAD_INPUT;
+}
+
+int kcfd_solver_amg(const kcfd_solver* s, kcfd_amg** out) {
+    KCFD_REQUIRE(s && out, "kcfd_solver_amg: NULL argument");
+    *out = s->amg;
+    return KCFD_OK;
+}
+
 int kcfd_solver_info(const kcfd_solver* s, int32_t* info4) {
     KCFD_REQUIRE(s && info4, "kcfd_solver_info: NULL argument");
     info4[0] = s->team;
     info4[1] = s->lanes;
     info4[2] = s->block;
-    info4[3] = s->nlev > 0 ? s->nlev : 1;
+    info4[3] = s->amg ? amg::levels(s->amg) : (s->nlev > 0 ? s->nlev : 1);
     return KCFD_OK;
 }
 

@@ -14,7 +14,7 @@ LIB_PATH = os.path.join(PKG_DIR, "libkcfd.so")
 
 OK, MAXITER, BREAKDOWN, BAD_INPUT, CUDA_ERROR, TIMEOUT = 0, 1, 2, 3, 4, 5
 STATUS_NAMES = {0: "OK", 1: "MAXITER", 2: "BREAKDOWN", 3: "BAD_INPUT", 4: "CUDA_ERROR", 5: "TIMEOUT"}
-PREC = {"none": 0, "jacobi": 1, "ilu0": 2}
+PREC = {"none": 0, "jacobi": 1, "ilu0": 2, "amg": 3}
 STOP_SCIPY, STOP_GPU = 0, 1
 MODE_FP64, MODE_MIXED = 0, 1
 
@@ -47,7 +47,16 @@ class Csr(C.Structure):
 class SolverOpts(C.Structure):
     _fields_ = [("precond", i32), ("stop", i32), ("mode", i32), ("nrhs", i32), ("maxiter", i32), ("team", i32),
                 ("lanes", i32), ("block", i32), ("rtol", f64), ("atol", f64), ("inner_rtol", f64),
-                ("max_refine", i32), ("inner_maxiter", i32), ("fill_level", i32)]
+                ("max_refine", i32), ("inner_maxiter", i32), ("fill_level", i32), ("amg_max_levels", i32),
+                ("amg_coarse_max", i32)]
+
+
+class AmgOpts(C.Structure):
+    _fields_ = [("mode", i32), ("coarse_max", i32), ("max_levels", i32), ("power_iters", i32)]
+
+
+AMG_ITEMS = {"aggregates": 0, "indptr": 1, "indices": 2, "values": 3, "p_indptr": 4, "p_indices": 5,
+             "p_values": 6, "omega": 7, "coarse_inverse": 8}
 
 
 class TfParams(C.Structure):
@@ -76,6 +85,14 @@ SIGNATURES = {
     "kcfd_solver_solve": (i32, [vp, C.POINTER(Csr), vp, vp, vp, vp, vp, vp]),
     "kcfd_solver_error": (i32, [vp, P_i32, vp]),
     "kcfd_solver_info": (i32, [vp, P_i32]),
+    "kcfd_solver_apply_precond": (i32, [vp, C.POINTER(Csr), vp, vp, vp]),
+    "kcfd_solver_amg": (i32, [vp, C.POINTER(vp)]),
+    "kcfd_amg_create": (i32, [C.POINTER(Csr), C.POINTER(AmgOpts), C.POINTER(vp)]),
+    "kcfd_amg_setup": (i32, [vp, C.POINTER(Csr), vp]),
+    "kcfd_amg_apply": (i32, [vp, vp, vp, vp]),
+    "kcfd_amg_info": (i32, [vp, P_i32, P_i64, P_i64]),
+    "kcfd_amg_export": (i32, [vp, i32, i32, vp]),
+    "kcfd_amg_destroy": (None, [vp]),
     "kcfd_lsq_gradient": (i32, [vp, vp, vp, vp, vp]),
     "kcfd_tf_drag": (i32, [vp, vp, vp, vp, vp, vp, vp]),
     "kcfd_tf_interfacial": (i32, [vp, vp, vp, vp, vp, vp, vp]),

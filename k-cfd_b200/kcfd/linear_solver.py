@@ -13,8 +13,10 @@ device failure raises instead of falling back to the CPU. Semantics kept:
     so agreement with it is at the solution level) | 'iluk' (structural ILU(k),
     fill_level=k, default 1, on a distance-(k+1) colouring; the reference's 'iluk'
     is SuperLU's threshold ILU with fill_factor=3 (:56-61), so agreement is again at
-    the solution level and fill_factor is not used) | 'amg' (falls back to 'ilu0' as
-    the reference does without pyamg, :63-66).
+    the solution level and fill_factor is not used) | 'amg' (device smoothed-aggregation
+    multigrid, kcfd.amg; the reference's is pyamg's (:63-74), absent here, so
+    agreement is at the solution level; max_levels and max_coarse are honoured, the
+    coarsest level being at most 256 rows).
   * method='direct': the device has no sparse LU; BiCGSTAB + ILU(0) to a relative
     residual of 1e-12 stands in for spsolve (documented difference).
 system may be the reference's FVMSystem (anything with .to_sparse() and .rhs), a
@@ -34,26 +36,47 @@ SCIPY_DEFAULT_RTOL = 1e-5
 
 
 def create_preconditioner(A_csr, method="none", **kwargs):
-    """Returns (M, info) like core/preconditioner.py:18-76. M is a device
-    preconditioner descriptor consumed by solve_linear_system / Solver."""
+    """(M, info) as core/preconditioner.py:18-76: M is None for 'none', else a
+    scipy.sparse.linalg.LinearOperator whose matvec applies the device preconditioner
+    (host vector in, host vector out; kcfd_solver_apply_precond), so M can be handed to
+    scipy's Krylov solvers as the reference's is. info carries 'method' and
+    'setup_time' like the reference's, ('levels', 'complexity' for 'amg'), and under
+    'device' the handle and device matrix for callers that stay on the device."""
+    from scipy.sparse.linalg import LinearOperator
+    torch = _lib.require_cuda()
     t0 = time.time()
-    if method == "amg":
-        print("  [Preconditioner] amg not built on the device path; using ILU(0).")
-        return create_preconditioner(A_csr, "ilu0")
-    fill = 0
-    name = method
-    if method == "iluk":
-        fill = int(kwargs.get("fill_level", 1))
-        method, name = "ilu0", f"iluk(level={fill})"
-    if method not in _lib.PREC:
-        raise ValueError(f"Unknown preconditioner: {method}")
     if method == "none":
         return None, {"method": "none", "setup_time": 0.0}
+    fill = 0
+    name = method
+    prec = method
+    if method == "iluk":
+        fill = int(kwargs.get("fill_level", 1))
+        prec, name = "ilu0", f"iluk(level={fill})"
+    if prec not in _lib.PREC:
+        raise ValueError(f"Unknown preconditioner: {method}")
     d = DeviceCSR.from_scipy(A_csr) if not isinstance(A_csr, DeviceCSR) else A_csr
-    s = Solver(d, precond=method, levels=None if fill else kwargs.get("levels"), fill_level=fill)
+    s = Solver(d, precond=prec, levels=None if fill else kwargs.get("levels"), fill_level=fill,
+               amg_max_levels=int(kwargs.get("max_levels", 0)) if prec == "amg" else 0,
+               amg_coarse_max=min(int(kwargs.get("max_coarse", 0)), 256) if prec == "amg" else 0)
     s.setup(d)
-    _lib.require_cuda().cuda.synchronize()
-    return {"method": name, "solver": s, "csr": d}, {"method": name, "setup_time": time.time() - t0}
+    n = d.n
+    r_dev = torch.empty(n, dtype=torch.float64, device=d.vals64.device)
+    z_dev = torch.empty_like(r_dev)
+
+    def matvec(v):
+        r_dev.copy_(torch.from_numpy(np.ascontiguousarray(np.asarray(v, dtype=np.float64).ravel())))
+        s.apply_precond(d, r_dev, z_dev)
+        return z_dev.cpu().numpy()
+
+    M = LinearOperator((n, n), matvec=matvec, dtype=np.float64)
+    torch.cuda.synchronize()
+    info = {"method": name, "setup_time": time.time() - t0, "device": {"solver": s, "csr": d}}
+    if prec == "amg":
+        ai = s.amg_info()
+        info["levels"] = ai["levels"]
+        info["complexity"] = float(sum(ai["nnz"]) / max(ai["nnz"][0], 1))
+    return M, info
 
 
 def _as_device(system):
@@ -80,8 +103,6 @@ def solve_linear_system(system, x0=None, method="direct", tol=1e-8, maxiter=1000
         prec, atol, rtol_eff, its = "ilu0", 0.0, DIRECT_RTOL, max(maxiter, 20 * n)
     elif method == "bicgstab":
         prec, atol, rtol_eff, its = preconditioner, float(tol), float(rtol), maxiter
-        if prec == "amg":
-            prec = "ilu0"
         if prec == "iluk":
             prec, fill, levels = "ilu0", int(precond_kwargs.pop("fill_level", 1)), None
             precond_kwargs.pop("fill_factor", None)
@@ -91,8 +112,12 @@ def solve_linear_system(system, x0=None, method="direct", tol=1e-8, maxiter=1000
         raise ValueError(f"Unknown solver method: {method}")
     x = torch.zeros(n, dtype=torch.float64, device=b.device) if x0 is None else \
         torch.from_numpy(np.array(x0, dtype=np.float64)).to(b.device)
+    amg_kw = {}
+    if prec == "amg":
+        amg_kw = {"amg_max_levels": int(precond_kwargs.pop("max_levels", 0)),
+                  "amg_coarse_max": min(int(precond_kwargs.pop("max_coarse", 0)), 256)}
     s = Solver(d, precond=prec, stop=_lib.STOP_SCIPY, maxiter=its, rtol=rtol_eff, atol=atol, levels=levels,
-               fill_level=fill)
+               fill_level=fill, **amg_kw)
     s.setup(d)
     it, rr, st = s.solve(d, b, x)
     status = int(st[0])

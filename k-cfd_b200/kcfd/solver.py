@@ -76,7 +76,9 @@ class DeviceCSR:
 class Solver:
     """BiCGSTAB handle for one pattern.
 
-    precond: 'none' | 'jacobi' | 'ilu0'; stop: _lib.STOP_SCIPY | _lib.STOP_GPU;
+    precond: 'none' | 'jacobi' | 'ilu0' | 'amg' (smoothed-aggregation multigrid, one right-hand
+    side, graph engine; mode MIXED keeps the Krylov iteration FP64 and stores the multigrid
+    hierarchy in FP32); stop: _lib.STOP_SCIPY | _lib.STOP_GPU;
     mode: _lib.MODE_FP64 | _lib.MODE_MIXED; nrhs: 1 or 3; team: 0 auto, 1 one CTA,
     2 whole grid (persistent cooperative kernel), 3 graph engine (phase kernels in a
     CUDA graph with a device-side WHILE loop; FP64 only); levels: ILU(0) level of each row (e.g. mesh.cell_color), None for
@@ -86,7 +88,7 @@ class Solver:
 
     def __init__(self, csr, precond="jacobi", stop=_lib.STOP_SCIPY, mode=_lib.MODE_FP64, nrhs=1, maxiter=1000,
                  rtol=1e-8, atol=0.0, team=0, lanes=0, block=0, inner_rtol=1e-3, max_refine=60, levels=None,
-                 inner_maxiter=400, fill_level=0):
+                 inner_maxiter=400, fill_level=0, amg_max_levels=0, amg_coarse_max=0):
         torch = _lib.require_cuda()
         if precond not in _lib.PREC:
             raise ValueError(f"Unknown preconditioner: {precond}")
@@ -96,6 +98,7 @@ class Solver:
         o.rtol, o.atol, o.inner_rtol, o.max_refine = float(rtol), float(atol), float(inner_rtol), int(max_refine)
         o.inner_maxiter = int(inner_maxiter)
         o.fill_level = int(fill_level)
+        o.amg_max_levels, o.amg_coarse_max = int(amg_max_levels), int(amg_coarse_max)
         self.opts = o
         self.n, self.nrhs, self.mode = csr.n, nrhs, mode
         self.precond = precond
@@ -140,8 +143,29 @@ class Solver:
                                                 _lib.stream_handle(stream)), "kcfd_solver_solve")
         return self.iters, self.relres, self.status
 
+    def apply_precond(self, csr, r, z=None, stream=None):
+        """z = M^-1 r with the set-up preconditioner (one right-hand side, FP64 tensors)."""
+        torch = _lib.require_cuda()
+        if z is None:
+            z = torch.empty_like(r)
+        d = csr.desc()
+        _lib.check(_lib.lib().kcfd_solver_apply_precond(self._h, C.byref(d), _lib.ptr(r), _lib.ptr(z),
+                                                        _lib.stream_handle(stream)), "kcfd_solver_apply_precond")
+        return z
+
+    def amg_info(self):
+        """Levels, rows and entries per level and device bytes of the multigrid hierarchy
+        (precond 'amg')."""
+        from .amg import info_of
+        h = C.c_void_p()
+        _lib.check(_lib.lib().kcfd_solver_amg(self._h, C.byref(h)), "kcfd_solver_amg")
+        if not h.value:
+            raise ValueError("not an AMG handle")
+        return info_of(h)
+
     def info(self):
-        """Resolved launch shape: dict(team, lanes, block, levels)."""
+        """Resolved launch shape: dict(team, lanes, block, levels); levels is the ILU
+        level count, or the multigrid level count with precond 'amg'."""
         v = np.zeros(4, dtype=np.int32)
         _lib.check(_lib.lib().kcfd_solver_info(self._h, v.ctypes.data_as(_lib.P_i32)), "kcfd_solver_info")
         return {"team": int(v[0]), "lanes": int(v[1]), "block": int(v[2]), "levels": int(v[3])}

@@ -284,3 +284,54 @@ def spilu_reference(A):
     from scipy.sparse.linalg import spilu
     ilu = spilu(sparse.csr_matrix(A).tocsc(), fill_factor=1, drop_tol=0)
     return ilu.solve
+
+
+def greedy_colouring(A):
+    """Greedy colouring of A's rows in row order: each row takes the smallest colour not
+    used by an already coloured neighbour (off-diagonal entries of its row). The same
+    rule as the device mesh builder's cell colouring (one colour per level of the
+    device ILU(0)); on hexahedral meshes it gives the red-black parity colouring."""
+    A = sparse.csr_matrix(A)
+    n = A.shape[0]
+    ip, ix = A.indptr.tolist(), A.indices.tolist()
+    col = [-1] * n
+    for i in range(n):
+        used = {col[j] for j in ix[ip[i]:ip[i + 1]] if j != i and col[j] >= 0}
+        c = 0
+        while c in used:
+            c += 1
+        col[i] = c
+    return np.asarray(col, dtype=np.int64)
+
+
+def ilu0_two_colour(A, colour):
+    """Structural ILU(0) of A in a two-colour ordering (colour 0 rows first, row order
+    kept inside a colour), vectorised: with no coupling inside a colour the factor is
+    L = I + A_10 D_0^-1, U = [D_0, A_01; 0, D_1'] with D_1' = D_1 - diag(A_10 D_0^-1 A_01)
+    -- the IKJ ILU(0) (ilu0_factor) of the permuted matrix, entry for entry. Returns
+    M^-1 as a function of a vector in A's own ordering."""
+    A = sparse.csr_matrix(A)
+    colour = np.asarray(colour)
+    if colour.max() > 1:
+        raise ValueError("ilu0_two_colour needs a two-colour ordering")
+    r = np.flatnonzero(colour == 0)
+    k = np.flatnonzero(colour == 1)
+    A00, A01 = A[r][:, r], A[r][:, k]
+    A10, A11 = A[k][:, r], A[k][:, k]
+    if (A00 - sparse.diags(A00.diagonal())).count_nonzero() or (A11 - sparse.diags(A11.diagonal())).count_nonzero():
+        raise ValueError("rows of one colour are coupled")
+    d0 = A00.diagonal()
+    L10 = (A10 @ sparse.diags(1.0 / d0)).tocsr()
+    d1 = A11.diagonal() - np.asarray(L10.multiply(A01.T.tocsr()).sum(axis=1)).ravel()
+    A01 = A01.tocsr()
+
+    def apply(q):
+        q = np.asarray(q, dtype=np.float64)
+        y0 = q[r]
+        z1 = (q[k] - L10 @ y0) / d1
+        z = np.empty_like(q)
+        z[k] = z1
+        z[r] = (y0 - A01 @ z1) / d0
+        return z
+
+    return apply

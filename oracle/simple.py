@@ -52,7 +52,7 @@ class Simple:
         self.solver = "direct"      # or "bicgstab"
         self.rtol = 1e-8
         self.precond_u = "jacobi"
-        self.precond_p = "jacobi"   # 'jacobi' | 'ilu0' (structural) | 'spilu' (reference)
+        self.precond_p = "jacobi"   # 'jacobi' | 'ilu0' (structural, two-colour) | 'spilu' (reference)
         self.maxiter = 5000
         self.muscl = None
         self.nonorth = False
@@ -228,6 +228,12 @@ class Simple:
             M = linsolve.jacobi(A)
         elif precond == "spilu":
             M = linsolve.spilu_reference(A)
+        elif precond == "ilu0":
+            # structural ILU(0) in the greedy (red-black on hexes) cell colouring, the
+            # device's ILU(0) ordering; the colouring depends on the pattern only
+            if getattr(self, "_colour", None) is None or len(self._colour) != A.shape[0]:
+                self._colour = linsolve.greedy_colouring(A)
+            M = linsolve.ilu0_two_colour(A, self._colour)
         elif precond == "none":
             M = None
         else:

@@ -59,7 +59,7 @@ def _mirrors():
     return {"kcfd_mesh_export_t": _lib.MeshExport, "kcfd_csr_t": _lib.Csr, "kcfd_solver_opts_t": _lib.SolverOpts,
             "kcfd_batch_opts_t": BatchOpts, "kcfd_dmesh_t": DMeshDesc, "kcfd_bc_t": BCDesc,
             "kcfd_mom_params_t": _lib.MomParams, "kcfd_tf_params_t": _lib.TfParams,
-            "kcfd_face_layout_t": _lib.FaceLayout}
+            "kcfd_face_layout_t": _lib.FaceLayout, "kcfd_amg_opts_t": _lib.AmgOpts}
 
 
 @pytest.mark.skipif(shutil.which("gcc") is None, reason="needs gcc")

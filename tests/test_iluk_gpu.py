@@ -71,4 +71,6 @@ def test_iluk_drop_in_and_create_preconditioner():
                                 rtol=1e-10, fill_level=lvl, fill_factor=3)
         assert _rel(x, xd) < 1e-8
     M, info = create_preconditioner(A, "iluk", fill_level=2)
-    assert info["method"] == "iluk(level=2)" and M["solver"].info()["levels"] >= 2
+    assert info["method"] == "iluk(level=2)" and info["device"]["solver"].info()["levels"] >= 2
+    x, inf = spla.bicgstab(A, b, rtol=1e-10, atol=0.0, maxiter=3000, M=M)
+    assert inf == 0 and _rel(x, xd) < 1e-8

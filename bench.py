@@ -4,21 +4,32 @@ Workload (the headline config that fits one GPU): 128^3 hexahedra (2,097,152 cel
 the unit cube, interior nodes jittered by U(-0.2, 0.2) x spacing (seed 0), Re = 400
 (rho = 1, mu = 0.0025), MUSCL van Leer deferred correction, over-relaxed
 non-orthogonal correction, Green-Gauss gradients, BiCGSTAB + Jacobi for u, v, w and
-BiCGSTAB + ILU(0) (red-black levels) for p', each to a 1e-8 relative residual;
-alpha_u = 0.7, alpha_p = 0.3. FP64 throughout; both solves run on the graph engine
-(phase kernels in one CUDA graph per solve with a device-side WHILE loop).
+BiCGSTAB for p' preconditioned by the device smoothed-aggregation multigrid (one V-cycle
+per apply; --p-precond ilu0 takes the red-black ILU(0) instead), each solve to a 1e-8
+relative residual; alpha_u = 0.7, alpha_p = 0.3. FP64 throughout; the solves run on the
+graph engine (phase kernels in one CUDA graph per solve with a device-side WHILE loop).
 
 A "step" is one SIMPLE outer iteration. Inputs (mesh, matrices, fields: several GB)
 are far larger than the 126 MB L2, so no flush is needed between steps.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference] [--size S]
 
+The line also carries, measured in the same run: the config's own p' preconditioner
+(ILU(0)) as `ilu0_variant`; the mixed form (FP32 multigrid hierarchy and momentum inner
+iterations, FP64 Krylov residuals) with its relative L2 error against the FP64 fields
+per component (u, v, w, p, p'); a bounded batched leg of C4 (1,024-system p' batch:
+its first systems, batched against the plain drop-in) and a short served leg of C5
+(Poisson-arriving cavities, served against serial); and the CPU baseline: one full
+outer iteration of the same 128^3 workload by the oracle on the host, measured, not
+scaled.
+
 Multi-GPU: one mesh does not shard without a halo exchange, so N > 1 runs N
 independent replicas (one per rank, torch.distributed over NCCL for the barrier and
 the max-over-ranks timing); value = total iterations / max time.
 
 --impl reference times the oracle (the numpy/scipy restatement of the reference's
-path) on the host cores with a bounded per-step sample (see cpu_baseline.sample).
+path, with the device's red-black ILU(0) for p') on the host cores on the full 128^3
+workload, as many whole outer iterations as fit its time budget.
 """
 from __future__ import annotations
 
@@ -38,7 +49,7 @@ import numpy as np  # noqa: E402
 
 METRIC = "SIMPLE outer iterations/s (3D jittered cavity, 1e-8 relative residual per solve)"
 UNIT = "iters/s"
-CPU_SAMPLE_N = 40
+REF_BUDGET_S = 160.0   # reference arm: whole 128^3 outer iterations while the timed work stays below this
 
 
 def cavity_arrays(N, seed=0):
@@ -48,14 +59,15 @@ def cavity_arrays(N, seed=0):
     return nodes, cells, cf, bd
 
 
-def make_solver(N, precision="mixed", graph=True):
+def make_solver(N, precision="fp64", graph=True, p_precond="amg", mesh=None):
     from kcfd import mesh as km
     from kcfd.simple import SIMPLESolver
-    nodes, cells, cf, bd = cavity_arrays(N)
-    m = km.build_mesh(nodes, cells, bd, ndim=3, cell_face_node_list=cf)
-    s = SIMPLESolver(m, rho=1.0, mu=0.0025, precision=precision, precond_p="ilu0", ilu_order="color",
+    if mesh is None:
+        nodes, cells, cf, bd = cavity_arrays(N)
+        mesh = km.build_mesh(nodes, cells, bd, ndim=3, cell_face_node_list=cf)
+    s = SIMPLESolver(mesh, rho=1.0, mu=0.0025, precision=precision, precond_p=p_precond, ilu_order="color",
                      rtol=1e-8, maxiter=20000, muscl="van_leer", nonorth=True, graph=graph)
-    for nm in m.boundary_patches:
+    for nm in mesh.boundary_patches:
         s.set_velocity_bc(nm, "dirichlet", [1.0, 0.0, 0.0] if nm == "lid" else [0.0, 0.0, 0.0])
         s.set_pressure_bc(nm, "zero_gradient")
     s.alpha_u, s.alpha_p, s.tol = 0.7, 0.3, 0.0
@@ -123,30 +135,65 @@ def measured_peak():
     return 6650.0, "fallback"
 
 
-# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of the nine phase kernels
-# of one p' Krylov iteration on the 128^3 cavity, from one ncu capture of the graph
-# engine (KCFD_ENGINE_EAGER=1, one Krylov iteration captured); the roofline's traffic is this
-# times the solve's Krylov count (the kernels and their sizes repeat every iteration).
-NCU_P_ITER_DRAM_BYTES_128 = 857019136
+# DRAM bytes (dram__bytes_read.sum + dram__bytes_write.sum) of one p' Krylov iteration
+# on the 128^3 cavity, from an ncu launch list of one solve on the graph engine
+# (KCFD_ENGINE_EAGER=1, every kernel of the solve captured, one pass each), divided
+# by the solve's Krylov count; the roofline's traffic is this times the timed solve's
+# count. Keyed by preconditioner; None where no capture was made.
+NCU_P_ITER_DRAM_BYTES_128 = {"ilu0": 857019136, "amg": None}
 
 
-def solver_bytes(n, nnz, iters, precond, w, nrhs=1):
+def amg_levels(solver):
+    """Rows, entries and prolongator entries of each level of an AMG handle."""
+    return solver.amg_levels() if solver.precond == "amg" else None
+
+
+def vcycle_bytes(levels, w):
+    """Algorithmic bytes of one V(1,1) cycle (each array once per kernel): per level l
+    above the coarsest, the pre-smoothing and residual (W values and columns, b, omega
+    D^-1, x and r written), the restriction (P^T values and columns, row pointers, r,
+    the coarse right-hand side), the prolongation (P values and columns, row pointers,
+    the coarse correction, x read and written) and the post-smoothing (A values and
+    columns, x, b, omega D^-1, y); at the coarsest level the dense inverse and two
+    vectors. Level 0's b and y are the Krylov FP64 vectors."""
+    b = 0
+    L = len(levels)
+    for l in range(L - 1):
+        n, nnz, pn = levels[l]["rows"], levels[l]["nnz"], levels[l]["p_nnz"]
+        nc = levels[l + 1]["rows"]
+        wi = 8 if l == 0 else w
+        b += nnz * (w + 4) + n * (wi + 3 * w)                 # pre + residual
+        b += pn * (w + 4) + 4 * (nc + 1) + n * w + nc * w     # restriction
+        b += pn * (w + 4) + 4 * (n + 1) + nc * w + 2 * n * w  # prolongation
+        b += nnz * (w + 4) + n * (2 * w + 2 * wi)             # post-smoothing
+    nc = levels[-1]["rows"]
+    wi = 8 if L == 1 else w
+    return b + nc * nc * w + 2 * nc * wi
+
+
+def solver_bytes(n, nnz, iters, precond, w, nrhs=1, amg=None):
     """Algorithmic bytes of BiCGSTAB iterations (each array counted once per use):
     SpMV nnz(w+4) + 4(n+1) + 2 n w nrhs; ILU(0) apply nnz(w+4) + 8(n+1) + 4 n w;
-    Jacobi iteration 2 SpMV + 21 n w nrhs; ILU iteration 2 SpMV + 2 ILU + 19 n w."""
+    Jacobi iteration 2 SpMV + 21 n w nrhs; ILU iteration 2 SpMV + 2 ILU + 19 n w;
+    multigrid iteration 2 FP64 SpMV + 2 V-cycles (vcycle_bytes, hierarchy value width w)
+    + 17 n 8 (the engine's FP64 vector streams: p update 4, v.rhat 1, s 3, s read 1,
+    x and r update 8)."""
     spmv = nnz * (w + 4) + 4 * (n + 1) + 2 * n * w * nrhs
+    if precond == "amg":
+        spmv8 = nnz * 12 + 4 * (n + 1) + 16 * n
+        return iters * (2 * spmv8 + 2 * vcycle_bytes(amg, w) + 17 * n * 8)
     if precond == "ilu0":
         ilu = nnz * (w + 4) + 8 * (n + 1) + 4 * n * w
         return iters * (2 * spmv + 2 * ilu + 19 * n * w)
     return iters * (2 * spmv + 21 * n * w * nrhs)
 
 
-def outer_step_bytes(n, Fi, Fb, nnz, ndim, its_m, its_p, w=8):
+def outer_step_bytes(n, Fi, Fb, nnz, ndim, its_m, its_p, p_precond="amg", amg=None, w=8):
     """Algorithmic bytes of one SIMPLE outer iteration by the fixed formulas (each
     array counted once per use): mass flux twice, Green-Gauss of U (ndim components)
     and of p', MUSCL and momentum assembly per component, p' assembly, the momentum
-    solve (Jacobi, ndim right-hand sides) and the p' solve (ILU(0)) at the step's
-    Krylov counts. The correction and residual bookkeeping are left out."""
+    solve (Jacobi, ndim right-hand sides) and the p' solve at the step's Krylov counts.
+    The correction, residual bookkeeping and preconditioner set-up are left out."""
     F = Fi + Fb
     mass_flux = F * (8 + 8 + (1 + ndim) * 8 + 8) + n * ndim * 8
     gg = Fi * (8 + ndim * 8 + 8) + Fb * (4 + ndim * 8 + 8) + n * (16 + ndim * 8)
@@ -154,19 +201,39 @@ def outer_step_bytes(n, Fi, Fb, nnz, ndim, its_m, its_p, w=8):
     asm = Fi * (8 + (1 + ndim) * 8 + 16 + 8 + 2 * w) + Fb * (4 + (1 + ndim) * 8 + 8 + 8 + 8) + n * (32 + 2 * w)
     b = 2 * mass_flux + (ndim + 1) * gg + ndim * (muscl + asm) + asm
     b += solver_bytes(n, nnz, its_m, "jacobi", w, nrhs=ndim)
-    b += solver_bytes(n, nnz, its_p, "ilu0", w)
+    b += solver_bytes(n, nnz, its_p, p_precond, w, amg=amg)
     return b
 
 
-def solve_launches(solver, iters, precond, nlev):
+def solve_launches(solver, iters):
     """Kernels one solve launches: the persistent kernels launch once; the graph
     engine launches the value fill, init, final and the two copies plus, per loop
-    trip, the phase kernels (5, and 2 (nlev - 1) ILU sweeps for each of phat and
-    shat)."""
+    trip, the phase kernels (5), 2 (nlev - 1) ILU sweeps for each of phat and shat, or
+    two V-cycles (4 kernels per level above the coarsest and the coarse solve)."""
     if not solver.graph_engine:
         return 1
-    body = 5 + (4 * (nlev - 1) if precond == "ilu0" else 0)
+    info = solver.info()
+    body = 5
+    if solver.precond == "ilu0":
+        body += 4 * (info["levels"] - 1)
+    elif solver.precond == "amg":
+        L = info["levels"]
+        body += 2 * (1 if L == 1 else 4 * (L - 1) + 1)
     return 5 + body * int(iters)
+
+
+def setup_launches(solver, power_iters=4):
+    """Kernels of one preconditioner set-up: Jacobi 1; ILU(0) permute + factor (+ 2
+    SELL fills on the graph engine); AMG per level above the coarsest 9 (level 0) or
+    10 + power iterations, and 2 for the coarsest."""
+    if solver.precond == "jacobi":
+        return 1
+    if solver.precond == "ilu0":
+        return 2 + (2 if solver.graph_engine else 0)
+    if solver.precond == "amg":
+        L = solver.info()["levels"]
+        return (9 if L > 1 else 0) + max(0, L - 2) * (10 + power_iters) + 2
+    return 0
 
 
 def launches_per_step(s, its_m, its_p):
@@ -179,46 +246,55 @@ def launches_per_step(s, its_m, its_p):
     pp = per_colour_pass + 1
     n = 2                       # mass flux x2
     n += gg if s.gU_t is not None else 0
-    n += mom + 1 + 2            # momentum, jacobi set-up, residual norms (2)
-    n += pp + 2 + 2             # p' assembly, ILU permute + factor, norm + record
+    n += mom + 2                # momentum assembly, residual norms (2)
+    n += pp + 2                 # p' assembly, norm + record
     n += gg + 2 + 1             # GG p', correction (2), residual bookkeeping
-    nlev = s.s_p.info()["levels"]
-    n += solve_launches(s.s_m, its_m, "jacobi", 1)
-    n += solve_launches(s.s_p, its_p, "ilu0", nlev)
+    n += setup_launches(s.s_m) + setup_launches(s.s_p)
+    n += solve_launches(s.s_m, its_m)
+    n += solve_launches(s.s_p, its_p)
     return n
 
 
 def p_solve_roofline(s, peak, reps=3):
-    """The p' solve (the dominant work: >90% of the device time of an outer
-    iteration) timed alone with CUDA events on its stream; algorithmic bytes from
-    its Krylov count. Also the FP64 SpMV kernel alone on the same matrix."""
+    """The p' solve timed alone with CUDA events on its stream (after its set-up, which
+    is timed on its own); algorithmic bytes from its Krylov count. Also the FP64 SpMV
+    kernel alone on the same matrix."""
     import torch
     n, nnz = s.mesh.n_cells, s.mesh.nnz
+    pc = s.s_p.precond
     mixed = s.mode == 1
     w = 4 if mixed else 8
-    times, byts = [], []
+    amg = amg_levels(s.s_p)
+    times, byts, setups = [], [], []
     for _ in range(reps):
+        torch.cuda.synchronize()
+        e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+        e0.record()
         s.s_p.setup(s.A_p)
+        e1.record()
         s.pp_t.zero_()
         torch.cuda.synchronize()
-        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        e0.record()
+        e1b = torch.cuda.Event(enable_timing=True)
+        e1b.record()
         s.s_p.solve(s.A_p, s.b_p, s.pp_t)
-        e1.record()
+        e2.record()
         torch.cuda.synchronize()
         it = int(s.s_p.iters[0])
-        b = solver_bytes(n, nnz, it, "ilu0", w)
-        if mixed:  # outer FP64 residuals (about one per 4 inner iterations) + updates
+        b = solver_bytes(n, nnz, it, pc, w, amg=amg)
+        if mixed and pc != "amg":  # outer FP64 residuals (about one per 40 inner iterations) + updates
             nref = max(2, it // 40)
             b += nref * (nnz * 12 + 4 * (n + 1) + 2 * n * 8 + 5 * n * 8)
-        times.append(e0.elapsed_time(e1) / 1e3)
+        times.append(e1b.elapsed_time(e2) / 1e3)
+        setups.append(e0.elapsed_time(e1) / 1e3)
         byts.append(b)
     t = float(np.mean(times))
     ach = float(np.mean(byts)) / t / 1e9
     info = s.s_p.info()
-    kern = ("graph engine: g_p, g_fwd, g_bwd, g_spmv_v, g_s, g_spmv_t, g_xr per Krylov iteration "
-            "(p' BiCGSTAB + ILU(0), FP64)") if info["team"] == 3 else \
-        f"solve_grid_kernel (p' BiCGSTAB + ILU(0), {'mixed' if mixed else 'FP64'})"
+    prec_name = {"amg": f"smoothed-aggregation multigrid ({info['levels']} levels, one V(1,1) cycle per apply)",
+                 "ilu0": "ILU(0), red-black levels", "jacobi": "Jacobi"}[pc]
+    kern = (f"graph engine: g_p, V-cycle/ILU sweeps, g_spmv_v, g_s, g_spmv_t, g_xr per Krylov iteration "
+            f"(p' BiCGSTAB + {prec_name}, {'FP32 hierarchy / FP64 Krylov' if mixed else 'FP64'})"
+            if info["team"] == 3 else f"solve_grid_kernel (p' BiCGSTAB + {prec_name})")
     # SpMV alone: nnz (8 + 4) + 4 (n + 1) + 8 n (x) + 8 n (y)
     x = torch.randn(n, dtype=torch.float64, device="cuda")
     y = torch.empty_like(x)
@@ -234,29 +310,31 @@ def p_solve_roofline(s, peak, reps=3):
     torch.cuda.synchronize()
     ts = e0.elapsed_time(e1) / 1e3 / K
     sb = nnz * 12 + 4 * (n + 1) + 16 * n
-    spmv = {"kernel": "spmv_row_kernel<double> (kcfd_spmv_f64, row per thread, entries loaded before the x gathers)", "bytes": int(sb), "launch_us": round(ts * 1e6, 2),
-            "achieved": round(sb / ts / 1e9, 1), "frac": round(sb / ts / 1e9 / peak[0], 3)}
-    # bytes the engine actually moves: on ILU level 0 A M^-1 q = q, so two SpMVs skip
-    # those rows' values, columns and row pointers, and v = p, t = s there are neither
-    # stored nor read back (g_p, g_s and g_xr read p and s in their place)
+    spmv = {"kernel": "spmv_row_kernel<double> (kcfd_spmv_f64, row per thread, entries loaded before the x gathers)",
+            "bytes": int(sb), "launch_us": round(ts * 1e6, 2), "achieved": round(sb / ts / 1e9, 1),
+            "frac": round(sb / ts / 1e9 / peak[0], 3)}
+    it = int(s.s_p.iters[0])
+    per_it = solver_bytes(n, nnz, 1, pc, w, amg=amg)
     moved = None
-    if info["team"] == 3 and info["levels"] >= 2:
+    if pc == "ilu0" and info["team"] == 3 and info["levels"] >= 2:
+        # on ILU level 0 A M^-1 q = q, so two SpMVs skip those rows' values, columns
+        # and row pointers, and v = p, t = s there are neither stored nor read back
         lev = np.asarray(s.mesh.cell_color)
         rl = np.diff(np.asarray(s.mesh.indptr))
         n0, nnz0 = int((lev == 0).sum()), int(rl[lev == 0].sum())
-        per_it = solver_bytes(n, nnz, 1, "ilu0", w) - 2 * (nnz0 * (w + 4) + 4 * n0) - 4 * n0 * w
-        moved = {"bytes_per_krylov_iter": int(per_it), "achieved": round(per_it * it / t / 1e9, 1),
-                 "frac": round(per_it * it / t / 1e9 / peak[0], 3)}
+        mv = per_it - 2 * (nnz0 * (w + 4) + 4 * n0) - 4 * n0 * w
+        moved = {"bytes_per_krylov_iter": int(mv), "achieved": round(mv * it / t / 1e9, 1),
+                 "frac": round(mv * it / t / 1e9 / peak[0], 3)}
+    ncu = NCU_P_ITER_DRAM_BYTES_128.get(pc) if (n == 128 ** 3 and info["team"] == 3 and not mixed) else None
     return {"bound": "hbm", "kernel": kern, "unit_of_work": "one p' solve (Krylov iterations x bytes/iteration)",
             "achieved": round(ach, 1), "peak": peak[0], "unit": "GB/s", "frac": round(ach / peak[0], 3),
-            "moved": moved,
-            "peak_source": peak[1],
-            "traffic": (int(NCU_P_ITER_DRAM_BYTES_128 * int(s.s_p.iters[0]))
-                        if (n == 128 ** 3 and info["team"] == 3) else None),
-            "traffic_source": "ncu capture of one Krylov iteration (9 kernels) x Krylov count" if n == 128 ** 3
-            else None, "launch_ms": round(t * 1e3, 3),
-            "krylov_iters": int(s.s_p.iters[0]), "bytes_per_krylov_iter": int(solver_bytes(n, nnz, 1, "ilu0", w)),
-            "spmv": spmv}
+            "moved": moved, "peak_source": peak[1],
+            "traffic": int(ncu * it) if ncu else None,
+            "traffic_source": "ncu launch list of one solve (DRAM bytes per Krylov iteration) x Krylov count"
+            if ncu else None,
+            "launch_ms": round(t * 1e3, 3), "setup_ms": round(float(np.mean(setups)) * 1e3, 3),
+            "krylov_iters": it, "bytes_per_krylov_iter": int(per_it),
+            "hierarchy": amg, "spmv": spmv}
 
 
 def timed_iterations(s, steps):
@@ -274,6 +352,54 @@ def timed_iterations(s, steps):
     return e0.elapsed_time(e1) / 1e3, [(int(a), int(b)) for a, b in its]
 
 
+def fields_of(s):
+    return {"u": s.U.values[:, 0], "v": s.U.values[:, 1], "w": s.U.values[:, 2], "p": s.p.values,
+            "pp": s.pp_t.detach().cpu().numpy().copy()}
+
+
+def field_errors(ref, test):
+    """Relative L2 error of each field of `test` against `ref`."""
+    return {k: float(np.linalg.norm(test[k] - ref[k]) / max(np.linalg.norm(ref[k]), 1e-300)) for k in ref}
+
+
+def start_cpu_sample(N):
+    """The CPU baseline in a separate host process (it runs beside the GPU legs that
+    follow the timed region): one full outer iteration of the same workload by the
+    oracle. BLAS threads capped at 8 so it cannot crowd the launching thread."""
+    env = dict(os.environ, OMP_NUM_THREADS="8", OPENBLAS_NUM_THREADS="8", MKL_NUM_THREADS="8")
+    return subprocess.Popen([sys.executable, os.path.abspath(__file__), "--impl", "cpu-sample", "--size", str(N)],
+                            stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True, env=env)
+
+
+def collect_cpu_sample(proc, timeout_s=900.0):
+    if proc is None:
+        return None
+    try:
+        out, _ = proc.communicate(timeout=timeout_s)
+    except subprocess.TimeoutExpired:
+        proc.kill()
+        proc.communicate()
+        return {"unavailable": f"the host oracle did not finish within {timeout_s:.0f} s"}
+    lines = [ln for ln in out.splitlines() if ln.startswith("{")]
+    if proc.returncode != 0 or not lines:
+        return {"unavailable": f"the host oracle exited with {proc.returncode}"}
+    r = json.loads(lines[-1])
+    return cpu_baseline_entry(r)
+
+
+def cpu_baseline_entry(r):
+    t = float(np.mean([x["s"] for x in r["steps"]]))
+    kry = [x["p_krylov"] for x in r["steps"]]
+    return {"value": round(1.0 / t, 6), "unit": UNIT, "cores": 1, "kind": "port",
+            "host_cores_available": r["host_cores"],
+            "sample": f"the oracle (numpy/scipy restatement of the reference path: BiCGSTAB + Jacobi for u, v, w, "
+                      f"BiCGSTAB + ILU(0) in the device's red-black order for p', rtol 1e-8, MUSCL van Leer, "
+                      f"non-orthogonal correction) on the full {r['N']}^3 workload: {len(r['steps'])} whole outer "
+                      f"iteration(s) from the initial state, {t:.1f} s each (p' Krylov counts {kry}); mesh build "
+                      f"{r['build_s']:.0f} s and colouring not timed; single-threaded sparse kernels",
+            "seconds_per_step": [round(x["s"], 2) for x in r["steps"]], "p_krylov": kry}
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -282,21 +408,22 @@ def run_ours(args):
     local = int(os.environ.get("LOCAL_RANK", "0"))
     if world > 1:
         torch.cuda.set_device(local)
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=600))
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=900))
     dev = torch.cuda.current_device()
     N = args.size
     t_setup = time.time()
-    s = make_solver(N, precision="fp64", graph=True)
+    s = make_solver(N, precision="fp64", graph=True, p_precond=args.p_precond)
     setup_s = time.time() - t_setup
-    n_faces, nnz = int(s.mesh.n_faces), int(s.mesh.nnz)
+    mesh = s.mesh
+    n_faces, nnz = int(mesh.n_faces), int(mesh.nnz)
     s.reset_history()
     s.iterate(args.warmup)
     torch.cuda.synchronize()
     # the state the timed region starts from (U, p: everything else is rebuilt from
     # them each outer iteration); the e2e leg replays the same steps from it
     D = 3
-    Uh = torch.empty(s.mesh.n_cells, D, dtype=torch.float64).pin_memory()
-    ph = torch.empty(s.mesh.n_cells, dtype=torch.float64).pin_memory()
+    Uh = torch.empty(mesh.n_cells, D, dtype=torch.float64).pin_memory()
+    ph = torch.empty(mesh.n_cells, dtype=torch.float64).pin_memory()
     Uh.copy_(s.U_t.cpu())
     ph.copy_(s.p_t.cpu())
     if world > 1:
@@ -311,6 +438,7 @@ def run_ours(args):
         t = float(tt.item())
     clocks = cs.summary()
     value = world * args.steps / t
+    fields64 = fields_of(s)
     stats = s.solver_stats()
     launches = sum(launches_per_step(s, a, b) for a, b in its)
     res_hist = s.hist[: args.warmup + args.steps].cpu().numpy()
@@ -334,66 +462,92 @@ def run_ours(args):
         tt = torch.tensor([te], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         te = float(tt.item())
-    e2e = {"value": round(world * ke / te, 3), "unit": UNIT, "h2d_bytes_per_step": int(s.mesh.n_cells * (D + 1) * 8),
-           "d2h_bytes_per_step": int(s.mesh.n_cells * (D + 1) * 8), "steps": ke}
+    e2e = {"value": round(world * ke / te, 3), "unit": UNIT, "h2d_bytes_per_step": int(mesh.n_cells * (D + 1) * 8),
+           "d2h_bytes_per_step": int(mesh.n_cells * (D + 1) * 8), "steps": ke}
+    cpu_proc = start_cpu_sample(N) if (rank == 0 and world == 1 and not args.no_cpu) else None
     roof = p_solve_roofline(s, measured_peak()) if rank == 0 else None
     if roof is not None:
         # the whole outer iteration against the same peak
-        Fi = int(s.mesh.n_internal_faces)
-        ob = sum(outer_step_bytes(s.mesh.n_cells, Fi, n_faces - Fi, nnz, 3, a, b) for a, b in its)
+        Fi = int(mesh.n_internal_faces)
+        amg = roof["hierarchy"]
+        ob = sum(outer_step_bytes(mesh.n_cells, Fi, n_faces - Fi, nnz, 3, a, b, args.p_precond, amg) for a, b in its)
         roof["outer_iteration"] = {"bytes_per_step": int(ob / len(its)), "achieved": round(ob / t / 1e9, 1),
                                    "frac": round(ob / t / 1e9 / roof["peak"], 3),
                                    "note": "formula bytes of all assembly, gradient, mass-flux and solve work of "
-                                           "the timed steps (their Krylov counts) / the timed region"}
-        if roof.get("moved"):
-            # less the level-0 rows the engine's SpMV phases do not multiply
-            skip = roof["bytes_per_krylov_iter"] - roof["moved"]["bytes_per_krylov_iter"]
-            om = ob - skip * sum(b for _, b in its)
-            roof["outer_iteration"]["moved"] = {"bytes_per_step": int(om / len(its)),
-                                                "achieved": round(om / t / 1e9, 1),
-                                                "frac": round(om / t / 1e9 / roof["peak"], 3)}
-    # the mixed-precision form (FP32 inner Krylov on the persistent kernel, FP64
-    # refinement) on the same mesh, for comparison
-    alt = None
+                                           "the timed steps (their Krylov counts; preconditioner set-up not "
+                                           "counted) / the timed region"}
+    del s
+    torch.cuda.empty_cache()
+    variants = {}
     if args.plain and rank == 0:
-        del s
-        torch.cuda.empty_cache()
-        sm = make_solver(N, precision="mixed", graph=True)
-        sm.iterate(max(1, args.warmup))
+        # the mixed form on the same mesh, the same number of outer iterations from the
+        # same initial state: rate and each field's error against the FP64 fields
+        sm = make_solver(N, precision="mixed", graph=True, p_precond=args.p_precond, mesh=mesh)
+        sm.iterate(args.warmup)
         torch.cuda.synchronize()
-        k = max(2, min(args.steps, 5))
-        tm, _ = timed_iterations(sm, k)
-        alt = {"value": round(k / tm, 3), "unit": UNIT, "steps": k,
-               "desc": "same workload, mixed precision (FP32 inner Krylov on the persistent grid kernel, "
-                       "FP64 residual/refinement), outer iteration captured as a CUDA graph"}
+        tm, its_m = timed_iterations(sm, args.steps)
+        variants["mixed_precision_variant"] = {
+            "value": round(args.steps / tm, 3), "unit": UNIT, "steps": args.steps, "krylov_iters_per_step": its_m,
+            "field_error": field_errors(fields64, fields_of(sm)),
+            "desc": "same workload, mixed form: momentum BiCGSTAB + Jacobi with FP32 inner iterations and FP64 "
+                    "refinement; p' multigrid hierarchy and V-cycles stored in FP32 (FP64 arithmetic) under an "
+                    "FP64 Krylov iteration; field_error = relative L2 against the FP64 run after the same "
+                    f"{args.warmup + args.steps} outer iterations (u, v, w, p, and p' of the last iteration)"}
         del sm
         torch.cuda.empty_cache()
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_baseline(N, its_p=roof["krylov_iters"] if roof else None)
+        if args.p_precond != "ilu0":
+            si = make_solver(N, precision="fp64", graph=True, p_precond="ilu0", mesh=mesh)
+            si.iterate(args.warmup)
+            torch.cuda.synchronize()
+            k = args.steps
+            ti, its_i = timed_iterations(si, k)
+            variants["ilu0_variant"] = {
+                "value": round(k / ti, 3), "unit": UNIT, "steps": k, "krylov_iters_per_step": its_i,
+                "field_error_vs_main": field_errors(fields64, fields_of(si)),
+                "desc": "same workload with the config's named p' preconditioner: BiCGSTAB + ILU(0) (red-black "
+                        "levels) on the graph engine, FP64; field_error_vs_main: two FP64 runs whose p' solves "
+                        "stop at the same 1e-8 residual with different preconditioners, the noise floor of the "
+                        "field errors at this tolerance"}
+            del si
+            torch.cuda.empty_cache()
+    legs = {}
+    if rank == 0 and world == 1 and args.legs:
+        if "c4" in args.legs:
+            legs["batched_c4"] = c4_measure(count=args.leg_systems, steps=1, warmup=1, mode="fp64", plain=True,
+                                            plain_budget_s=20.0, cpu=False)
+        if "c5" in args.legs:
+            legs["served_c5"] = c5_measure(requests=args.leg_requests, rate=args.rate, cont_tol=args.cont_tol,
+                                           max_iters=args.max_iters, max_active=args.max_active,
+                                           policy=args.policy, serial=True)
+    cpu = collect_cpu_sample(cpu_proc)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
+        pname = {"amg": "smoothed-aggregation multigrid", "ilu0": "ILU(0) red-black"}.get(args.p_precond,
+                                                                                           args.p_precond)
         line = {
             "metric": METRIC, "value": round(value, 4), "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": f"3D jittered lid-driven cavity {N}^3 hex ({N**3} cells), Re 400, MUSCL van Leer, "
-                                   "over-relaxed non-orthogonal, ILU(0) p' / Jacobi u,v,w, rtol 1e-8, FP64, "
-                                   "graph-engine solves",
-                       "cells": N ** 3, "faces": n_faces, "nnz": nnz,
+                                   f"over-relaxed non-orthogonal, BiCGSTAB + {pname} p' / Jacobi u,v,w, rtol 1e-8, "
+                                   "FP64, graph-engine solves",
+                       "cells": N ** 3, "faces": n_faces, "nnz": nnz, "p_precond": args.p_precond,
                        "parallelism": f"replicas x{world}" if world > 1 else "1 GPU",
                        "l2": "working set >> 126 MB L2; no flush needed", "setup_s": round(setup_s, 2)},
-            "clocks": clocks, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "mixed_precision_variant": alt,
+            "clocks": clocks, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu,
             "gpu_launches": launches, "krylov_iters_per_step": its,
             "solver_stats_last_step": stats,
             "residual_first_last": [float(res_hist[0]), float(res_hist[-1])],
         }
+        line.update(variants)
+        line.update(legs)
         print(json.dumps(line))
 
 
 C4_METRIC = "p' systems solved/s (1,024 Delaunay systems, 1e-8 relative residual each)"
+C4_TOTAL = 1024
 
 
 def _c4_bytes(n, nnz, iters, mixed):
@@ -408,45 +562,40 @@ def _c4_bytes(n, nnz, iters, mixed):
     return b
 
 
-def run_c4(args):
-    """C4: 1,024 pressure-correction systems on Delaunay triangle meshes (cell counts
-    log-uniform in [2e3, 2e5], seed 0) solved together: FP64 BiCGSTAB + Jacobi to
-    1e-8 per system, one persistent launch per size tier (--c4-mode mixed: FP32 inner
-    iterations with FP64 refinement, which does not converge on most of these
-    systems). Multi-GPU: systems are spread over ranks by LPT on nnz, no data-path
-    collective."""
+def c4_measure(count=C4_TOTAL, steps=1, warmup=1, mode="fp64", plain=True, plain_budget_s=60.0, cpu=True,
+               restarts=20, world=1, rank=0):
+    """The first `count` of the 1,024 C4 systems (cell counts log-uniform in [2e3, 2e5],
+    seed 0; the same systems whatever the count) solved together: BiCGSTAB + Jacobi to
+    1e-8 per system, one persistent launch per size tier, a system whose rho or omega
+    breaks down restarted (up to `restarts` times). Returns the measurements: batched
+    solves/s over converged systems, e2e with host buffers, the plain FP64 drop-in per
+    system over a bounded prefix, the CPU scipy path over a bounded prefix."""
     import torch
     import torch.distributed as dist
+    from scipy import sparse
     from kcfd.batch import BatchSolver, lpt_shards, p_prime_batch, p_prime_sizes
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
-    if world > 1:
-        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
-        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=900))
-    count = args.systems
-    sizes = p_prime_sizes(count, 2000, 200000, 0)
+    sizes = p_prime_sizes(C4_TOTAL, 2000, 200000, 0)[:count]
     mine = lpt_shards(sizes * 4, world)[rank] if world > 1 else list(range(count))
     workers = max(1, min(os.cpu_count() or 1, 64) // max(world, 1))
     t0 = time.time()
-    if workers > 1:
+    from kcfd.batch import _p_prime_host
+    if workers > 1 and len(mine) > 1:
         import multiprocessing as mp
         from concurrent.futures import ProcessPoolExecutor
-        from kcfd.batch import _p_prime_host
         with ProcessPoolExecutor(max_workers=workers, mp_context=mp.get_context("spawn")) as ex:
-            host = list(ex.map(_p_prime_host, mine, [sizes[k] for k in mine], [0] * len(mine), chunksize=4))
+            host = list(ex.map(_p_prime_host, mine, [sizes[k] for k in mine], [0] * len(mine), chunksize=2))
     else:
-        from kcfd.batch import _p_prime_host
         host = [_p_prime_host(k, sizes[k], 0) for k in mine]
     gen_s = time.time() - t0
     pats, vals, rhs, _ = p_prime_batch(len(mine), host=host)
     n_sys = np.array([len(ip) - 1 for ip, _ in pats])
     nnz_sys = np.array([len(ix) for _, ix in pats])
-    mixed = args.c4_mode == "mixed"
-    bs = BatchSolver(pats, mode=args.c4_mode, precond="jacobi", rtol=1e-8, maxiter=20000)
+    mixed = mode == "mixed"
+    bs = BatchSolver(pats, mode=mode, precond="jacobi", rtol=1e-8, maxiter=20000, restarts=restarts)
     v = torch.cat(vals)
     b = bs.pack(rhs)
     x = torch.zeros_like(b)
-    for _ in range(args.warmup):
+    for _ in range(warmup):
         x.zero_()
         bs.solve(v, b, x)
     torch.cuda.synchronize()
@@ -456,7 +605,7 @@ def run_c4(args):
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with ClockSampler(dev) as cs:
         e0.record()
-        for _ in range(args.steps):
+        for _ in range(steps):
             x.zero_()
             bs.solve(v, b, x)
         e1.record()
@@ -471,13 +620,14 @@ def run_c4(args):
     st = bs.status.cpu().numpy()
     xs = bs.unpack(x)
     # parity: true FP64 residual of every system (host scipy CSR)
-    from scipy import sparse
-    worst = 0.0
+    true_rel = []
     for k in range(len(mine)):
         A = sparse.csr_matrix((vals[k].cpu().numpy(), pats[k][1], pats[k][0]), shape=(n_sys[k], n_sys[k]))
-        worst = max(worst, float(np.linalg.norm(rhs[k] - A @ xs[k]) / np.linalg.norm(rhs[k])))
+        true_rel.append(float(np.linalg.norm(rhs[k] - A @ xs[k]) / np.linalg.norm(rhs[k])))
+    true_rel = np.asarray(true_rel)
+    ok = (st == 0) & (true_rel <= 1.5e-8)
     byts = sum(_c4_bytes(int(n_sys[k]), int(nnz_sys[k]), int(its[k]), mixed) for k in range(len(mine)))
-    launch = t / args.steps
+    launch = t / steps
     peak = measured_peak()
     tiers = bs.tiers()
     roof = {"bound": "hbm", "kernel": f"batch_cluster_kernel<MIXED={int(mixed)}, JACOBI> (systems of >= 131,072 rows, "
@@ -494,7 +644,7 @@ def run_c4(args):
     xh = torch.empty_like(bh).pin_memory()
     torch.cuda.synchronize()
     te0 = time.perf_counter()
-    for _ in range(args.steps):
+    for _ in range(steps):
         v.copy_(vh, non_blocking=True)
         b.copy_(bh, non_blocking=True)
         x.zero_()
@@ -506,12 +656,19 @@ def run_c4(args):
         tt = torch.tensor([te], device="cuda", dtype=torch.float64)
         dist.all_reduce(tt, op=dist.ReduceOp.MAX)
         te = float(tt.item())
-    e2e = {"value": round(count * args.steps / te, 3), "unit": "solves/s",
+    n_ok = int(ok.sum())
+    if world > 1:
+        nt = torch.tensor([n_ok], device="cuda", dtype=torch.int64)
+        dist.all_reduce(nt)
+        n_ok_all = int(nt.item())
+    else:
+        n_ok_all = n_ok
+    e2e = {"value": round(n_ok_all * steps / te, 3), "unit": "solves/s",
            "h2d_bytes_per_step": int(vh.numel() * 8 + bh.numel() * 8), "d2h_bytes_per_step": int(xh.numel() * 8)}
     # plain FP64 drop-in (solve_linear_system, host CSR in, ndarray out) once per
     # system, over a bounded prefix of this rank's systems (rank 0 only)
-    plain = None
-    if rank == 0 and args.plain:
+    plain_d = None
+    if rank == 0 and plain:
         from kcfd.fvm_operators import FVMSystem
         from kcfd.linear_solver import solve_linear_system
         host_sys = [(sparse.csr_matrix((vals[k].cpu().numpy(), pats[k][1], pats[k][0]),
@@ -524,16 +681,18 @@ def run_c4(args):
         for A, r in host_sys:
             solve_linear_system(FVMSystem.from_csr(A, r), None, "bicgstab", 0.0, 20000, "b200", "jacobi", rtol=1e-8)
             done += 1
-            if time.perf_counter() - tp0 > 60.0:
+            if time.perf_counter() - tp0 > plain_budget_s:
                 break
         tp = time.perf_counter() - tp0
         frac = float(nnz_sys[:done].sum() / nnz_sys.sum())
-        plain = {"value": round(done / tp, 3), "unit": "solves/s", "systems_timed": done,
-                 "desc": "plain FP64 drop-in: kcfd solve_linear_system(backend='b200', bicgstab + jacobi, "
-                         "rtol 1e-8) per system, host CSR in / ndarray out",
-                 "all_systems_s_estimate": round(tp / max(frac, 1e-12), 2)}
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
+        plain_d = {"value": round(len(mine) * frac / tp, 3) if done < len(mine) else round(done / tp, 3),
+                   "unit": "solves/s", "systems_timed": done, "seconds": round(tp, 2),
+                   "desc": "plain FP64 drop-in: kcfd solve_linear_system(backend='b200', bicgstab + jacobi, "
+                           "rtol 1e-8) once per system, host CSR in / ndarray out"
+                           + ("" if done == len(mine) else "; the timed prefix's rate weighted by its share of "
+                              "the entries")}
+    cpu_d = None
+    if rank == 0 and world == 1 and cpu:
         import scipy.sparse.linalg as spla
         tc0 = time.perf_counter()
         done = 0
@@ -548,87 +707,120 @@ def run_c4(args):
                 break
         tc = time.perf_counter() - tc0
         frac = float(nnz_sys[:done].sum() / nnz_sys.sum())
-        cpu = {"value": round(count / (tc / frac), 4), "unit": "solves/s", "cores": 1, "kind": "port",
-               "sample": f"scipy bicgstab + Jacobi (the reference's create_preconditioner 'jacobi' path) on the "
-                         f"first {done} systems ({tc:.1f} s, {100 * frac:.1f}% of the nnz), scaled by nnz to all "
-                         f"{count}"}
+        cpu_d = {"value": round(len(mine) / (tc / frac), 4), "unit": "solves/s", "cores": 1, "kind": "port",
+                 "sample": f"scipy bicgstab + Jacobi (the reference's create_preconditioner 'jacobi' path) on the "
+                           f"first {done} systems ({tc:.1f} s, {100 * frac:.1f}% of the entries), weighted by "
+                           f"entries to all {len(mine)}"}
+    value = n_ok_all * steps / t
+    return {"value": round(value, 3), "unit": "solves/s", "systems": int(count), "steps": steps, "warmup": warmup,
+            "ms_per_step": round(1e3 * t / steps, 3), "mixed": mixed, "clocks": clocks, "e2e": e2e,
+            "roofline": roof, "plain_fp64_dropin": plain_d, "cpu_baseline": cpu_d,
+            "batched_over_plain": round(value / plain_d["value"], 2) if plain_d else None,
+            "gpu_launches": (1 + sum(1 for k in ("cluster", "big", "small") if tiers[k] > 0)) * steps,
+            "tiers": tiers, "status_ok": int((st == 0).sum()), "breakdown": int((st == 2).sum()),
+            "converged": n_ok, "restarts_allowed": restarts, "max_true_relres": float(true_rel.max()),
+            "krylov_iters": {"min": int(its.min()), "median": int(np.median(its)), "max": int(its.max())},
+            "cells_this_rank": int(n_sys.sum()), "nnz_this_rank": int(nnz_sys.sum()),
+            "generation_s": round(gen_s, 1),
+            "desc": f"the first {count} of the 1,024 p' systems on Delaunay triangle meshes (n log-uniform in "
+                    "[2e3, 2e5], seed 0), diffusion (harmonic, Gamma log-uniform [0.1, 10]) + one Dirichlet side, "
+                    "RHS N(0,1); batched " + ("FP32 BiCGSTAB + Jacobi with FP64 refinement" if mixed else
+                                              "FP64 BiCGSTAB + Jacobi") +
+                    f", rtol 1e-8, breakdown restarts <= {restarts}, one persistent launch per size tier; value "
+                    "counts converged systems only"}
+
+
+def run_c4(args):
+    """C4: 1,024 pressure-correction systems on Delaunay triangle meshes solved
+    together (c4_measure). Multi-GPU: systems are spread over ranks by LPT on nnz, no
+    data-path collective."""
+    import torch
+    import torch.distributed as dist
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    if world > 1:
+        torch.cuda.set_device(int(os.environ.get("LOCAL_RANK", "0")))
+        dist.init_process_group("nccl", init_method="env://", timeout=__import__("datetime").timedelta(seconds=900))
+    r = c4_measure(count=args.systems, steps=args.steps, warmup=args.warmup, mode=args.c4_mode, plain=bool(args.plain),
+                   cpu=not args.no_cpu, world=world, rank=rank)
     if world > 1:
         dist.barrier()
         dist.destroy_process_group()
     if rank == 0:
-        line = {
-            "metric": C4_METRIC, "value": round(count * args.steps / t, 3), "unit": "solves/s",
-            "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": round(1e3 * t / args.steps, 3), "higher_is_better": True,
-            "scaling": "strong", "vs_baseline": None,
-            "dtype": "fp32-inner/fp64-refine" if mixed else "f64", "data": "synthetic",
-            "config": {"workload": f"{count} p' systems on Delaunay triangle meshes, n log-uniform in [2e3, 2e5] "
-                                   "(seed 0), diffusion (harmonic, Gamma log-uniform [0.1, 10]) + one Dirichlet "
-                                   "side (x = 0, sqrt(n/2) faces), RHS N(0,1); batched "
-                                   + ("FP32 BiCGSTAB + Jacobi with FP64 refinement" if mixed else
-                                      "FP64 BiCGSTAB + Jacobi") + ", rtol 1e-8, one persistent launch per size tier",
-                       "cells_this_rank": int(n_sys.sum()), "nnz_this_rank": int(nnz_sys.sum()),
-                       "parallelism": f"LPT shards x{world}" if world > 1 else "1 GPU",
-                       "l2": "working set >> 126 MB L2; no flush needed", "generation_s": round(gen_s, 1)},
-            "clocks": clocks, "e2e": e2e, "roofline": roof, "cpu_baseline": cpu, "plain_fp64_dropin": plain,
-            "gpu_launches": (1 + sum(1 for k in ("cluster", "big", "small") if tiers[k] > 0)) * args.steps,
-            "tiers": tiers,
-            "status_ok": int((st == 0).sum()), "max_true_relres": worst,
-            "krylov_iters": {"min": int(its.min()), "median": int(np.median(its)), "max": int(its.max())},
-        }
+        line = {"metric": C4_METRIC, "value": r["value"], "unit": "solves/s", "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": r["ms_per_step"], "higher_is_better": True,
+                "scaling": "strong", "vs_baseline": None,
+                "dtype": "fp32-inner/fp64-refine" if r["mixed"] else "f64", "data": "synthetic",
+                "config": {"workload": r["desc"], "cells_this_rank": r["cells_this_rank"],
+                           "nnz_this_rank": r["nnz_this_rank"],
+                           "parallelism": f"LPT shards x{world}" if world > 1 else "1 GPU",
+                           "l2": "working set >> 126 MB L2; no flush needed", "generation_s": r["generation_s"]}}
+        for k in ("clocks", "e2e", "roofline", "cpu_baseline", "plain_fp64_dropin", "batched_over_plain",
+                  "gpu_launches", "tiers", "status_ok", "breakdown", "converged", "restarts_allowed",
+                  "max_true_relres", "krylov_iters"):
+            line[k] = r[k]
         print(json.dumps(line))
 
 
 C5_METRIC = "served SIMPLE cavities/s (Poisson arrivals, continuous batching)"
 
 
-def run_c5(args):
-    """C5: Poisson-arriving cavity requests (half 2D N^2, N in [32, 512]; half 3D N^3,
-    N in [16, 96]; Re in [100, 1000]; seed 0) served by the continuous-batching loop
-    (kcfd.serve.Server: HBM-budget admission, one stream and graph per case), each
-    run to a continuity residual ||b_p'|| / ||b_p'(first)|| below --cont-tol. The
-    comparator serves the same requests one case at a time."""
+def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active=4, policy="sjf", serial=True):
+    """Poisson-arriving cavity requests (half 2D N^2, N in [32, 512]; half 3D N^3, N in
+    [16, 96]; Re in [100, 1000]; seed 0) served by the continuous-batching loop
+    (kcfd.serve.Server: HBM-budget admission, one stream and graph per case), each run
+    to a continuity residual ||b_p'|| / ||b_p'(first)|| below cont_tol; the comparator
+    serves the same requests one case at a time."""
     import torch
-    from kcfd.serve import Server, make_requests, summarize
-    reqs = make_requests(args.requests, args.rate, seed=0)
-    common = dict(budget_bytes=150e9, iters_per_tick=10, max_iters=args.max_iters, cont_tol=args.cont_tol,
+    from kcfd.serve import Request, Server, make_requests, summarize
+    reqs = make_requests(requests, rate, seed=0)
+    common = dict(budget_bytes=150e9, iters_per_tick=10, max_iters=max_iters, cont_tol=cont_tol,
                   precision="fp64", graph=True, precond_p="ilu0", keep_fields=True)
     # warm-up: one small case of each dimension (kernel loading, allocator)
-    from kcfd.serve import Request
     Server(**common).run([Request(0, 2, 32, 400.0, 0.0), Request(1, 3, 16, 400.0, 0.0)])
     torch.cuda.synchronize()
     dev = torch.cuda.current_device()
     with ClockSampler(dev) as cs:
-        res = Server(max_active=args.max_active, policy=args.policy, builders=2, **common).run(reqs)
+        res = Server(max_active=max_active, policy=policy, builders=2, **common).run(reqs)
     clocks = cs.summary()
     ours = summarize(res)
     d2h = int(sum(r.cells * (r.ndim + 1) * 8 for r in res))
-    serial = None
-    if args.plain:
+    serial_d = None
+    if serial:
         sres = Server(max_active=1, policy="fifo", **common).run(reqs, serial=True)
-        serial = summarize(sres)
+        serial_d = summarize(sres)
         # the serial run takes the library's single-case solvers (the grid kernel for
         # small cases), the served run one CTA per small case: same algorithm, other
         # reduction partition, so the fields agree to the solver tolerance
         diffs = [float(np.linalg.norm(a.fields["U"] - b.fields["U"]) / max(np.linalg.norm(b.fields["U"]), 1e-300))
                  for a, b in zip(sorted(res, key=lambda r: r.rid), sorted(sres, key=lambda r: r.rid))]
-        serial["max_rel_l2_U_vs_batched"] = max(diffs)
+        serial_d["max_rel_l2_U_vs_batched"] = max(diffs)
+    return {"value": round(ours["cases_per_s"], 3), "unit": "cases/s", "requests": len(reqs), "rate": rate,
+            "clocks": clocks, "p50_ms": round(ours["p50_ms"], 1), "p99_ms": round(ours["p99_ms"], 1),
+            "converged": ours["converged"], "mean_iterations": ours["mean_iterations"],
+            "d2h_bytes_per_case": int(d2h / max(len(res), 1)), "serial_comparator": serial_d,
+            "served_over_serial": round(ours["cases_per_s"] / serial_d["cases_per_s"], 2) if serial_d else None,
+            "desc": f"{len(reqs)} cavity requests at {rate} req/s (Poisson, seed 0): 2D N^2 N~U{{32..512}}, 3D N^3 "
+                    f"N~U{{16..96}}, Re~U(100,1000); each to continuity {cont_tol:g} (max {max_iters} outer "
+                    f"iterations); FP64, ILU(0) p', HBM budget 150 GB; continuous batching (max {max_active} "
+                    f"resident, {policy} admission, cases built on 2 host threads)"}
+
+
+def run_c5(args):
+    r = c5_measure(args.requests, args.rate, args.cont_tol, args.max_iters, args.max_active, args.policy,
+                   bool(args.plain))
     line = {
-        "metric": C5_METRIC, "value": round(ours["cases_per_s"], 3), "unit": "cases/s", "n_gpus": 1,
-        "steps": len(reqs), "warmup": 2, "ms_per_step": round(1e3 / max(ours["cases_per_s"], 1e-9), 1),
+        "metric": C5_METRIC, "value": r["value"], "unit": "cases/s", "n_gpus": 1,
+        "steps": r["requests"], "warmup": 2, "ms_per_step": round(1e3 / max(r["value"], 1e-9), 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-        "config": {"workload": f"{len(reqs)} cavity requests at {args.rate} req/s (Poisson, seed 0): 2D N^2 "
-                               "N~U{32..512}, 3D N^3 N~U{16..96}, Re~U(100,1000); each to continuity "
-                               f"{args.cont_tol:g} (max {args.max_iters} outer iterations); FP64, ILU(0) p', "
-                               "HBM budget 150 GB",
-                   "parallelism": f"1 GPU, continuous batching (max {args.max_active} resident, {args.policy} "
-                                  "admission, cases built on 2 host threads)"},
-        "clocks": clocks, "p50_ms": round(ours["p50_ms"], 1), "p99_ms": round(ours["p99_ms"], 1),
-        "converged": ours["converged"], "mean_iterations": ours["mean_iterations"],
-        "e2e": {"value": round(ours["cases_per_s"], 3), "unit": "cases/s", "h2d_bytes_per_step": None,
-                "d2h_bytes_per_step": int(d2h / max(len(res), 1)),
+        "config": {"workload": r["desc"], "parallelism": "1 GPU, continuous batching"},
+        "clocks": r["clocks"], "p50_ms": r["p50_ms"], "p99_ms": r["p99_ms"],
+        "converged": r["converged"], "mean_iterations": r["mean_iterations"],
+        "e2e": {"value": r["value"], "unit": "cases/s", "h2d_bytes_per_step": None,
+                "d2h_bytes_per_step": r["d2h_bytes_per_case"],
                 "note": "the served loop is end to end already: host mesh arrays in, fields out per case"},
-        "serial_comparator": serial, "roofline": None, "cpu_baseline": None,
+        "serial_comparator": r["serial_comparator"], "served_over_serial": r["served_over_serial"],
+        "roofline": None, "cpu_baseline": None,
     }
     print(json.dumps(line))
 
@@ -879,73 +1071,77 @@ def run_c3(args):
     print(json.dumps(line))
 
 
+
+
 def oracle_cavity(N):
+    """The oracle on the same workload: BiCGSTAB + Jacobi for u, v, w and BiCGSTAB +
+    structural ILU(0) in the greedy (red-black) cell colouring for p' -- the device's
+    ILU(0) ordering; the reference's own 'ilu0' (SuperLU spilu, COLAMD) needs about
+    twice the Krylov iterations on these systems -- each to rtol 1e-8."""
     from oracle import mesh as om, simple as osim
     nodes, cells, cf, bd = cavity_arrays(N)
     m = om.build_3d(nodes, cells, cf, bd)
     o = osim.Simple(m, rho=1.0, mu=0.0025)
     osim.cavity_setup(o)
     o.muscl, o.nonorth = "van_leer", True
-    o.solver, o.rtol, o.precond_u, o.precond_p = "bicgstab", 1e-8, "jacobi", "spilu"
+    o.solver, o.rtol, o.precond_u, o.precond_p = "bicgstab", 1e-8, "jacobi", "ilu0"
     o.alpha_u, o.alpha_p = 0.7, 0.3
     return o
 
 
-def cpu_sample_scale(N_full, n_sample_iters_p=None, its_p_full=None):
-    ns, nf = CPU_SAMPLE_N ** 3, N_full ** 3
-    # Krylov iterations of ILU-preconditioned Poisson grow ~linearly with N
-    its_scale = (its_p_full / n_sample_iters_p) if (its_p_full and n_sample_iters_p) else N_full / CPU_SAMPLE_N
-    return nf / ns, its_scale
-
-
-def cpu_baseline(N_full, its_p=None, iters=1):
-    """The oracle (numpy/scipy restatement of the reference path: bicgstab + Jacobi
-    for u,v,w, scipy spilu -- the reference's 'ilu0' -- for p') on the same workload at
-    40^3, one outer iteration after one warm-up, scaled to N_full^3 by cell count
-    and by the growth of the p' Krylov count."""
-    import threadpoolctl  # noqa: F401
-    o = oracle_cavity(CPU_SAMPLE_N)
-    o.iterate()
-    t0 = time.perf_counter()
-    for _ in range(iters):
+def cpu_outer_iterations(N, max_steps, budget_s):
+    """Whole outer iterations of the N^3 workload by the oracle from the initial state,
+    timed one by one; stops after max_steps or when another step would take the timed
+    work past budget_s (at least one step). The mesh build and the ILU(0) colouring
+    (pattern only) are set-up, not timed; an 8^3 copy runs one iteration first."""
+    from oracle import linsolve, mesh as om
+    w = oracle_cavity(8)
+    w.iterate()
+    t0 = time.time()
+    o = oracle_cavity(N)
+    ip, ix = om.csr_pattern(o.mesh)
+    from scipy import sparse
+    o._colour = linsolve.greedy_colouring(sparse.csr_matrix((np.ones(len(ix)), ix, ip), shape=(len(ip) - 1,) * 2))
+    build_s = time.time() - t0
+    steps = []
+    while len(steps) < max_steps:
+        ts = time.perf_counter()
         o.iterate()
-    t = (time.perf_counter() - t0) / iters
-    its_sample = [v for k, v in o.iters_log if k == "p"][-1]
-    cell_scale, its_scale = cpu_sample_scale(N_full, its_sample, its_p)
-    # assembly + momentum scale with cells; the p' solve additionally with its count
-    t_full = t * cell_scale * (0.3 + 0.7 * its_scale)
-    return {"value": round(1.0 / t_full, 6), "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"1 SIMPLE outer iteration of the same workload at {CPU_SAMPLE_N}^3 "
-                      f"({CPU_SAMPLE_N**3} cells): {t:.2f} s; scaled x{cell_scale:.1f} (cells) and the p' "
-                      f"share (0.7) x{its_scale:.2f} (Krylov count) to {N_full}^3",
-            "sample_s": round(t, 3)}
+        dt = time.perf_counter() - ts
+        log = dict(o.iters_log[-4:])
+        steps.append({"s": dt, "p_krylov": int(log.get("p", 0)), "mom_krylov": [int(log.get(f"u{c}", 0)) for c in range(3)]})
+        if sum(x["s"] for x in steps) + dt > budget_s:
+            break
+    return {"N": N, "build_s": build_s, "steps": steps, "host_cores": os.cpu_count(),
+            "colours": int(o._colour.max()) + 1}
+
+
+def run_cpu_sample(args):
+    print(json.dumps(cpu_outer_iterations(args.size, max_steps=1, budget_s=0.0)))
 
 
 def run_reference(args):
+    """The reference's path on the host cores: the oracle on the full workload, whole
+    outer iterations (as many of the requested steps as fit REF_BUDGET_S of timed
+    work, at least one), measured one by one; nothing is scaled."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
     N = args.size
-    o = oracle_cavity(CPU_SAMPLE_N)
-    for _ in range(args.warmup):
-        o.iterate()
-    t0 = time.perf_counter()
-    for _ in range(args.steps):
-        o.iterate()
-    t = (time.perf_counter() - t0) / args.steps
-    its_sample = [v for k, v in o.iters_log if k == "p"][-1]
-    cell_scale, its_scale = cpu_sample_scale(N, its_sample, None)
-    t_full = t * cell_scale * (0.3 + 0.7 * its_scale)
-    v = 1.0 / t_full
-    line = {"impl": "reference", "metric": METRIC, "value": round(v, 6), "unit": UNIT, "n_gpus": 1,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * t_full, 1),
-            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": {"workload": f"3D jittered lid-driven cavity {N}^3 (oracle numpy/scipy on host cores)"},
-            "cpu_baseline": {"value": round(v, 6), "unit": UNIT, "cores": 1, "kind": "port",
-                             "host_cores_available": os.cpu_count(),
-                             "sample": f"per step: 1 outer iteration at {CPU_SAMPLE_N}^3 ({t:.2f} s), scaled "
-                                       f"x{cell_scale:.1f} (cells) and p' share x{its_scale:.2f} (Krylov growth ~N)"},
-            "e2e": {"value": round(v, 6), "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    r = cpu_outer_iterations(N, max_steps=args.steps, budget_s=REF_BUDGET_S)
+    cb = cpu_baseline_entry(r)
+    t = 1.0 / cb["value"]
+    line = {"impl": "reference", "metric": METRIC, "value": cb["value"], "unit": UNIT, "n_gpus": 1,
+            "steps": len(r["steps"]), "steps_requested": args.steps, "warmup": 1,
+            "ms_per_step": round(1e3 * t, 1), "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic",
+            "config": {"workload": f"3D jittered lid-driven cavity {N}^3 hex ({N**3} cells), Re 400, MUSCL van Leer, "
+                                   "over-relaxed non-orthogonal, BiCGSTAB + ILU(0) (red-black) p' / Jacobi u,v,w, "
+                                   "rtol 1e-8, FP64, the oracle (numpy/scipy) on the host cores",
+                       "cells": N ** 3, "warmup_note": "one outer iteration of an 8^3 copy of the workload",
+                       "setup_s": round(r["build_s"], 1), "ilu0_colours": r["colours"]},
+            "cpu_baseline": cb,
+            "e2e": {"value": cb["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
 
 
@@ -954,12 +1150,16 @@ def main():
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
-    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference", "cpu-sample"])
     ap.add_argument("--size", type=int, default=128)
+    ap.add_argument("--p-precond", default="amg", choices=["amg", "ilu0"], help="c2: p' preconditioner")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--config", default="c2", choices=["c1", "c2", "c3", "c4", "c5"],
                     help="c2: 128^3 cavity SIMPLE (default); c3: two-fluid on ~1M tets; c4: 1,024 batched p' "
                          "systems; c5: served cavities")
+    ap.add_argument("--legs", default="c4,c5", help="c2: bounded C4 / C5 legs in the same line ('' for none)")
+    ap.add_argument("--leg-systems", type=int, default=128, help="c2: C4 leg systems (the first of the 1,024)")
+    ap.add_argument("--leg-requests", type=int, default=12, help="c2: C5 leg requests")
     ap.add_argument("--tets", type=int, default=1000000, help="c3: target tetrahedra")
     ap.add_argument("--c1-iters", type=int, default=500, help="c1: outer iterations")
     ap.add_argument("--cpu-tets", type=int, default=6000, help="c3: oracle sample size")
@@ -971,12 +1171,15 @@ def main():
     ap.add_argument("--policy", default="sjf", choices=["sjf", "fifo"], help="c5: admission order")
     ap.add_argument("--systems", type=int, default=1024, help="c4: number of systems")
     ap.add_argument("--c4-mode", default="fp64", choices=["fp64", "mixed"], help="c4: batched solve precision")
-    ap.add_argument("--plain", type=int, default=1, help="also time the mixed-precision form (rank 0)")
+    ap.add_argument("--plain", type=int, default=1, help="also time the variants (rank 0)")
     args = ap.parse_args()
+    args.legs = [x for x in args.legs.split(",") if x]
     if args.warmup < 3:
         args.warmup = 3
     if args.impl == "reference":
         run_reference(args)
+    elif args.impl == "cpu-sample":
+        run_cpu_sample(args)
     elif args.config == "c1":
         run_c1(args)
     elif args.config == "c3":

@@ -322,6 +322,10 @@ typedef struct {
     int32_t cluster_rows;  /* cluster tier threshold: 0 default (131072), < 0 none     */
     int32_t cluster_size;  /* CTAs per cluster team: 0 default (4), 2..8               */
     double  rtol, atol, inner_rtol;
+    int32_t restarts;      /* KCFD_STOP_SCIPY: a system whose rho or omega breaks down
+                              (|.| < eps^2) restarts from its current iterate with
+                              rhat = r, p = r, up to this many times; 0 stops there with
+                              KCFD_BREAKDOWN as scipy does                            */
 } kcfd_batch_opts_t;
 /* indptr_host: per system n[s]+1 local row pointers, concatenated; indices_host:
  * local column indices, concatenated (host arrays, copied to the device).          */

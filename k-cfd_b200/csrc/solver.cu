@@ -80,6 +80,7 @@ struct SolveArgs {
     int maxiter;
     int max_refine;
     int inner_maxiter;
+    int max_restarts;    // KCFD_STOP_SCIPY: restarts on rho / omega breakdown (0: scipy's stop)
     double rtol, atol, inner_rtol;
     int* iters_out;
     double* relres_out;
@@ -280,6 +281,7 @@ template <int NRHS>
 struct KState {
     double rho[NRHS], rho_prev[NRHS], alpha[NRHS], omega[NRHS], beta[NRHS], thr[NRHS], bnorm[NRHS], rnorm[NRHS];
     int done[NRHS], status[NRHS], iters[NRHS], nonfinite[NRHS];
+    int restarts[NRHS], rs[NRHS];  // restarts used; 1 while this iteration restarts
     int active, any_left;
 };
 
@@ -347,6 +349,8 @@ __device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict
                 st.beta[c] = 0.0;
                 st.iters[c] = 0;
                 st.status[c] = KCFD_OK;
+                st.restarts[c] = 0;
+                st.rs[c] = 0;
                 st.nonfinite[c] = !finite(red[c]) || !finite(red[NRHS + c]);
                 if (gpu) {
                     st.thr[c] = rtol;  // relative: ||.|| / ||b|| < tol
@@ -382,11 +386,21 @@ __device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict
                 if (st.done[c]) continue;
                 if (!gpu) {
                     if (st.rnorm[c] < st.thr[c]) { st.done[c] = 1; st.status[c] = KCFD_OK; continue; }
-                    if (fabs(st.rho[c]) < kEps2) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; continue; }
-                    if (it > 0) {
-                        if (fabs(st.omega[c]) < kEps2) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; continue; }
-                        st.beta[c] = (st.rho[c] / st.rho_prev[c]) * (st.alpha[c] / st.omega[c]);
+                    if (fabs(st.rho[c]) < kEps2 || (it > 0 && fabs(st.omega[c]) < kEps2)) {
+                        if (st.restarts[c] < a.max_restarts && st.rnorm[c] > 0.0) {
+                            // restart: rhat = r, p = r (this iteration), rho = ||r||^2
+                            st.restarts[c] += 1;
+                            st.rs[c] = 1;
+                            st.rho[c] = st.rnorm[c] * st.rnorm[c];
+                            st.rho_prev[c] = st.alpha[c] = st.omega[c] = 1.0;
+                            active = 1;
+                            continue;
+                        }
+                        st.done[c] = 1;
+                        st.status[c] = KCFD_BREAKDOWN;
+                        continue;
                     }
+                    if (it > 0) st.beta[c] = (st.rho[c] / st.rho_prev[c]) * (st.alpha[c] / st.omega[c]);
                 } else {
                     if (fabs(st.rho[c]) < 1e-30) { st.done[c] = 1; st.status[c] = KCFD_BREAKDOWN; st.iters[c] = it + 1; continue; }
                     st.beta[c] = (fabs(st.rho_prev[c] * st.omega[c]) > 1e-30)
@@ -428,8 +442,9 @@ __device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict
                         const double om = st.omega[c], be = st.beta[c];
                         V pn;
                         if (gpu) pn = (V)((double)rr[u][c] + be * ((double)pp[u][c] - om * (double)vv[u][c]));
-                        else if (it == 0) pn = rr[u][c];
+                        else if (it == 0 || st.rs[c]) pn = rr[u][c];
                         else pn = (V)(((double)pp[u][c] - om * (double)vv[u][c]) * be + (double)rr[u][c]);
+                        if (st.rs[c]) w.rh[q] = rr[u][c];
                         w.p[q] = pn;
                         if (PREC == KCFD_PREC_JACOBI) w.ph[q] = dd[u] * pn;
                     }
@@ -457,6 +472,7 @@ __device__ bool bicgstab_body(Team& tm, const SolveArgs& a, const VM* __restrict
         if (!tm.template allreduce<NRHS>(red1, 1, smem)) return false;
         if (t0) {
             for (int c = 0; c < NRHS; ++c) {
+                st.rs[c] = 0;
                 if (st.done[c]) continue;
                 if (gpu) {
                     st.alpha[c] = (fabs(red1[c]) > 1e-30) ? st.rho[c] / red1[c] : 0.0;
@@ -945,7 +961,7 @@ struct BatchSys {
 };
 
 struct BatchArgs {
-    int nsys, lanes, mixed, precond, stop, maxiter, max_refine, inner_maxiter;
+    int nsys, lanes, mixed, precond, stop, maxiter, max_refine, inner_maxiter, max_restarts;
     int nq;  // systems in this launch's queue (order[0..nq))
     double rtol, atol, inner_rtol;
     const BatchSys* sys;
@@ -1026,6 +1042,7 @@ __device__ SolveArgs batch_args(const BatchArgs& B, int sid) {
     a.maxiter = B.maxiter;
     a.max_refine = B.max_refine;
     a.inner_maxiter = B.inner_maxiter;
+    a.max_restarts = B.max_restarts;
     a.rtol = B.rtol;
     a.atol = B.atol;
     a.inner_rtol = B.inner_rtol;
@@ -2344,6 +2361,7 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
     KCFD_REQUIRE(opts->precond == KCFD_PREC_NONE || opts->precond == KCFD_PREC_JACOBI,
                  "kcfd_batch_create: precond must be none or jacobi");
     KCFD_REQUIRE(opts->mode == KCFD_MODE_FP64 || opts->mode == KCFD_MODE_MIXED, "kcfd_batch_create: bad mode");
+    KCFD_REQUIRE(opts->restarts >= 0 && opts->restarts <= 1000, "kcfd_batch_create: restarts must be 0..1000");
     KCFD_REQUIRE(opts->stop == KCFD_STOP_SCIPY || (opts->stop == KCFD_STOP_GPU && opts->mode == KCFD_MODE_FP64),
                  "kcfd_batch_create: bad stop rule");
     auto* b = new kcfd_batch();
@@ -2497,6 +2515,7 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
     B.maxiter = b->o.maxiter;
     B.max_refine = b->o.max_refine;
     B.inner_maxiter = b->o.inner_maxiter;
+    B.max_restarts = b->o.restarts;
     B.rtol = b->o.rtol;
     B.atol = b->o.atol;
     B.inner_rtol = b->o.inner_rtol;

@@ -25,6 +25,20 @@ def info_of(h):
     return {"levels": L, "rows": rn[0:2 * L:2].tolist(), "nnz": rn[1:2 * L:2].tolist(), "device_bytes": by.value}
 
 
+def levels_of(h):
+    """Per level: rows, entries and (above the coarsest) prolongator entries."""
+    inf = info_of(h)
+    out = []
+    for l in range(inf["levels"]):
+        d = {"rows": inf["rows"][l], "nnz": inf["nnz"][l], "p_nnz": 0}
+        if l < inf["levels"] - 1:
+            pip = np.zeros(inf["rows"][l] + 1, dtype=np.int32)
+            _lib.check(_lib.lib().kcfd_amg_export(h, l, _lib.AMG_ITEMS["p_indptr"], pip.ctypes.data), "kcfd_amg_export")
+            d["p_nnz"] = int(pip[-1])
+        out.append(d)
+    return out
+
+
 class AMG:
     def __init__(self, csr, mode=_lib.MODE_FP64, coarse_max=0, max_levels=0, power_iters=0):
         _lib.require_cuda()

@@ -24,7 +24,7 @@ class BatchOpts(C.Structure):
     _fields_ = [("precond", C.c_int32), ("stop", C.c_int32), ("mode", C.c_int32), ("maxiter", C.c_int32),
                 ("lanes", C.c_int32), ("max_refine", C.c_int32), ("inner_maxiter", C.c_int32), ("big_rows", C.c_int32),
                 ("cluster_rows", C.c_int32), ("cluster_size", C.c_int32),
-                ("rtol", C.c_double), ("atol", C.c_double), ("inner_rtol", C.c_double)]
+                ("rtol", C.c_double), ("atol", C.c_double), ("inner_rtol", C.c_double), ("restarts", C.c_int32)]
 
 
 class BatchSolver:
@@ -33,11 +33,15 @@ class BatchSolver:
     Tiers by system size: at least cluster_rows rows (0: 131072, negative: none) are
     solved by a thread-block cluster of cluster_size CTAs (0: 4); at least big_rows
     rows (0: 16384, negative: none) by one 512-thread CTA; the rest by one 256-thread
-    CTA. tiers() reports the split."""
+    CTA. tiers() reports the split.
+
+    restarts: with the scipy stopping rule, a system whose rho or omega breaks down
+    restarts from its current iterate (rhat = r, p = r) up to this many times (0: it
+    stops with BREAKDOWN, as scipy's bicgstab does)."""
 
     def __init__(self, patterns, mode="mixed", precond="jacobi", rtol=1e-8, atol=0.0, maxiter=20000, lanes=1,
                  inner_rtol=1e-3, inner_maxiter=400, max_refine=60, stop=_lib.STOP_SCIPY, big_rows=0,
-                 cluster_rows=0, cluster_size=0, device="cuda"):
+                 cluster_rows=0, cluster_size=0, restarts=20, device="cuda"):
         torch = _lib.require_cuda()
         self.nsys = len(patterns)
         self.n = np.array([len(ip) - 1 for ip, _ in patterns], dtype=np.int32)
@@ -54,6 +58,7 @@ class BatchSolver:
         o.rtol, o.atol, o.inner_rtol = float(rtol), float(atol), float(inner_rtol)
         o.big_rows = int(big_rows)
         o.cluster_rows, o.cluster_size = int(cluster_rows), int(cluster_size)
+        o.restarts = int(restarts)
         h = C.c_void_p()
         _lib.check(_lib.lib().kcfd_batch_create(self.nsys, self.n.ctypes.data, self.nnz.ctypes.data, ip.ctypes.data,
                                                 ix.ctypes.data, C.byref(o), C.byref(h)), "kcfd_batch_create")

@@ -153,15 +153,23 @@ class Solver:
                                                         _lib.stream_handle(stream)), "kcfd_solver_apply_precond")
         return z
 
-    def amg_info(self):
-        """Levels, rows and entries per level and device bytes of the multigrid hierarchy
-        (precond 'amg')."""
-        from .amg import info_of
+    def _amg_handle(self):
         h = C.c_void_p()
         _lib.check(_lib.lib().kcfd_solver_amg(self._h, C.byref(h)), "kcfd_solver_amg")
         if not h.value:
             raise ValueError("not an AMG handle")
-        return info_of(h)
+        return h
+
+    def amg_levels(self):
+        """Rows, entries and prolongator entries of every multigrid level (precond 'amg')."""
+        from .amg import levels_of
+        return levels_of(self._amg_handle())
+
+    def amg_info(self):
+        """Levels, rows and entries per level and device bytes of the multigrid hierarchy
+        (precond 'amg')."""
+        from .amg import info_of
+        return info_of(self._amg_handle())
 
     def info(self):
         """Resolved launch shape: dict(team, lanes, block, levels); levels is the ILU

@@ -120,3 +120,30 @@ def test_cluster_tier_same_result_alone_and_in_the_batch(batch):
         x1 = torch.zeros(one.n_total, dtype=torch.float64, device="cuda")
         one.solve(vals[k], one.pack([rhs[k]]), x1)
         np.testing.assert_array_equal(x1.cpu().numpy(), xs[k])
+
+
+def test_breakdown_restart():
+    """Systems drawn like the 1,024-system batch (log-uniform cell counts, Delaunay
+    triangles, seed 0): with restarts every system converges to the true residual; a
+    system that never breaks down takes the same path with or without restarts, so its
+    result is bitwise unchanged."""
+    import torch
+    from kcfd.batch import BatchSolver, p_prime_batch
+    pats, vals, rhs, sizes = p_prime_batch(48, n_min=2000, n_max=20000, seed=0)
+    v = torch.cat(vals)
+    out = {}
+    for restarts in (0, 20):
+        bs = BatchSolver(pats, mode="fp64", precond="jacobi", rtol=1e-8, maxiter=20000, restarts=restarts)
+        b = bs.pack(rhs)
+        x = torch.zeros_like(b)
+        it, rr, st = bs.solve(v, b, x)
+        out[restarts] = (st.cpu().numpy(), bs.unpack(x))
+    st0, x0 = out[0]
+    st1, x1 = out[20]
+    assert (st1 == 0).all(), st1
+    for k in range(len(pats)):
+        A = _csr(pats[k], vals[k])
+        assert np.linalg.norm(rhs[k] - A @ x1[k]) / np.linalg.norm(rhs[k]) < 1.5e-8
+        if st0[k] == 0:
+            np.testing.assert_array_equal(x0[k], x1[k])
+    print(f"breakdowns without restarts: {int((st0 == 2).sum())} of {len(pats)}")

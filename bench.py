@@ -140,7 +140,7 @@ def measured_peak():
 # (KCFD_ENGINE_EAGER=1, every kernel of the solve captured, one pass each), divided
 # by the solve's Krylov count; the roofline's traffic is this times the timed solve's
 # count. Keyed by preconditioner; None where no capture was made.
-NCU_P_ITER_DRAM_BYTES_128 = {"ilu0": 857019136, "amg": None}
+NCU_P_ITER_DRAM_BYTES_128 = {"ilu0": 857019136, "amg": 1902220908}
 
 
 def amg_levels(solver):
@@ -222,7 +222,7 @@ def solve_launches(solver, iters):
     return 5 + body * int(iters)
 
 
-def setup_launches(solver, power_iters=4):
+def setup_launches(solver, power_iters=8):
     """Kernels of one preconditioner set-up: Jacobi 1; ILU(0) permute + factor (+ 2
     SELL fills on the graph engine); AMG per level above the coarsest 9 (level 0) or
     10 + power iterations, and 2 for the coarsest."""

@@ -281,7 +281,7 @@ typedef struct {
                              vectors stored in FP32, arithmetic in FP64            */
     int32_t coarse_max;   /* stop coarsening at or below this many rows (0: 128, <= 256) */
     int32_t max_levels;   /* 0: 12 (at most 16)                                     */
-    int32_t power_iters;  /* power iterations for rho(D^-1 A) below level 0 (0: 4)   */
+    int32_t power_iters;  /* power iterations for rho(D^-1 A) below level 0 (0: 8)   */
 } kcfd_amg_opts_t;
 int  kcfd_amg_create(const kcfd_csr_t* A, const kcfd_amg_opts_t* opts, kcfd_amg** out);
 int  kcfd_amg_setup(kcfd_amg* h, const kcfd_csr_t* A, void* stream);
@@ -579,16 +579,19 @@ int kcfd_tf_copy(int32_t n, int32_t ncopy, const double* src, int32_t src_stride
 
 /* ------------------------------------------- allocation-free solve ---------- */
 /* No counterpart in the reference. For callers that cannot call cudaMalloc --
- * code running during CUDA graph capture, real-time loops that must not block on
- * the allocator, hosts confined to a pre-reserved memory budget -- this solves
+ * real-time loops that must not block on the device allocator, and host programs
+ * whose device memory is owned and pre-reserved by someone else (a framework's
+ * caching allocator, a fixed budget per tenant) -- this solves
  * one system of at most kcfd_noalloc_max_rows() rows (32768) with the single-CTA
  * FP64 BiCGSTAB (precond KCFD_PREC_NONE or KCFD_PREC_JACOBI, stop rule as in
  * kcfd_solver_create) and allocates nothing: its Krylov vectors live in a fixed
  * array inside libkcfd (about 2.6 MB held on every GPU that loads the library until
  * the process exits). Larger systems are rejected with KCFD_BAD_INPUT. The first
  * call on a device looks up the array's device address, so make that call before
- * any stream capture. All calls share the array: calls that overlap on the GPU
- * (on different streams) race. A, b, x (x0 on entry), iters, relres and status
+ * any stream capture (a first call on a capturing stream returns KCFD_BAD_INPUT and
+ * says so). All calls share the array and it keeps the last call's contents (each
+ * call initialises what it reads): calls that overlap on the GPU (on different
+ * streams) race. A, b, x (x0 on entry), iters, relres and status
  * are caller device memory, as in kcfd_solver_solve.                              */
 int kcfd_noalloc_max_rows(void);
 int kcfd_bicgstab_noalloc(const kcfd_csr_t* A, const double* b, double* x, int32_t precond, int32_t stop,

@@ -64,6 +64,7 @@ struct Level {
     int *pip = nullptr, *pix = nullptr, *pdiag = nullptr;
     int *prow = nullptr, *plp = nullptr, *pla = nullptr;  // P entry -> its row; its A entries [plp, plp+1) in pla
     int rlanes = 1;                                        // lanes per coarse row of the restriction
+    int slanes = 1;                                        // lanes per row of the smoothing kernels
     double* p64 = nullptr;
     void* pV = nullptr;
     int *rip = nullptr, *rix = nullptr, *rsrc = nullptr;
@@ -169,20 +170,58 @@ __device__ __forceinline__ double csr_row_dot(int k0, int k1, const int* __restr
     return acc;
 }
 
+// Lane q of the L lanes sharing row i of a sliced-ELL matrix: the partial sum over the
+// row's entries q, q + L, ... (L = 1: the whole row, entries loaded in batches of 8).
+template <int L, typename V, typename T>
+__device__ __forceinline__ double sell_row_part(const int* __restrict__ off, const int* __restrict__ col,
+                                                const V* __restrict__ val, int i, const T* x, int q) {
+    if (L == 1) return sell_row_dot(off, col, val, i, x);
+    const int sl = i >> 5;
+    const int o0 = __ldg(off + sl), o1 = __ldg(off + sl + 1);
+    const int base = o0 + (i & 31), w = (o1 - o0) >> 5;
+    double acc = 0.0;
+    for (int k = q; k < w; k += L) {
+        const int j = __ldg(col + base + 32 * k);
+        if (j >= 0) acc += (double)__ldg(val + base + 32 * k) * (double)x[j];
+    }
+    return acc;
+}
+
+// Rows of a level handled by groups of L lanes (the small coarse levels, whose rows are
+// long and few, take several lanes per row so that more loads are in flight): f(i,
+// partial sum of row i) for each row, called on every lane with i < n after the L
+// partials are combined by a fixed xor-shuffle tree (lane q == 0 writes). The trip
+// count depends on the warp's first group only, so every lane of a warp runs it.
+template <int L, typename F>
+__device__ __forceinline__ void rows_by_lanes(int n, F f) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int q = tid & (L - 1);
+    const int groups = (gridDim.x * blockDim.x) / L;
+    const int g = tid / L, g0 = (tid & ~31) / L;
+    for (int t = 0; g0 + t * groups < n; ++t) {
+        const int i = g + t * groups;
+        f(i, q);
+    }
+}
+
 // ------------------------------------------------------------------ cycle kernels --
 // Pre-smoothing from a zero guess and the residual: x = sd b, r = b - W b (W = omega A D^-1).
-template <typename V, typename TI>
+template <typename V, typename TI, int L = 1>
 __global__ void __launch_bounds__(256) k_pre(int n, const int* __restrict__ off, const int* __restrict__ col,
                                              const V* __restrict__ W, const V* __restrict__ sd, const TI* b, V* x,
                                              V* r, const int* active) {
     pdl_enter();
     if (inactive(active)) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double bi = (double)b[i];
-        const double wb = sell_row_dot(off, col, W, i, b);
-        x[i] = (V)((double)__ldg(sd + i) * bi);
-        r[i] = (V)(bi - wb);
-    }
+    rows_by_lanes<L>(n, [&](int i, int q) {
+        double wb = i < n ? sell_row_part<L>(off, col, W, i, b, q) : 0.0;
+#pragma unroll
+        for (int o = L / 2; o > 0; o >>= 1) wb += __shfl_xor_sync(0xffffffffu, wb, o);
+        if (i < n && q == 0) {
+            const double bi = (double)b[i];
+            x[i] = (V)((double)__ldg(sd + i) * bi);
+            r[i] = (V)(bi - wb);
+        }
+    });
 }
 
 // Restriction bc = P^T r (P^T in CSR). A coarse row gathers the fine rows of its
@@ -205,8 +244,24 @@ __global__ void __launch_bounds__(256) k_restrict(int nc, const int* __restrict_
         const bool row = I < nc;
         double acc = 0.0;
         if (row) {
+            // four entries per lane in flight: columns and values first, then the gathers
             const int k0 = __ldg(rip + I), k1 = __ldg(rip + I + 1);
-            for (int k = k0 + q; k < k1; k += L) acc += (double)__ldg(R + k) * (double)r[__ldg(rix + k)];
+            for (int k = k0 + q; k < k1; k += 4 * L) {
+                int jj[4];
+                double vv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) {
+                    const bool in = k + u * L < k1;
+                    jj[u] = in ? __ldg(rix + k + u * L) : -1;
+                    vv[u] = in ? (double)__ldg(R + k + u * L) : 0.0;
+                }
+                double xv[4];
+#pragma unroll
+                for (int u = 0; u < 4; ++u) xv[u] = jj[u] >= 0 ? (double)r[jj[u]] : 0.0;
+#pragma unroll
+                for (int u = 0; u < 4; ++u)
+                    if (jj[u] >= 0) acc += vv[u] * xv[u];
+            }
         }
 #pragma unroll
         for (int o = L / 2; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
@@ -241,16 +296,18 @@ __global__ void __launch_bounds__(256) k_prolong(int n, const int* __restrict__ 
 }
 
 // Post-smoothing: y = x + sd (b - A x).
-template <typename V, typename TI, typename TO>
+template <typename V, typename TI, typename TO, int L = 1>
 __global__ void __launch_bounds__(256) k_post(int n, const int* __restrict__ off, const int* __restrict__ col,
                                               const V* __restrict__ A, const V* __restrict__ sd, const TI* b,
                                               const V* x, TO* y, const int* active) {
     pdl_enter();
     if (inactive(active)) return;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const double ax = sell_row_dot(off, col, A, i, x);
-        y[i] = (TO)((double)x[i] + (double)__ldg(sd + i) * ((double)b[i] - ax));
-    }
+    rows_by_lanes<L>(n, [&](int i, int q) {
+        double ax = i < n ? sell_row_part<L>(off, col, A, i, x, q) : 0.0;
+#pragma unroll
+        for (int o = L / 2; o > 0; o >>= 1) ax += __shfl_xor_sync(0xffffffffu, ax, o);
+        if (i < n && q == 0) y[i] = (TO)((double)x[i] + (double)__ldg(sd + i) * ((double)b[i] - ax));
+    });
 }
 
 // ------------------------------------------------------------------ set-up kernels --
@@ -435,98 +492,101 @@ __global__ void k_dense(int nc, const int* __restrict__ ip, const int* __restric
 }
 
 // When `smem` is set the matrix and its inverse live in dynamic shared memory (2 nc^2
-// doubles): every elimination step then stays on the SM.
+// doubles): every elimination step then stays on the SM. Warp w of the block owns rows
+// w, w + 32, ... and lane l columns l, l + 32, ... of [M | Inv], so no thread divides
+// an index; warp 0 alone finds the pivot. A step is the pivot search, the row swap,
+// the staging of the scaled pivot row and the pivot column, and the elimination.
 template <typename V>
 __global__ void __launch_bounds__(1024) k_gj(int nc, double* Mg, double* Invg, V* C, int smem) {
     extern __shared__ double dyn[];
     double* M = smem ? dyn : Mg;
     double* Inv = smem ? dyn + (size_t)nc * nc : Invg;
-    if (smem)
-        for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) M[t] = Mg[t];
-    __shared__ double f[kDenseMax];
-    __shared__ double sv[32];
-    __shared__ int si[32];
-    __shared__ double scale_s;
-    __shared__ int piv_s;
+    __shared__ double prow[2 * kDenseMax];   // the scaled pivot row of [M | Inv]
+    __shared__ double fcol[kDenseMax];       // the pivot column before the step
     __shared__ int drop[kDenseMax];
-    const int tid = threadIdx.x, nt = blockDim.x, lane = tid & 31, wid = tid >> 5;
-    for (int t = tid; t < nc * nc; t += nt) Inv[t] = ((t / nc) == (t % nc)) ? 1.0 : 0.0;
-    __syncthreads();
-    for (int t = tid; t < nc; t += nt) drop[t] = 0;
-    // largest |entry|
+    __shared__ double wmax[32];
+    __shared__ int piv_s;
+    __shared__ double tol_s;
+    const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, nty = blockDim.x >> 5;
+    const int W = 2 * nc;
     double m = 0.0;
-    for (int t = tid; t < nc * nc; t += nt) m = fmax(m, fabs(M[t]));
+    for (int i = ty; i < nc; i += nty)
+        for (int j = tx; j < nc; j += 32) {
+            const double v = Mg[(size_t)i * nc + j];
+            if (smem) M[(size_t)i * nc + j] = v;
+            Inv[(size_t)i * nc + j] = (i == j) ? 1.0 : 0.0;
+            m = fmax(m, fabs(v));
+        }
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) drop[t] = 0;
     for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (lane == 0) sv[wid] = m;
+    if (tx == 0) wmax[ty] = m;
     __syncthreads();
-    if (tid == 0) {
+    if (threadIdx.x == 0) {
         double mm = 0.0;
-        for (int w = 0; w < (nt >> 5); ++w) mm = fmax(mm, sv[w]);
-        scale_s = mm;
+        for (int w = 0; w < nty; ++w) mm = fmax(mm, wmax[w]);
+        tol_s = 1e-13 * mm;
     }
     __syncthreads();
-    const double tol = 1e-13 * scale_s;
     for (int k = 0; k < nc; ++k) {
-        // pivot: largest |M[i][k]| over i >= k, smallest i on ties
-        double bv = -1.0;
-        int bi = nc;
-        for (int i = k + tid; i < nc; i += nt) {
-            const double v = fabs(M[(size_t)i * nc + k]);
-            if (v > bv) { bv = v; bi = i; }
-        }
-        for (int o = 16; o > 0; o >>= 1) {
-            const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
-            const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-            if (ov > bv || (ov == bv && oi < bi)) { bv = ov; bi = oi; }
-        }
-        if (lane == 0) { sv[wid] = bv; si[wid] = bi; }
-        __syncthreads();
-        if (tid == 0) {
-            double b = -1.0;
-            int p = nc;
-            for (int w = 0; w < (nt >> 5); ++w)
-                if (sv[w] > b || (sv[w] == b && si[w] < p)) { b = sv[w]; p = si[w]; }
-            piv_s = (b > tol) ? p : -1;
-            if (piv_s < 0) drop[k] = 1;
+        if (ty == 0) {
+            // pivot: the largest |M[i][k]| over i >= k, the smallest i on ties
+            double bv = -1.0;
+            int bi = nc;
+            for (int i = k + tx; i < nc; i += 32) {
+                const double v = fabs(M[(size_t)i * nc + k]);
+                if (v > bv) {
+                    bv = v;
+                    bi = i;
+                }
+            }
+            for (int o = 16; o > 0; o >>= 1) {
+                const double ov = __shfl_xor_sync(0xffffffffu, bv, o);
+                const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+                if (ov > bv || (ov == bv && oi < bi)) {
+                    bv = ov;
+                    bi = oi;
+                }
+            }
+            if (tx == 0) {
+                piv_s = (bv > tol_s) ? bi : -1;
+                if (piv_s < 0) drop[k] = 1;
+            }
         }
         __syncthreads();
         const int p = piv_s;
-        if (p < 0) continue;  // dropped unknown: its row of M stays, its inverse row is cleared below
+        if (p < 0) continue;  // a dropped unknown: its inverse row and column are cleared below
         if (p != k)
-            for (int j = tid; j < nc; j += nt) {
-                double t = M[(size_t)k * nc + j];
-                M[(size_t)k * nc + j] = M[(size_t)p * nc + j];
-                M[(size_t)p * nc + j] = t;
-                t = Inv[(size_t)k * nc + j];
-                Inv[(size_t)k * nc + j] = Inv[(size_t)p * nc + j];
-                Inv[(size_t)p * nc + j] = t;
+            for (int j = threadIdx.x; j < W; j += blockDim.x) {
+                double* A = j < nc ? M : Inv;
+                const int c = j < nc ? j : j - nc;
+                const double t = A[(size_t)k * nc + c];
+                A[(size_t)k * nc + c] = A[(size_t)p * nc + c];
+                A[(size_t)p * nc + c] = t;
             }
         __syncthreads();
         const double inv_p = 1.0 / M[(size_t)k * nc + k];
+        for (int j = threadIdx.x; j < W; j += blockDim.x)
+            prow[j] = (j < nc ? M[(size_t)k * nc + j] : Inv[(size_t)k * nc + j - nc]) * inv_p;
+        for (int i = threadIdx.x; i < nc; i += blockDim.x) fcol[i] = M[(size_t)i * nc + k];
         __syncthreads();
-        for (int j = tid; j < nc; j += nt) {
-            M[(size_t)k * nc + j] *= inv_p;
-            Inv[(size_t)k * nc + j] *= inv_p;
-        }
-        __syncthreads();
-        for (int i = tid; i < nc; i += nt) f[i] = (i == k) ? 0.0 : M[(size_t)i * nc + k];
-        __syncthreads();
-        for (int t = tid; t < nc * nc; t += nt) {
-            const int i = t / nc, j = t % nc;
-            if (i == k) continue;
-            const double fi = f[i];
-            if (fi == 0.0) continue;
-            M[t] -= fi * M[(size_t)k * nc + j];
-            Inv[t] -= fi * Inv[(size_t)k * nc + j];
+        for (int i = ty; i < nc; i += nty) {
+            const double f = fcol[i];
+            for (int j = tx; j < W; j += 32) {
+                double* A = j < nc ? M : Inv;
+                const size_t q = (size_t)i * nc + (j < nc ? j : j - nc);
+                if (i == k) A[q] = prow[j];
+                else if (f != 0.0) A[q] -= f * prow[j];
+            }
         }
         __syncthreads();
     }
-    for (int t = tid; t < nc * nc; t += nt) {
-        const int i = t / nc, j = t % nc;
-        const double v = (drop[i] || drop[j]) ? 0.0 : Inv[t];
-        Invg[t] = v;
-        C[t] = (V)v;
-    }
+    for (int i = ty; i < nc; i += nty)
+        for (int j = tx; j < nc; j += 32) {
+            const size_t q = (size_t)i * nc + j;
+            const double v = (drop[i] || drop[j]) ? 0.0 : Inv[q];
+            Invg[q] = v;
+            C[q] = (V)v;
+        }
 }
 
 // ---------------------------------------------------------------- host: patterns --
@@ -888,14 +948,18 @@ int vcycle_t(const kcfd_amg* h, const double* in, double* out, const int* active
         const Level& lv = h->lv[l];
         const Level& nx = h->lv[l + 1];
         const int g = grid_for(h, lv.n);
-        if (l == 0)
+        if (l == 0) {
             launch(k_pre<V, double>, g, 256, st, pdl, lv.n, (const int*)lv.soff, (const int*)lv.scol, (const V*)lv.sW,
                    (const V*)lv.sd, in, (V*)lv.x, (V*)lv.r, active);
-        else
-            launch(k_pre<V, V>, g, 256, st, pdl, lv.n, (const int*)lv.soff, (const int*)lv.scol, (const V*)lv.sW,
-                   (const V*)lv.sd, (const V*)lv.b, (V*)lv.x, (V*)lv.r, active);
+        } else {
+            const int L_ = lv.slanes;
+            auto pk = L_ >= 32 ? k_pre<V, V, 32> : L_ == 16 ? k_pre<V, V, 16> : L_ == 8 ? k_pre<V, V, 8>
+                    : L_ == 4 ? k_pre<V, V, 4> : L_ == 2 ? k_pre<V, V, 2> : k_pre<V, V, 1>;
+            launch(pk, grid_for(h, (int64_t)lv.n * L_), 256, st, pdl, lv.n, (const int*)lv.soff, (const int*)lv.scol,
+                   (const V*)lv.sW, (const V*)lv.sd, (const V*)lv.b, (V*)lv.x, (V*)lv.r, active);
+        }
         const int gr = grid_for(h, (int64_t)nx.n * lv.rlanes);
-        auto rk = lv.rlanes >= 16 ? k_restrict<V, 16> : lv.rlanes == 8 ? k_restrict<V, 8>
+        auto rk = lv.rlanes >= 32 ? k_restrict<V, 32> : lv.rlanes == 16 ? k_restrict<V, 16> : lv.rlanes == 8 ? k_restrict<V, 8>
                 : lv.rlanes == 4 ? k_restrict<V, 4> : lv.rlanes == 2 ? k_restrict<V, 2> : k_restrict<V, 1>;
         launch(rk, gr, 256, st, pdl, nx.n, (const int*)lv.rip, (const int*)lv.rix, (const V*)lv.rV, (const V*)lv.r,
                (V*)nx.b, active);
@@ -909,12 +973,16 @@ int vcycle_t(const kcfd_amg* h, const double* in, double* out, const int* active
         const int g = grid_for(h, lv.n);
         launch(k_prolong<V>, g, 256, st, pdl, lv.n, (const int*)lv.pip, (const int*)lv.pix, (const V*)lv.pV,
                (const V*)nx.y, (V*)lv.x, active);
-        if (l == 0)
+        if (l == 0) {
             launch(k_post<V, double, double>, g, 256, st, pdl, lv.n, (const int*)lv.soff, (const int*)lv.scol,
                    (const V*)lv.sA, (const V*)lv.sd, in, (const V*)lv.x, out, active);
-        else
-            launch(k_post<V, V, V>, g, 256, st, pdl, lv.n, (const int*)lv.soff, (const int*)lv.scol, (const V*)lv.sA,
-                   (const V*)lv.sd, (const V*)lv.b, (const V*)lv.x, (V*)lv.y, active);
+        } else {
+            const int L_ = lv.slanes;
+            auto qk = L_ >= 32 ? k_post<V, V, V, 32> : L_ == 16 ? k_post<V, V, V, 16> : L_ == 8 ? k_post<V, V, V, 8>
+                    : L_ == 4 ? k_post<V, V, V, 4> : L_ == 2 ? k_post<V, V, V, 2> : k_post<V, V, V, 1>;
+            launch(qk, grid_for(h, (int64_t)lv.n * L_), 256, st, pdl, lv.n, (const int*)lv.soff, (const int*)lv.scol,
+                   (const V*)lv.sA, (const V*)lv.sd, (const V*)lv.b, (const V*)lv.x, (V*)lv.y, active);
+        }
     }
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
@@ -951,7 +1019,7 @@ int kcfd_amg_create(const kcfd_csr_t* A, const kcfd_amg_opts_t* opts, kcfd_amg**
     KCFD_REQUIRE(o.mode == KCFD_MODE_FP64 || o.mode == KCFD_MODE_MIXED, "kcfd_amg_create: bad mode");
     if (o.coarse_max <= 0) o.coarse_max = 128;
     if (o.max_levels <= 0) o.max_levels = 12;
-    if (o.power_iters <= 0) o.power_iters = 4;
+    if (o.power_iters <= 0) o.power_iters = 8;
     KCFD_REQUIRE(o.coarse_max <= kDenseMax, "kcfd_amg_create: coarse_max above %d", kDenseMax);
     KCFD_REQUIRE(o.max_levels <= kMaxLevels, "kcfd_amg_create: max_levels above %d", kMaxLevels);
     KCFD_REQUIRE(o.power_iters <= 100, "kcfd_amg_create: power_iters above 100");
@@ -1037,7 +1105,12 @@ int kcfd_amg_create(const kcfd_csr_t* A, const kcfd_amg_opts_t* opts, kcfd_amg**
         // restriction lanes: about three entries per lane of a coarse row
         const double ravg = (double)pn / std::max(1, na);
         lv.rlanes = 1;
-        while (lv.rlanes < 16 && 3.0 * lv.rlanes < ravg) lv.rlanes <<= 1;
+        while (lv.rlanes < 32 && 3.0 * lv.rlanes < ravg) lv.rlanes <<= 1;
+        // smoothing lanes: a level of few long rows shares each row between lanes until
+        // about 64k threads are busy (at least two entries per lane)
+        const double savg = (double)cur.ip[cur.n] / std::max(1, cur.n);
+        lv.slanes = 1;
+        while (lv.slanes < 32 && (int64_t)cur.n * lv.slanes < 65536 && 2.0 * 2 * lv.slanes <= savg) lv.slanes <<= 1;
         lv.agg = agg;
         lv.nc = na;
         lv.pnnz = t.P.ip[cur.n];

@@ -2635,12 +2635,19 @@ __global__ void noalloc_prep_kernel(int n, const int* __restrict__ ip, const int
 static std::mutex g_noalloc_mu;
 static double* g_noalloc_ptr[64] = {};
 
-static int noalloc_scratch(double** out) {
+static int noalloc_scratch(double** out, cudaStream_t st) {
     int dev = 0;
     KCFD_CUDA(cudaGetDevice(&dev));
     KCFD_REQUIRE(dev >= 0 && dev < 64, "kcfd_bicgstab_noalloc: device index %d out of range", dev);
     std::lock_guard<std::mutex> lk(g_noalloc_mu);
     if (!g_noalloc_ptr[dev]) {
+        // the address look-up may not run inside a capture: refuse with a message that
+        // names the cause instead of leaving the caller's capture broken
+        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+        KCFD_CUDA(cudaStreamIsCapturing(st, &cap));
+        KCFD_REQUIRE(cap == cudaStreamCaptureStatusNone,
+                     "kcfd_bicgstab_noalloc: the first call on device %d must come before any stream capture "
+                     "(it looks up the scratch array's address)", dev);
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess || !p) {
@@ -2671,7 +2678,7 @@ int kcfd_bicgstab_noalloc(const kcfd_csr_t* A, const double* b, double* x, int32
     KCFD_REQUIRE(stop == KCFD_STOP_SCIPY || stop == KCFD_STOP_GPU, "kcfd_bicgstab_noalloc: bad stop rule");
     KCFD_REQUIRE(maxiter >= 0, "kcfd_bicgstab_noalloc: maxiter < 0");
     double* scratch = nullptr;
-    if (int e = kcfd::noalloc_scratch(&scratch)) return e;
+    if (int e = kcfd::noalloc_scratch(&scratch, (cudaStream_t)stream)) return e;
     const int n = A->n;
     double* work = scratch;                                     // 9 vectors of n
     double* dinv = scratch + (size_t)9 * kcfd::kNoAllocMaxRows;  // n

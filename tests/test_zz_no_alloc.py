@@ -1,9 +1,10 @@
 """The allocation-free BiCGSTAB entry point (kcfd_bicgstab_noalloc) against the
 handle-based one (kcfd_solver_create / kcfd_solver_solve).
 
-Callers that cannot allocate device memory -- code running during CUDA graph
-capture, real-time loops, hosts with a fixed memory budget -- use the no-alloc entry
-point; its Krylov scratch is a fixed array inside libkcfd. This file is collected
+Callers that cannot allocate device memory -- real-time loops that must not block on
+the device allocator, host programs whose device memory is owned by someone else --
+use the no-alloc entry point; its Krylov scratch is a fixed array inside libkcfd that
+every call shares and that keeps the last call's contents. This file is collected
 last so that a run stopping at the first failure has already run every other test.
 Both entry points run the same single-CTA FP64 kernel, so their solutions must agree
 to the 1e-12 relative L2 tolerance used for same-algorithm comparisons elsewhere.
@@ -68,6 +69,7 @@ def test_noalloc_matches_handle_two_calls_in_a_row():
     A2, b2 = _hex_system(12, seed=4)
     cases = [(A1, b1, np.zeros(len(b1)), "jacobi"),
              (A2, b2, np.linspace(-1.0, 1.0, len(b2)), "none")]
+    first = None
     for A, b, x0, pc in cases:  # two calls in a row on the shared scratch
         d = DeviceCSR.from_scipy(A)
         xn, itn, stn = _noalloc(d, b, x0, pc, 1e-10)
@@ -76,6 +78,13 @@ def test_noalloc_matches_handle_two_calls_in_a_row():
         assert itn == ith
         assert _rel(xn, xh) < 1e-12
         assert np.linalg.norm(b - A @ xn) / np.linalg.norm(b) < 2e-10
+        if first is None:
+            first = (xn, itn)
+    # the smaller system again after the larger one left its data in the shared array
+    A, b, x0, pc = cases[0]
+    xn, itn, stn = _noalloc(DeviceCSR.from_scipy(A), b, x0, pc, 1e-10)
+    assert stn == 0 and itn == first[1]
+    np.testing.assert_array_equal(xn, first[0])
 
 
 def test_noalloc_rejects_oversized_systems():

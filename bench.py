@@ -412,8 +412,15 @@ def run_ours(args):
     dev = torch.cuda.current_device()
     N = args.size
     t_setup = time.time()
-    s = make_solver(N, precision="fp64", graph=True, p_precond=args.p_precond)
+    s = make_solver(N, precision="mixed" if args.mixed else "fp64", graph=True, p_precond=args.p_precond)
     setup_s = time.time() - t_setup
+    if args.iterate_only:
+        # a fixed number of outer iterations from the initial state and nothing else:
+        # the command the committed ncu launch lists are taken on (no timing here)
+        s.iterate(args.iterate_only)
+        torch.cuda.synchronize()
+        print(json.dumps({"iterated": args.iterate_only, "setup_s": round(setup_s, 2), **s.solver_stats()}))
+        return
     mesh = s.mesh
     n_faces, nnz = int(mesh.n_faces), int(mesh.nnz)
     s.reset_history()
@@ -775,7 +782,7 @@ def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active
     from kcfd.serve import Request, Server, make_requests, summarize
     reqs = make_requests(requests, rate, seed=0)
     common = dict(budget_bytes=150e9, iters_per_tick=10, max_iters=max_iters, cont_tol=cont_tol,
-                  precision="fp64", graph=True, precond_p="ilu0", keep_fields=True)
+                  precision="fp64", graph=True, precond_p="auto", keep_fields=True)
     # warm-up: one small case of each dimension (kernel loading, allocator)
     Server(**common).run([Request(0, 2, 32, 400.0, 0.0), Request(1, 3, 16, 400.0, 0.0)])
     torch.cuda.synchronize()
@@ -802,7 +809,7 @@ def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active
             "served_over_serial": round(ours["cases_per_s"] / serial_d["cases_per_s"], 2) if serial_d else None,
             "desc": f"{len(reqs)} cavity requests at {rate} req/s (Poisson, seed 0): 2D N^2 N~U{{32..512}}, 3D N^3 "
                     f"N~U{{16..96}}, Re~U(100,1000); each to continuity {cont_tol:g} (max {max_iters} outer "
-                    f"iterations); FP64, ILU(0) p', HBM budget 150 GB; continuous batching (max {max_active} "
+                    f"iterations); FP64, p' by the multigrid above 32,768 cells and ILU(0) below, HBM budget 150 GB; continuous batching (max {max_active} "
                     f"resident, {policy} admission, cases built on 2 host threads)"}
 
 
@@ -907,16 +914,22 @@ def run_c1(args):
 C3_METRIC = "two-fluid time steps/s (Delaunay tets, 10 SIMPLE inner iterations per step, 6-equation energy)"
 
 
-def c3_solver(n_target, seed=0, oracle=False):
+def c3_solver(n_target, seed=0, oracle=False, p_precond="amg", precision="fp64", arrays=None):
     """The two-fluid workload: a 0.2 x 0.2 x 1.0 m box of Delaunay tetrahedra
     (jittered lattice, ~n_target cells), bottom 'inlet_gas', top 'outlet', 'wall'
     elsewhere; water / air (rho 998 / 1.2, mu 1e-3 / 1.8e-5, cp_l 4182), d_b = 3 mm,
     Lee rate 0.1 1/s, T_sat 373.15 K; inlet superficial gas velocity 0.01 m/s at
     alpha_in = 0.05 (u_g = 0.2 m/s); alpha_g ~ U(0.02, 0.08), T_l = T_g = 370 + U(0, 6) K;
-    dt = 1e-3, 10 inner iterations, energy on. oracle=True builds the numpy oracle."""
+    dt = 1e-3, 10 inner iterations, energy on. oracle=True builds the numpy oracle.
+    arrays: the (nodes, cells, cf, bd) of an earlier call with the same n_target and seed
+    (the mesh is not generated again; the initial fields are the same draws)."""
     from kcfd import meshgen
     rng = np.random.default_rng(seed)
-    nodes, cells, cf, bd = meshgen.delaunay_tet_arrays((0.2, 0.2, 1.0), n_target, rng)
+    if arrays is None:
+        arrays = meshgen.delaunay_tet_arrays((0.2, 0.2, 1.0), n_target, rng)
+    else:
+        rng.integers(0, 2**31)   # the generator's one draw (its jitter seed)
+    nodes, cells, cf, bd = arrays
     if oracle:
         from oracle import mesh as om
         from oracle.two_fluid import TwoFluid
@@ -927,7 +940,7 @@ def c3_solver(n_target, seed=0, oracle=False):
         from kcfd import mesh as km
         from kcfd.two_fluid import TwoFluidSolver
         m = km.build_mesh(nodes, cells, bd, ndim=3, cell_face_node_list=cf)
-        sv = TwoFluidSolver(m)
+        sv = TwoFluidSolver(m, p_precond=p_precond, precision=precision)
         setf = lambda k, v: setattr(getattr(sv, k), "values", v)  # noqa: E731
     sv.rho_l, sv.mu_l, sv.cp_l = 998.0, 1e-3, 4182.0
     sv.rho_g, sv.mu_g = 1.2, 1.8e-5
@@ -944,6 +957,7 @@ def c3_solver(n_target, seed=0, oracle=False):
     setf("alpha_l", 1.0 - ag)
     setf("T_l", T)
     setf("T_g", T.copy())
+    sv._arrays = arrays
     return sv, m
 
 
@@ -969,7 +983,8 @@ def run_c3(args):
     the steps whose fields are still finite are counted, each timed on its own."""
     import torch
     t0 = time.time()
-    sv, m = c3_solver(args.tets)
+    sv, m = c3_solver(args.tets, p_precond=args.p_precond)
+    arrays = sv._arrays
     setup_s = time.time() - t0
     state0 = {k: t.clone() for k, t in _c3_tensors(sv).items()}
 
@@ -1006,13 +1021,17 @@ def run_c3(args):
     roof = None
     if n_ok:
         k = [v.cpu().numpy() for v in kry[: n_ok + 1]]
-        it1, itg = int(k[-1][0] - k[0][0]), int(k[-1][1] - k[0][1])
+        it1, itg, itp = (int(k[-1][j] - k[0][j]) for j in range(3))
         nnz = int(m.nnz)
+        amg = amg_levels(sv._sp) if args.p_precond == "amg" else None
         byts = solver_bytes(m.n_cells, nnz, it1, "ilu0", 8) + solver_bytes(m.n_cells, nnz, itg, "ilu0", 8, nrhs=3)
+        if amg:
+            byts += solver_bytes(m.n_cells, nnz, itp, "amg", 8, amg=amg)
         peak = measured_peak()
-        roof = {"bound": "hbm", "kernel": "graph engine BiCGSTAB + ILU(0) solves (all 80 systems of a step)",
+        roof = {"bound": "hbm", "kernel": "graph engine BiCGSTAB solves (all 80 systems of a step: ILU(0), and the "
+                                          "multigrid for p')",
                 "unit_of_work": "the solves of the counted steps (formula bytes x Krylov iterations)",
-                "krylov_iters": {"one_rhs": it1, "three_rhs": itg},
+                "krylov_iters": {"one_rhs_ilu0": it1, "three_rhs_ilu0": itg, "p_multigrid": itp},
                 "achieved": round(byts / t / 1e9, 1), "peak": peak[0], "unit": "GB/s",
                 "frac": round(byts / t / 1e9 / peak[0], 3), "peak_source": peak[1], "traffic": None,
                 "note": "the time is the whole step (assembly, closures and set-up included), so this is a "
@@ -1035,6 +1054,37 @@ def run_c3(args):
             break
         te += dt_e
         ne += 1
+    # the mixed form (the multigrid p' hierarchy in FP32) from the same initial state,
+    # its fields after the same finite steps against FP64's
+    mixed = None
+    if args.plain and args.p_precond == "amg" and n_ok:
+        # the steps before the model's divergence shows (residual below 1e3): past it
+        # both runs' fields grow without bound and their difference says nothing
+        ncmp = max(1, next((i for i, r in enumerate(res[:n_ok]) if not (float(r) < 1e3)), n_ok))
+        restore()
+        for _ in range(ncmp):
+            sv.step()
+        ref = {k: getattr(sv, k).values for k in ("alpha_g", "U_l", "U_g", "p", "T_l", "T_g")}
+        del sv
+        torch.cuda.empty_cache()
+        sm, _ = c3_solver(args.tets, p_precond="amg", precision="mixed", arrays=arrays)
+        cur = _c3_tensors(sm)
+        for k2, t2 in state0.items():
+            if k2 in cur and cur[k2].shape == t2.shape:
+                cur[k2].copy_(t2)
+        torch.cuda.synchronize()
+        tm0 = time.perf_counter()
+        for _ in range(ncmp):
+            sm.step()
+        torch.cuda.synchronize()
+        tm = time.perf_counter() - tm0
+        errs = {k2: float(np.linalg.norm(getattr(sm, k2).values - v) / max(np.linalg.norm(v), 1e-300))
+                for k2, v in ref.items()}
+        mixed = {"value": round(ncmp / tm, 4), "unit": "steps/s", "steps": ncmp, "field_error": errs,
+                 "desc": "the same workload with the multigrid p' hierarchy stored in FP32 (FP64 Krylov iteration "
+                         "and every other system FP64); field_error = relative L2 against the FP64 run after the "
+                         "same steps from the same initial state (alpha_g, U_l, U_g, p, T_l, T_g), over the "
+                         "steps before the model's residual passes 1e3"}
     cpu = None
     if not args.no_cpu:
         so, mo = c3_solver(args.cpu_tets, oracle=True)
@@ -1054,13 +1104,14 @@ def run_c3(args):
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
         "config": {"workload": f"two-fluid bubble column, {m.n_cells} Delaunay tets in 0.2x0.2x1.0 m, water/air, "
                                "d_b 3 mm, Lee phase change, dt 1e-3, 10 inner SIMPLE iterations per step, energy on; "
-                               "every system BiCGSTAB + ILU(0) to 1e-12",
+                               "every system BiCGSTAB to 1e-12: ILU(0), and for p' "
+                               + ("the multigrid" if args.p_precond == "amg" else "ILU(0)"),
                    "cells": int(m.n_cells), "faces": int(m.n_faces), "setup_s": round(setup_s, 1),
                    "parallelism": "1 GPU", "l2": "working set >> 126 MB L2; no flush needed"},
         "clocks": clocks,
         "e2e": {"value": round(ne / te, 4) if ne else None, "unit": "steps/s", "h2d_bytes_per_step": int(nbytes),
                 "d2h_bytes_per_step": int(nbytes), "steps": ne},
-        "cpu_baseline": cpu, "roofline": roof,
+        "cpu_baseline": cpu, "roofline": roof, "mixed_precision_variant": mixed,
         "finite_steps": n_ok, "max_residual_per_step": [float(r) for r in res],
         "max_abs_velocity_after_all_steps": umax,
         "note": "the reference two-fluid model diverges on this workload within a few steps (its numpy "
@@ -1172,6 +1223,9 @@ def main():
     ap.add_argument("--systems", type=int, default=1024, help="c4: number of systems")
     ap.add_argument("--c4-mode", default="fp64", choices=["fp64", "mixed"], help="c4: batched solve precision")
     ap.add_argument("--plain", type=int, default=1, help="also time the variants (rank 0)")
+    ap.add_argument("--iterate-only", type=int, default=0,
+                    help="c2: run this many outer iterations from the initial state and exit (for profilers)")
+    ap.add_argument("--mixed", action="store_true", help="c2 with --iterate-only: the mixed form")
     args = ap.parse_args()
     args.legs = [x for x in args.legs.split(",") if x]
     if args.warmup < 3:

@@ -49,6 +49,7 @@ namespace amg {
 constexpr int kMaxLevels = 16;
 constexpr int kDenseMax = 256;   // largest coarsest level solved by its dense inverse
 constexpr int kRedGrid = 1024;   // blocks of the power-iteration reductions (at most)
+constexpr int kGjSmemMax = 200 * 1024;  // dynamic shared memory of the Gauss-Jordan kernel (at most)
 
 struct Level {
     int n = 0, nnz = 0, nc = 0;                 // rows, entries, rows of the next level
@@ -480,9 +481,11 @@ __global__ void k_product(int64_t m, const int64_t* __restrict__ ptr, const int*
 }
 
 // Coarsest level: the dense matrix, then its inverse by Gauss-Jordan elimination with
-// partial pivoting in one CTA. A pivot below 1e-13 of the largest entry drops its
-// unknown (row and column of the inverse set to zero), so a singular coarsest operator
-// still gives a bounded cycle.
+// partial pivoting in one CTA. A pivot below 1e-13 of the largest entry of its column
+// (in the matrix before elimination) drops its unknown (row and column of the inverse
+// set to zero), so a singular coarsest operator still gives a bounded cycle; the
+// tolerance is per column so that one huge entry (a row pinned by a large diagonal)
+// does not drop every other unknown.
 __global__ void k_dense(int nc, const int* __restrict__ ip, const int* __restrict__ ix, const double* __restrict__ a,
                         double* M) {
     for (int t = threadIdx.x; t < nc * nc; t += blockDim.x) M[t] = 0.0;
@@ -504,27 +507,21 @@ __global__ void __launch_bounds__(1024) k_gj(int nc, double* Mg, double* Invg, V
     __shared__ double prow[2 * kDenseMax];   // the scaled pivot row of [M | Inv]
     __shared__ double fcol[kDenseMax];       // the pivot column before the step
     __shared__ int drop[kDenseMax];
-    __shared__ double wmax[32];
+    __shared__ double ctol[kDenseMax];       // drop tolerance of each column
     __shared__ int piv_s;
-    __shared__ double tol_s;
     const int tx = threadIdx.x & 31, ty = threadIdx.x >> 5, nty = blockDim.x >> 5;
     const int W = 2 * nc;
-    double m = 0.0;
     for (int i = ty; i < nc; i += nty)
         for (int j = tx; j < nc; j += 32) {
             const double v = Mg[(size_t)i * nc + j];
             if (smem) M[(size_t)i * nc + j] = v;
             Inv[(size_t)i * nc + j] = (i == j) ? 1.0 : 0.0;
-            m = fmax(m, fabs(v));
         }
-    for (int t = threadIdx.x; t < nc; t += blockDim.x) drop[t] = 0;
-    for (int o = 16; o > 0; o >>= 1) m = fmax(m, __shfl_xor_sync(0xffffffffu, m, o));
-    if (tx == 0) wmax[ty] = m;
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        double mm = 0.0;
-        for (int w = 0; w < nty; ++w) mm = fmax(mm, wmax[w]);
-        tol_s = 1e-13 * mm;
+    for (int t = threadIdx.x; t < nc; t += blockDim.x) {
+        drop[t] = 0;
+        double cm = 0.0;
+        for (int i = 0; i < nc; ++i) cm = fmax(cm, fabs(Mg[(size_t)i * nc + t]));
+        ctol[t] = 1e-13 * cm;
     }
     __syncthreads();
     for (int k = 0; k < nc; ++k) {
@@ -548,7 +545,7 @@ __global__ void __launch_bounds__(1024) k_gj(int nc, double* Mg, double* Invg, V
                 }
             }
             if (tx == 0) {
-                piv_s = (bv > tol_s) ? bi : -1;
+                piv_s = (bv > ctol[k]) ? bi : -1;
                 if (piv_s < 0) drop[k] = 1;
             }
         }
@@ -1137,11 +1134,14 @@ int kcfd_amg_create(const kcfd_csr_t* A, const kcfd_amg_opts_t* opts, kcfd_amg**
     const size_t nc2 = (size_t)c.n * c.n;
     ok = alloc(h, (void**)&h->dense, nc2 * sizeof(double)) && alloc(h, (void**)&h->dinvm, nc2 * sizeof(double)) &&
          alloc(h, &h->cinv, nc2 * vs);
-    // the elimination in shared memory when the matrix and its inverse fit (nc <= 112)
-    if (ok && 2 * nc2 * sizeof(double) <= 200 * 1024) {
+    // the elimination in shared memory when the matrix and its inverse fit (nc <= 113).
+    // The launch limit is an attribute of the kernel, shared by every handle in the
+    // process, so it is always set to the same bound (a handle with a smaller coarsest
+    // level must not lower it under another's)
+    if (ok && 2 * nc2 * sizeof(double) <= (size_t)kGjSmemMax) {
         h->gj_smem = (int)(2 * nc2 * sizeof(double));
         const void* kf = h->mixed ? (const void*)k_gj<float> : (const void*)k_gj<double>;
-        if (cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, h->gj_smem) != cudaSuccess) {
+        if (cudaFuncSetAttribute(kf, cudaFuncAttributeMaxDynamicSharedMemorySize, kGjSmemMax) != cudaSuccess) {
             (void)cudaGetLastError();
             h->gj_smem = 0;
         }

@@ -166,8 +166,10 @@ def delaunay_tri_arrays(n_points, rng, dirichlet_name="dirichlet", wall_name="wa
 def delaunay_tet_arrays(box, n_target, rng, jitter=0.25):
     """Delaunay tetrahedra of a jittered lattice in box = (Lx, Ly, Lz).
 
-    The lattice spacing is chosen so that the tetrahedralisation has about n_target
-    cells (a Delaunay mesh of a jittered lattice has ~5.2-6 tets per point).
+    The lattice is chosen so that the tetrahedralisation has about n_target cells: a
+    Delaunay mesh of this jittered lattice has 6.35 tets per point (measured: 1,219,253
+    tets on 34 x 34 x 166 points), and the lattice counts follow the box's aspect, the
+    x count being the one whose predicted total is nearest n_target.
     Face node lists follow the reference's tet face order (_tet_faces in
     mesh/hybrid_mesh_generator.py:64-72); cells are ordered along a Morton curve.
     Boundary faces are the convex hull, tagged by face-centroid position: bottom
@@ -175,10 +177,15 @@ def delaunay_tet_arrays(box, n_target, rng, jitter=0.25):
     """
     from scipy.spatial import Delaunay
     Lx, Ly, Lz = box
-    vol = Lx * Ly * Lz
-    n_pts = n_target / 5.6
-    h = (vol / n_pts) ** (1.0 / 3.0)
-    nx, ny, nz = max(2, round(Lx / h)), max(2, round(Ly / h)), max(2, round(Lz / h))
+    best = None
+    for nx in range(2, 4096):
+        ny, nz = max(2, round(nx * Ly / Lx)), max(2, round(nx * Lz / Lx))
+        pred = 6.35 * (nx + 1) * (ny + 1) * (nz + 1)
+        if best is None or abs(pred - n_target) < best[0]:
+            best = (abs(pred - n_target), nx, ny, nz)
+        if pred > 2 * n_target:
+            break
+    _, nx, ny, nz = best
     k, j, i = np.meshgrid(np.arange(nz + 1), np.arange(ny + 1), np.arange(nx + 1), indexing="ij")
     sp = np.array([Lx / nx, Ly / ny, Lz / nz])
     pts = np.stack([i.reshape(-1) * sp[0], j.reshape(-1) * sp[1], k.reshape(-1) * sp[2]], axis=1)

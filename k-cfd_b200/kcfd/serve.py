@@ -70,8 +70,22 @@ def make_requests(count, rate, seed=0, n2d=(32, 512), n3d=(16, 96), re=(100.0, 1
     return out
 
 
-def footprint_bytes(ndim, N, precision="mixed"):
-    """Device bytes a resident case holds (mesh, two matrices, solver scratch, fields)."""
+AMG_MIN_CELLS = 32768   # precond_p "auto": multigrid p' above this many cells, ILU(0) below
+
+
+def p_precond_for(cells, precond_p):
+    """The p' preconditioner of a case: precond_p, or for "auto" the multigrid for cases
+    above AMG_MIN_CELLS cells (their p' solves run on the graph engine, where the
+    multigrid takes an order of magnitude fewer Krylov iterations than ILU(0)) and
+    ILU(0) for the small ones (one CTA each, so that concurrent cases overlap)."""
+    if precond_p != "auto":
+        return precond_p
+    return "amg" if cells > AMG_MIN_CELLS else "ilu0"
+
+
+def footprint_bytes(ndim, N, precision="mixed", precond_p="ilu0"):
+    """Device bytes a resident case holds (mesh, two matrices, solver scratch, fields;
+    a multigrid hierarchy at about 1.6 kB a cell, measured 3.3 GB at 128^3)."""
     n = N ** ndim
     F = ndim * n + ndim * N ** (ndim - 1)
     nnz = n + 2 * ndim * n
@@ -80,7 +94,8 @@ def footprint_bytes(ndim, N, precision="mixed"):
     vw = 4 if precision == "mixed" else 8
     solver = 9 * n * ndim * vw + 9 * n * vw + n * ndim * 8 + nnz * (8 + 4 + 4 + vw) + 4 * n * 8
     fields = n * (ndim * 4 + 8) * 8 + F * 8 + n * ndim * ndim * 8
-    return int(1.15 * (mesh + mats + solver + fields)) + (8 << 20)
+    amg = 1600 * n if p_precond_for(n, precond_p) == "amg" else 0
+    return int(1.15 * (mesh + mats + solver + fields + amg)) + (8 << 20)
 
 
 class Case:
@@ -104,8 +119,8 @@ class Case:
             # overlap on the device (0: the library's choice, best for one case alone);
             # the large ones take the grid-wide solvers either way
             team = small_team if m.n_cells * m.ndim <= 40000 else 0
-            s = SIMPLESolver(m, rho=1.0, mu=1.0 / req.Re, precision=precision, precond_p=precond_p, rtol=rtol,
-                             graph=graph, team=team)
+            s = SIMPLESolver(m, rho=1.0, mu=1.0 / req.Re, precision=precision,
+                             precond_p=p_precond_for(m.n_cells, precond_p), rtol=rtol, graph=graph, team=team)
             for nm in m.boundary_patches:
                 lid = [1.0] + [0.0] * (m.ndim - 1)
                 s.set_velocity_bc(nm, "dirichlet", lid if nm == "lid" else [0.0] * m.ndim)
@@ -203,7 +218,7 @@ class Server:
                     if self.policy == "sjf":
                         pick = min(range(len(queue)), key=lambda i: work_estimate(queue[i]))
                     r = queue[pick]
-                    fp = footprint_bytes(r.ndim, r.N, self.precision)
+                    fp = footprint_bytes(r.ndim, r.N, self.precision, self.precond_p)
                     if (active or building) and used + fp > self.budget:
                         break
                     queue.pop(pick)

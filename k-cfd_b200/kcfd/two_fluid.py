@@ -86,7 +86,11 @@ class _Field:
 
 
 class TwoFluidSolver:
-    def __init__(self, mesh, device="cuda", rtol=DIRECT_RTOL, maxiter=20000):
+    """p_precond: the pressure correction's preconditioner, 'ilu0' (as every other system)
+    or 'amg' (the device multigrid, on the graph engine); precision 'mixed' stores the
+    multigrid hierarchy in FP32 (the Krylov iteration and every other system stay FP64)."""
+
+    def __init__(self, mesh, device="cuda", rtol=DIRECT_RTOL, maxiter=20000, p_precond="ilu0", precision="fp64"):
         torch = _lib.require_cuda()
         if not isinstance(mesh, Mesh):
             mesh = from_fvmesh(mesh)
@@ -151,10 +155,18 @@ class TwoFluidSolver:
         levels = mesh.cell_color
         self._s1 = Solver(self._A, precond="ilu0", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels)
         self._sg = Solver(self._A, precond="ilu0", nrhs=nd, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels)
+        if p_precond == "amg":
+            self._sp = Solver(self._A, precond="amg", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter,
+                              mode=_lib.MODE_MIXED if precision == "mixed" else _lib.MODE_FP64)
+        elif p_precond == "ilu0":
+            self._sp = self._s1
+        else:
+            raise ValueError(f"unknown p' preconditioner {p_precond!r}")
         self._params = _lib.TfParams()
-        # Krylov iterations of the one-rhs and the ndim-rhs solves since the last
-        # reset (device counters, read by the caller when it wants them)
-        self.krylov = torch.zeros(2, dtype=torch.int64, device=device)
+        # Krylov iterations since the last reset of the one-rhs ILU(0) solves, the
+        # ndim-rhs solves and the multigrid p' solves (device counters, read by the
+        # caller when it wants them)
+        self.krylov = torch.zeros(3, dtype=torch.int64, device=device)
 
     # ---- set-up (models/two_fluid.py:97-165) ----
     def initialize(self, alpha_g_init=0.05):
@@ -295,7 +307,8 @@ class TwoFluidSolver:
     def _solve(self, solver, x, rhs):
         solver.setup(self._A)
         solver.solve(self._A, rhs, x)
-        self.krylov[0 if solver is self._s1 else 1] += solver.iters.max().to(self.krylov.dtype)
+        k = 1 if solver is self._sg else (2 if (solver is self._sp and solver is not self._s1) else 0)
+        self.krylov[k] += solver.iters.max().to(self.krylov.dtype)
 
     def _simple_iteration(self):
         self._sync_params()
@@ -441,7 +454,7 @@ class TwoFluidSolver:
             "pressure_assemble")
         pp = self._x[:n]
         pp.zero_()
-        self._solve(self._s1, pp, self._rhs[:n])
+        self._solve(self._sp, pp, self._rhs[:n])
         chk(L.kcfd_tf_guard(n, P(pp), None, 2, 0.0, 0.0, P(self._flag), st), "guard")
         chk(L.kcfd_tf_correct(dmd, self.alpha_p, P(pp), P(f["alpha_l"]), P(f["alpha_g"]), P(self._aP_l),
                               P(self._aP_g), P(self._grad), P(f["U_l"]), P(f["U_g"]), P(f["p"]), st), "correct")

@@ -136,17 +136,19 @@ def prolongator(A, agg, na, omega):
 
 def dense_inverse(M):
     """Gauss-Jordan inverse with partial pivoting (largest |entry| of the column, the
-    first row on ties). A pivot not above 1e-13 of the largest |entry| drops its
-    unknown: that row and column of the inverse are set to zero."""
+    first row on ties). A pivot not above 1e-13 of the largest |entry| of its column in
+    the matrix before elimination drops its unknown: that row and column of the inverse
+    are set to zero (per column, so that a row pinned by a huge diagonal does not drop
+    the others)."""
     M = np.array(M, dtype=np.float64)
     n = M.shape[0]
     inv = np.eye(n)
-    tol = 1e-13 * (np.abs(M).max() if n else 0.0)
+    tol = 1e-13 * (np.abs(M).max(axis=0) if n else np.zeros(0))
     drop = np.zeros(n, dtype=bool)
     for k in range(n):
         col = np.abs(M[k:, k])
         p = k + int(np.argmax(col))
-        if col[p - k] <= tol:
+        if col[p - k] <= tol[k]:
             drop[k] = True
             continue
         if p != k:

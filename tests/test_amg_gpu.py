@@ -176,3 +176,27 @@ def test_solve_linear_system_amg():
     x = solve_linear_system(FVMSystem.from_csr(A, b), None, "bicgstab", 0.0, 1000, "b200", "amg", rtol=1e-10,
                             max_levels=10, max_coarse=500)
     assert _rel(x, xd) < 1e-8
+
+
+def test_two_hierarchies_interleaved(systems):
+    """Handles whose coarsest levels differ in size (their dense inverses use different
+    amounts of shared memory) are set up and applied in turn: each keeps its results."""
+    import torch
+    from kcfd.amg import AMG
+    from kcfd.solver import DeviceCSR
+    out = {}
+    hs = {}
+    for name in ("pp16", "c16_80"):
+        A, b = systems[name]
+        d = DeviceCSR.from_scipy(A)
+        hs[name] = (AMG(d), d, torch.from_numpy(b).cuda())
+    sizes = {k: h.info()["rows"][-1] for k, (h, d, b) in hs.items()}
+    assert sizes["pp16"] != sizes["c16_80"]
+    for rep in range(2):
+        for name, (h, d, b) in hs.items():
+            h.setup(d)
+            x = h.apply(b).cpu().numpy()
+            if rep == 0:
+                out[name] = x
+            else:
+                np.testing.assert_array_equal(x, out[name])

@@ -77,6 +77,11 @@ def test_dense_inverse():
     S[:, 5] = 0.0
     inv = amg.dense_inverse(S)
     assert np.all(np.isfinite(inv))
+    # one row pinned by a huge diagonal (the two-fluid pressure correction's pin) drops
+    # nothing: the tolerance is per column
+    P = M * 1e-4
+    P[0, 0] += 1e10
+    np.testing.assert_allclose(amg.dense_inverse(P) @ P, np.eye(40), rtol=0, atol=1e-9)
 
 
 def test_power_omega_close_to_converged_estimate():

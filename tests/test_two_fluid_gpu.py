@@ -19,13 +19,13 @@ def _rel(a, b):
     return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-300))
 
 
-def _device_solver(tag, seed):
+def _device_solver(tag, seed, **kw):
     from kcfd import mesh as km
     from kcfd.two_fluid import TwoFluidSolver
     d = load_golden("mesh_" + tag)
     nodes, cells, bdict, cfl = golden_inputs(d)
     m = km.build_mesh(nodes, cells, bdict, ndim=int(d["ndim"]), cell_face_node_list=cfl)
-    sv = TwoFluidSolver(m)
+    sv = TwoFluidSolver(m, **kw)
 
     def set_field(name, arr):
         getattr(sv, name).values = arr
@@ -34,10 +34,11 @@ def _device_solver(tag, seed):
     return sv
 
 
+@pytest.mark.parametrize("p_precond", ["ilu0", "amg"])
 @pytest.mark.parametrize("tag,seed", CASES)
-def test_two_fluid_matches_reference(tag, seed):
+def test_two_fluid_matches_reference(tag, seed, p_precond):
     g = load_golden("two_fluid")
-    sv = _device_solver(tag, seed)
+    sv = _device_solver(tag, seed, p_precond=p_precond)
     np.testing.assert_array_equal(sv.alpha_g.values, g[f"{tag}_init_alpha_g"])
     for step in range(3):
         res = sv.step()
@@ -83,3 +84,16 @@ def test_two_fluid_adaptive_dt_follows_the_reference_loop():
     assert dts[0] != 1e-3
     for f in FIELDS:
         np.testing.assert_array_equal(getattr(sv, f).values, getattr(ref, f).values)
+
+
+@pytest.mark.parametrize("tag,seed", CASES)
+def test_two_fluid_mixed_field_errors(tag, seed):
+    """The mixed form (the multigrid p' hierarchy in FP32) against FP64 with the same
+    multigrid, 3 steps: alpha_g, U_l, U_g, p, T_l, T_g each within 1e-6 relative L2."""
+    a = _device_solver(tag, seed, p_precond="amg")
+    b = _device_solver(tag, seed, p_precond="amg", precision="mixed")
+    for _ in range(3):
+        a.step()
+        b.step()
+    for f in FIELDS:
+        assert _rel(getattr(b, f).values, getattr(a, f).values) < 1e-6, f

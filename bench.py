@@ -1081,9 +1081,12 @@ def run_c3(args):
         errs = {k2: float(np.linalg.norm(getattr(sm, k2).values - v) / max(np.linalg.norm(v), 1e-300))
                 for k2, v in ref.items()}
         mixed = {"value": round(ncmp / tm, 4), "unit": "steps/s", "steps": ncmp, "field_error": errs,
-                 "desc": "the same workload with the multigrid p' hierarchy stored in FP32 (FP64 Krylov iteration "
-                         "and every other system FP64); field_error = relative L2 against the FP64 run after the "
-                         "same steps from the same initial state (alpha_g, U_l, U_g, p, T_l, T_g), over the "
+                 "desc": "the same workload in the mixed form: the momentum, volume-fraction and energy systems "
+                         "(ILU(0)) on the graph engine's FP32 form (FP32 vectors and values, FP64 iterate, residual "
+                         "replacement against the FP64 matrix, the same 1e-12 FP64 stopping test), the multigrid p' "
+                         "hierarchy stored in FP32 under an FP64 Krylov iteration; wall time of the steps with a "
+                         "device synchronize on both sides; field_error = relative L2 against the FP64 run after "
+                         "the same steps from the same initial state (alpha_g, U_l, U_g, p, T_l, T_g), over the "
                          "steps before the model's residual passes 1e3"}
     cpu = None
     if not args.no_cpu:

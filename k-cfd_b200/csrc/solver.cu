@@ -1265,8 +1265,12 @@ struct kcfd_solver {
         int eager = 0;                     // host-driven loop instead of the graph
         bool pdl = true;                   // phase kernels with programmatic dependent launch
         bool ready = false;                // args (and graph) built
+        int mix = 0;                       // MIXED: FP32 vectors and values, FP64 x, b and residuals
         ge::Args args;
+        ge::ArgsT<float> args32;           // MIXED
         ge::Sell A, L, U;                  // sliced-ELL copies (L, U: ILU only)
+        ge::SellT<float> A32{}, L32{}, U32{};  // MIXED: FP32 values on the same slots
+        float* vec32 = nullptr;            // MIXED: the 7 Krylov vectors
         int* srcA = nullptr;               // per slot: index into the caller's values, -1 padding
         int* srcL = nullptr;               // per slot: index into the permuted CSR (lu), -1 padding
         int* srcU = nullptr;
@@ -1307,7 +1311,8 @@ int free_solver(kcfd_solver* s) {
         void* gp[] = {s->g.st, s->g.part, s->g.cnt, gx, gb, s->g.vec, s->g.res_i, s->g.res_d,
                       (void*)s->g.A.off, (void*)s->g.A.col, (void*)s->g.A.val, (void*)s->g.L.off, (void*)s->g.L.col,
                       (void*)s->g.L.val, (void*)s->g.U.off, (void*)s->g.U.col, (void*)s->g.U.val,
-                      s->g.srcA, s->g.srcL, s->g.srcU};
+                      s->g.srcA, s->g.srcL, s->g.srcU, (void*)s->g.A32.val, (void*)s->g.L32.val,
+                      (void*)s->g.U32.val, (void*)s->g.vec32};
         for (void* p : gp)
             if (p) cudaFree(p);
     }
@@ -1435,10 +1440,10 @@ int ge_fill_grid(const kcfd_solver* s, int64_t m) {
 // Grid of each phase kernel: its own occupancy on every SM, capped by the rows it has
 // (a vector kernel takes Ilp::U rows per thread and step) and by the partial slots.
 struct GeGrid {
-    int init, p, fwd, bwd, sv, s, st, xr;
+    int init, p, fwd, bwd, sv, s, st, xr, rr;
 };
 
-template <int NRHS, int PREC>
+template <int NRHS, int PREC, typename T>
 GeGrid ge_grids(int n, int sms, int gmax) {
     auto g = [&](const void* f, int rows_per_thread) {
         int occ = 0;
@@ -1449,14 +1454,15 @@ GeGrid ge_grids(int n, int sms, int gmax) {
     };
     constexpr int U = ge::Ilp<NRHS>::U;
     GeGrid r;
-    r.init = g((const void*)ge::g_init<NRHS>, 1);
-    r.p = g((const void*)ge::g_p<NRHS, PREC>, U);
-    r.fwd = g((const void*)ge::g_fwd<NRHS>, 1);
-    r.bwd = g((const void*)ge::g_bwd<NRHS>, 1);
-    r.sv = g((const void*)ge::g_spmv_v<NRHS, PREC>, 1);
-    r.s = g((const void*)ge::g_s<NRHS, PREC>, U);
-    r.st = g((const void*)ge::g_spmv_t<NRHS, PREC>, 1);
-    r.xr = g((const void*)ge::g_xr<NRHS, PREC>, NRHS == 1 ? 2 : U);  // g_xr's rows per thread
+    r.init = g((const void*)ge::g_init<NRHS, T>, 1);
+    r.p = g((const void*)ge::g_p<NRHS, PREC, T>, U);
+    r.fwd = g((const void*)ge::g_fwd<NRHS, T>, 1);
+    r.bwd = g((const void*)ge::g_bwd<NRHS, T>, 1);
+    r.sv = g((const void*)ge::g_spmv_v<NRHS, PREC, T>, 1);
+    r.s = g((const void*)ge::g_s<NRHS, PREC, T>, U);
+    r.st = g((const void*)ge::g_spmv_t<NRHS, PREC, T>, 1);
+    r.xr = g((const void*)ge::g_xr<NRHS, PREC, T>, NRHS == 1 ? 2 : U);  // g_xr's rows per thread
+    r.rr = ge::is_mixed<T>() ? g((const void*)ge::g_rr<NRHS, PREC, T>, 1) : 0;
     return r;
 }
 
@@ -1477,38 +1483,56 @@ void ge_launch(void (*k)(KArgs...), int grid, cudaStream_t cs, bool pdl, Act&&..
 }
 
 // One loop trip: the phase kernels of one BiCGSTAB iteration.
-template <int NRHS, int PREC>
-void ge_body(const ge::Args& a, const GeGrid& G, cudaStream_t cs, bool pdl) {
-    ge_launch(ge::g_p<NRHS, PREC>, G.p, cs, pdl, a);
+template <int NRHS, int PREC, typename T>
+void ge_body(const ge::ArgsT<T>& a, const GeGrid& G, cudaStream_t cs, bool pdl) {
+    ge_launch(ge::g_p<NRHS, PREC, T>, G.p, cs, pdl, a);
     auto sweeps = [&](int which) {
-        if (PREC == KCFD_PREC_AMG) {
+        if constexpr (PREC == KCFD_PREC_AMG && !ge::is_mixed<T>()) {
             // phat = M^-1 p, shat = M^-1 s: one V-cycle each, skipped once the loop flag drops
             amg::vcycle((const kcfd_amg*)a.amg, which ? a.r : a.p, which ? a.sh : a.ph, &a.st->active, cs, pdl);
             return;
         }
         if (PREC != KCFD_PREC_ILU0) return;
         if (a.nlev == 1) {
-            ge_launch(ge::g_bwd<NRHS>, G.bwd, cs, pdl, a, 0, which);
+            ge_launch(ge::g_bwd<NRHS, T>, G.bwd, cs, pdl, a, 0, which);
             return;
         }
-        for (int l = 1; l < a.nlev; ++l) ge_launch(ge::g_fwd<NRHS>, G.fwd, cs, pdl, a, l, which);
-        for (int l = a.nlev - 2; l >= 0; --l) ge_launch(ge::g_bwd<NRHS>, G.bwd, cs, pdl, a, l, which);
+        for (int l = 1; l < a.nlev; ++l) ge_launch(ge::g_fwd<NRHS, T>, G.fwd, cs, pdl, a, l, which);
+        for (int l = a.nlev - 2; l >= 0; --l) ge_launch(ge::g_bwd<NRHS, T>, G.bwd, cs, pdl, a, l, which);
     };
     sweeps(0);
-    ge_launch(ge::g_spmv_v<NRHS, PREC>, G.sv, cs, pdl, a);
-    ge_launch(ge::g_s<NRHS, PREC>, G.s, cs, pdl, a);
+    ge_launch(ge::g_spmv_v<NRHS, PREC, T>, G.sv, cs, pdl, a);
+    ge_launch(ge::g_s<NRHS, PREC, T>, G.s, cs, pdl, a);
     sweeps(1);
-    ge_launch(ge::g_spmv_t<NRHS, PREC>, G.st, cs, pdl, a);
-    ge_launch(ge::g_xr<NRHS, PREC>, G.xr, cs, pdl, a);
+    ge_launch(ge::g_spmv_t<NRHS, PREC, T>, G.st, cs, pdl, a);
+    ge_launch(ge::g_xr<NRHS, PREC, T>, G.xr, cs, pdl, a);
+    if constexpr (ge::is_mixed<T>()) ge_launch(ge::g_rr<NRHS, PREC, T>, G.rr, cs, pdl, a);
+}
+
+// The engine's arguments of this storage type.
+template <typename T>
+ge::ArgsT<T>& ge_args(kcfd_solver* s);
+template <>
+ge::ArgsT<double>& ge_args<double>(kcfd_solver* s) { return s->g.args; }
+template <>
+ge::ArgsT<float>& ge_args<float>(kcfd_solver* s) { return s->g.args32; }
+
+// Value fills at the head of every solve: the caller's FP64 values into the SELL
+// copy of A, and (MIXED) its FP32 difference form.
+template <typename T>
+void ge_fill_values(kcfd_solver* s, const double* vals, cudaStream_t st) {
+    ge::g_fill<double, double><<<ge_fill_grid(s, s->g.slotsA), 256, 0, st>>>(s->g.slotsA, s->g.srcA, vals, s->g.A.val);
+    if constexpr (ge::is_mixed<T>())
+        ge::g_diff32<<<ge_fill_grid(s, s->n), 256, 0, st>>>(s->n, s->g.A, s->g.A32.val);
 }
 
 // Eager form: init, body trips in chunks with a host read of the active flag, final.
-template <int NRHS, int PREC>
+template <int NRHS, int PREC, typename T>
 int ge_eager(kcfd_solver* s, cudaStream_t st) {
-    const ge::Args& a = s->g.args;
-    const GeGrid G = ge_grids<NRHS, PREC>(s->n, s->sm_count, s->g.gmax);
-    ge::g_fill<<<ge_fill_grid(s, s->g.slotsA), 256, 0, st>>>(s->g.slotsA, s->g.srcA, s->g.vals_key, s->g.A.val);
-    ge::g_init<NRHS><<<G.init, ge::kBlock, 0, st>>>(a);
+    const ge::ArgsT<T>& a = ge_args<T>(s);
+    const GeGrid G = ge_grids<NRHS, PREC, T>(s->n, s->sm_count, s->g.gmax);
+    ge_fill_values<T>(s, s->g.vals_key, st);
+    ge::g_init<NRHS, T><<<G.init, ge::kBlock, 0, st>>>(a);
     KCFD_CUDA(cudaGetLastError());
     constexpr int kChunk = 8;
     for (int trips = 0; trips <= a.maxiter + 2; trips += kChunk) {
@@ -1516,19 +1540,20 @@ int ge_eager(kcfd_solver* s, cudaStream_t st) {
         KCFD_CUDA(cudaMemcpyAsync(&active, &a.st->active, sizeof(int), cudaMemcpyDeviceToHost, st));
         KCFD_CUDA(cudaStreamSynchronize(st));
         if (!active) break;
-        for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC>(a, G, st, s->g.pdl);
+        for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC, T>(a, G, st, s->g.pdl);
         KCFD_CUDA(cudaGetLastError());
     }
-    ge::g_final<NRHS><<<ge_fill_grid(s, s->n), 256, 0, st>>>(a);
+    ge::g_final<NRHS, T><<<ge_fill_grid(s, s->n), 256, 0, st>>>(a);
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;
 }
 
-template <int NRHS, int PREC>
+template <int NRHS, int PREC, typename T>
 int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     auto& g = s->g;
     const int n = s->n;
-    ge::Args a;
+    constexpr bool mix = ge::is_mixed<T>();
+    ge::ArgsT<T> a;
     std::memset(&a, 0, sizeof(a));
     a.n = n;
     a.nlev = s->nlev;
@@ -1538,15 +1563,24 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     a.rtol = s->o.rtol;
     a.atol = s->o.atol;
     a.lev = s->lev_ptr;
-    a.A = g.A;
-    a.L = g.L;
-    a.U = g.U;
-    a.dinv = (const double*)s->dinv;
-    a.ldi = (const double*)s->ludinv;
+    if constexpr (mix) {
+        a.A = g.A32;
+        a.L = g.L32;
+        a.U = g.U32;
+    } else {
+        a.A = g.A;
+        a.L = g.L;
+        a.U = g.U;
+    }
+    a.A64 = g.A;
+    a.dinv = (const T*)s->dinv;
+    a.ldi = (const T*)s->ludinv;
     const size_t len = (size_t)n * NRHS;
     a.x = g.gx;
     a.b = g.gb;
-    double* v = g.vec;
+    T* v;
+    if constexpr (mix) v = g.vec32;
+    else v = g.vec;
     a.r = v; a.rh = v + len; a.p = v + 2 * len; a.v = v + 3 * len; a.t = v + 4 * len; a.ph = v + 5 * len;
     a.sh = v + 6 * len;
     a.st = g.st;
@@ -1564,8 +1598,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     g.ready = false;
     if (g.eager) {
         // no graph: the host loop launches the same kernels (ge_eager)
-        g.args = a;
-        g.vals_key = A->vals64;
+        ge_args<T>(s) = a;
         g.vals_key = A->vals64;
         g.ready = true;
         return KCFD_OK;
@@ -1574,8 +1607,8 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     cudaGraphConditionalHandle cond;
     KCFD_CUDA(cudaGraphConditionalHandleCreate(&cond, g.graph, 1, cudaGraphCondAssignDefault));
     a.cond = cond;
-    g.args = a;
-    const GeGrid G = ge_grids<NRHS, PREC>(n, s->sm_count, g.gmax);
+    ge_args<T>(s) = a;
+    const GeGrid G = ge_grids<NRHS, PREC, T>(n, s->sm_count, g.gmax);
     // node 1: the caller's values into the SELL copy (the graph holds their pointer)
     int64_t f_m = g.slotsA;
     const int* f_src = g.srcA;
@@ -1584,16 +1617,32 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     void* fargs[] = {&f_m, &f_src, &f_in, &f_out};
     cudaKernelNodeParams kf;
     std::memset(&kf, 0, sizeof(kf));
-    kf.func = (void*)ge::g_fill;
+    kf.func = (void*)ge::g_fill<double, double>;
     kf.gridDim = dim3(ge_fill_grid(s, g.slotsA));
     kf.blockDim = dim3(256);
     kf.kernelParams = fargs;
     cudaGraphNode_t n_fill, n_init, n_cond, n_fin;
     KCFD_CUDA(cudaGraphAddKernelNode(&n_fill, g.graph, nullptr, 0, &kf));
+    if constexpr (mix) {
+        // MIXED: the FP32 difference form of the values just filled
+        int d_n = n;
+        ge::Sell d_a = g.A;
+        float* d_out = g.A32.val;
+        void* dargs[] = {&d_n, &d_a, &d_out};
+        cudaKernelNodeParams kd;
+        std::memset(&kd, 0, sizeof(kd));
+        kd.func = (void*)ge::g_diff32;
+        kd.gridDim = dim3(ge_fill_grid(s, n));
+        kd.blockDim = dim3(256);
+        kd.kernelParams = dargs;
+        cudaGraphNode_t n_diff;
+        KCFD_CUDA(cudaGraphAddKernelNode(&n_diff, g.graph, &n_fill, 1, &kd));
+        n_fill = n_diff;
+    }
     void* args[] = {&a};
     cudaKernelNodeParams kp;
     std::memset(&kp, 0, sizeof(kp));
-    kp.func = (void*)ge::g_init<NRHS>;
+    kp.func = (void*)ge::g_init<NRHS, T>;
     kp.gridDim = dim3(G.init);
     kp.blockDim = dim3(ge::kBlock);
     kp.kernelParams = args;
@@ -1611,7 +1660,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     KCFD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        ge_body<NRHS, PREC>(a, G, cs, g.pdl);
+        ge_body<NRHS, PREC, T>(a, G, cs, g.pdl);
         cudaGraph_t outg = nullptr;
         const cudaError_t e2 = cudaStreamEndCapture(cs, &outg);
         if (e == cudaSuccess) e = e2;
@@ -1619,7 +1668,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     const cudaError_t e3 = cudaStreamDestroy(cs);
     KCFD_CUDA(e3);
     if (e == cudaSuccess) {
-        kp.func = (void*)ge::g_final<NRHS>;
+        kp.func = (void*)ge::g_final<NRHS, T>;
         kp.gridDim = dim3(ge_fill_grid(s, n));
         kp.blockDim = dim3(256);
         e = cudaGraphAddKernelNode(&n_fin, g.graph, &n_cond, 1, &kp);
@@ -1633,7 +1682,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
         g.exec = nullptr;
         g.graph = nullptr;
         g.pdl = false;
-        return ge_build<NRHS, PREC>(s, A);
+        return ge_build<NRHS, PREC, T>(s, A);
     }
     KCFD_CUDA(e);
     g.vals_key = A->vals64;
@@ -1642,25 +1691,31 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
 }
 
 // Run-time (nrhs, precond) -> template instance.
-template <template <int, int> class F, typename... Ts>
+template <template <int, int, typename> class F, typename... Ts>
 int ge_dispatch(const kcfd_solver* s, Ts... args) {
     const int r = s->o.nrhs, p = s->o.precond;
+    const bool m = s->g.mix != 0;
 #define GE_CASE(R, P) \
-    if (r == R && p == P) return F<R, P>::run(args...);
+    if (r == R && p == P && !m) return F<R, P, double>::run(args...);
+#define GE_CASE_MIX(R, P) \
+    if (r == R && p == P && m) return F<R, P, float>::run(args...);
     GE_CASE(1, 0) GE_CASE(1, 1) GE_CASE(1, 2) GE_CASE(2, 0) GE_CASE(2, 1) GE_CASE(2, 2)
     GE_CASE(3, 0) GE_CASE(3, 1) GE_CASE(3, 2) GE_CASE(1, 3)
+    GE_CASE_MIX(1, 0) GE_CASE_MIX(1, 1) GE_CASE_MIX(1, 2) GE_CASE_MIX(2, 0) GE_CASE_MIX(2, 1) GE_CASE_MIX(2, 2)
+    GE_CASE_MIX(3, 0) GE_CASE_MIX(3, 1) GE_CASE_MIX(3, 2)
 #undef GE_CASE
-    set_error("graph engine: unsupported configuration (nrhs %d, precond %d)", r, p);
+#undef GE_CASE_MIX
+    set_error("graph engine: unsupported configuration (nrhs %d, precond %d, mixed %d)", r, p, (int)m);
     return KCFD_BAD_INPUT;
 }
 
-template <int R, int P>
+template <int R, int P, typename T>
 struct GeBuild {
-    static int run(kcfd_solver* s, const kcfd_csr_t* A) { return ge_build<R, P>(s, A); }
+    static int run(kcfd_solver* s, const kcfd_csr_t* A) { return ge_build<R, P, T>(s, A); }
 };
-template <int R, int P>
+template <int R, int P, typename T>
 struct GeEager {
-    static int run(kcfd_solver* s, cudaStream_t st) { return ge_eager<R, P>(s, st); }
+    static int run(kcfd_solver* s, cudaStream_t st) { return ge_eager<R, P, T>(s, st); }
 };
 
 // Host SELL-32 of rows [0, n): row i's entries are [rb(i), re(i)) of a CSR with
@@ -1695,10 +1750,17 @@ bool make_sell(int n, RB rb, RE re, const std::vector<int>& col, const std::vect
     return true;
 }
 
-bool upload_sell(const SellHost& h, ge::Sell& d, int** src, int64_t& slots) {
+bool upload_sell(const SellHost& h, ge::Sell& d, int** src, int64_t& slots, ge::SellT<float>* d32) {
     slots = (int64_t)h.col.size();
-    return upload(&d.off, h.off) && upload(&d.col, h.col) && upload(src, h.src) &&
-           cudaMalloc(&d.val, std::max<int64_t>(slots, 1) * sizeof(double)) == cudaSuccess;
+    bool ok = upload(&d.off, h.off) && upload(&d.col, h.col) && upload(src, h.src) &&
+              cudaMalloc(&d.val, std::max<int64_t>(slots, 1) * sizeof(double)) == cudaSuccess;
+    if (ok && d32) {
+        // MIXED: FP32 values on the same slots
+        d32->off = d.off;
+        d32->col = d.col;
+        ok = cudaMalloc(&d32->val, std::max<int64_t>(slots, 1) * sizeof(float)) == cudaSuccess;
+    }
+    return ok;
 }
 
 // The engine's SELL copies: A from the rows (rowptr, cols; src maps an entry to the
@@ -1709,14 +1771,15 @@ int ge_build_sell(kcfd_solver* s, const std::vector<int>& rowptr, const std::vec
     auto& g = s->g;
     const int n = s->n;
     SellHost h;
+    const bool m = g.mix != 0;
     bool ok = make_sell(n, [&](int i) { return rowptr[i]; }, [&](int i) { return rowptr[i + 1]; }, cols, src, h) &&
-              upload_sell(h, g.A, &g.srcA, g.slotsA);
+              upload_sell(h, g.A, &g.srcA, g.slotsA, m ? &g.A32 : nullptr);
     if (ok && !diag.empty()) {
         const std::vector<int> none;
         ok = make_sell(n, [&](int i) { return rowptr[i]; }, [&](int i) { return diag[i]; }, cols, none, h) &&
-             upload_sell(h, g.L, &g.srcL, g.slotsL);
+             upload_sell(h, g.L, &g.srcL, g.slotsL, m ? &g.L32 : nullptr);
         ok = ok && make_sell(n, [&](int i) { return diag[i] + 1; }, [&](int i) { return rowptr[i + 1]; }, cols, none, h) &&
-             upload_sell(h, g.U, &g.srcU, g.slotsU);
+             upload_sell(h, g.U, &g.srcU, g.slotsU, m ? &g.U32 : nullptr);
     }
     if (!ok) {
         set_error("graph engine: sliced-ELL copy too large or device allocation failed");
@@ -1730,9 +1793,10 @@ int ge_alloc(kcfd_solver* s) {
     const size_t len = (size_t)s->n * s->o.nrhs;
     g.gmax = s->sm_count * 8;  // 256-thread blocks: at most 8 resident per SM
     bool ok = cudaMalloc(&g.st, sizeof(ge::St)) == cudaSuccess &&
-              cudaMalloc(&g.part, (size_t)ge::kSlotsG * 8 * g.gmax * sizeof(double)) == cudaSuccess &&
+              cudaMalloc(&g.part, (size_t)ge::kSlotsG * ge::kSlotK * g.gmax * sizeof(double)) == cudaSuccess &&
               cudaMalloc(&g.cnt, ge::kSlotsG * sizeof(unsigned)) == cudaSuccess &&
-              cudaMalloc(&g.vec, 7 * len * sizeof(double)) == cudaSuccess &&
+              (g.mix ? cudaMalloc(&g.vec32, 7 * len * sizeof(float)) : cudaMalloc(&g.vec, 7 * len * sizeof(double))) ==
+                  cudaSuccess &&
               cudaMalloc(&g.res_i, 6 * sizeof(int)) == cudaSuccess && cudaMalloc(&g.res_d, 3 * sizeof(double)) == cudaSuccess;
     if (ok) {
         if (s->perm) {
@@ -1928,6 +1992,14 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         if (ip[i + 1] < ip[i]) return fail("kcfd_solver_create: indptr not monotone at row %d", i);
     for (int k = 0; k < nnz; ++k)
         if (ix[k] < 0 || ix[k] >= n) return fail("kcfd_solver_create: column index %d out of range at %d", ix[k], k);
+    if (mixed) {
+        // the FP32 difference form keeps each row's sum on its stored diagonal entry
+        for (int i = 0; i < n; ++i) {
+            bool has = false;
+            for (int k = ip[i]; k < ip[i + 1] && !has; ++k) has = ix[k] == i;
+            if (!has) return fail("kcfd_solver_create: MIXED mode needs a stored diagonal entry in every row (row %d)", i);
+        }
+    }
     // team and launch shape
     // auto: one CTA for tiny systems; the persistent grid kernel up to 40,000 unknowns
     // (and for every mixed solve); the graph engine for large FP64 systems. Measured on
@@ -1937,12 +2009,16 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     int team = amg ? 3 : opts->team;
     if (team == 0) {
         const int64_t unk = (int64_t)n * nrhs;
+        // MIXED stays on the persistent kernel (FP32 inner iterations, FP64 refinement
+        // with revert): the engine's MIXED form (team 3, asked for explicitly) keeps the
+        // Krylov space across residual replacements, which diverges on near-singular
+        // operators such as a pinned pressure correction at 128^3
         team = (unk <= 1024) ? 1 : ((mixed || unk <= 40000) ? 2 : 3);
     }
     if (team < 1 || team > 3) return fail("kcfd_solver_create: team must be 0..3");
-    if (team == 3 && mixed) return fail("kcfd_solver_create: the graph engine (team 3) runs FP64 only");
     s->team = team;
     if (team == 3) {
+        s->g.mix = mixed ? 1 : 0;
         const char* ev = std::getenv("KCFD_ENGINE_EAGER");
         s->g.eager = (ev && ev[0] == '1') ? 1 : 0;
         const char* pv = std::getenv("KCFD_ENGINE_PDL");
@@ -2182,9 +2258,15 @@ int kcfd_solver_setup(kcfd_solver* s, const kcfd_csr_t* A, void* stream) {
         if (int e = launch_team(s, k, args, st)) return e;
         if (s->team == 3) {
             // the factor's strict lower / upper parts into the engine's SELL copies
-            const double* lu = (const double*)s->lu;
-            ge::g_fill<<<ge_fill_grid(s, s->g.slotsL), 256, 0, st>>>(s->g.slotsL, s->g.srcL, lu, s->g.L.val);
-            ge::g_fill<<<ge_fill_grid(s, s->g.slotsU), 256, 0, st>>>(s->g.slotsU, s->g.srcU, lu, s->g.U.val);
+            if (mixed) {
+                const float* lu = (const float*)s->lu;
+                ge::g_fill<float, float><<<ge_fill_grid(s, s->g.slotsL), 256, 0, st>>>(s->g.slotsL, s->g.srcL, lu, s->g.L32.val);
+                ge::g_fill<float, float><<<ge_fill_grid(s, s->g.slotsU), 256, 0, st>>>(s->g.slotsU, s->g.srcU, lu, s->g.U32.val);
+            } else {
+                const double* lu = (const double*)s->lu;
+                ge::g_fill<double, double><<<ge_fill_grid(s, s->g.slotsL), 256, 0, st>>>(s->g.slotsL, s->g.srcL, lu, s->g.L.val);
+                ge::g_fill<double, double><<<ge_fill_grid(s, s->g.slotsU), 256, 0, st>>>(s->g.slotsU, s->g.srcU, lu, s->g.U.val);
+            }
             KCFD_CUDA(cudaGetLastError());
         }
         return KCFD_OK;

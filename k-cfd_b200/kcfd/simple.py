@@ -16,7 +16,12 @@ CUDA graph and replayed.
 Linear solves: the reference calls spsolve; here BiCGSTAB runs to a relative
 residual `rtol` (1e-8 by default) from the current field (momentum) or zero (p').
 precision='mixed' keeps FP64 assembly values for the outer residual and an FP32
-copy (written by the same kernels) for the inner iterations.
+copy (written by the same kernels) for the inner iterations. On large meshes the
+momentum solve runs the graph engine's FP32 form (FP32 vectors and values, FP64
+iterate, residual replacement against the FP64 matrix); the p' solve keeps an FP64
+Krylov iteration over an FP32 multigrid hierarchy with precond_p='amg'; with ILU(0)
+or Jacobi it runs FP32 inner iterations with FP64 refinement up to 40,000 cells and
+FP64 above (FP32 inner iterations cannot resolve the pinned p' operator there).
 """
 from __future__ import annotations
 
@@ -96,12 +101,21 @@ class SIMPLESolver:
                              torch.zeros(nnz, dtype=torch.float32, device=device) if mixed else None)
         self.A_p = DeviceCSR(ip, ix, torch.zeros(nnz, **f64),
                              torch.zeros(nnz, dtype=torch.float32, device=device) if mixed else None)
+        # mixed momentum solves on large meshes: the graph engine's FP32 form (residual
+        # replacement against the FP64 matrix; these systems are well conditioned)
+        team_m = team if team else (3 if (mixed and n * D > 40000) else 0)
         self.s_m = Solver(self.A_m, precond="jacobi", mode=self.mode, nrhs=D, maxiter=maxiter, rtol=rtol,
-                          team=team, lanes=lanes, inner_rtol=inner_rtol, inner_maxiter=inner_maxiter)
+                          team=team_m, lanes=lanes, inner_rtol=inner_rtol, inner_maxiter=inner_maxiter)
         levels = None
         if precond_p == "ilu0":
             levels = mesh.cell_color if ilu_order == "color" else mesh.level_natural
-        self.s_p = Solver(self.A_p, precond=precond_p, mode=self.mode, nrhs=1, maxiter=maxiter, rtol=rtol,
+        # p' in the mixed form: an FP32 multigrid hierarchy under an FP64 Krylov iteration
+        # ('amg'); FP32 inner iterations with FP64 refinement up to 40,000 cells; FP64
+        # above, where the FP32 inner iterations cannot resolve the pinned operator
+        # (measured: BREAKDOWN on a 256^2 cavity, and divergence of the engine's FP32
+        # recursion on the 128^3 cavity, with ILU(0) and with Jacobi)
+        mode_p = self.mode if (precond_p == "amg" or n <= 40000) else _lib.MODE_FP64
+        self.s_p = Solver(self.A_p, precond=precond_p, mode=mode_p, nrhs=1, maxiter=maxiter, rtol=rtol,
                           team=team, lanes=lanes, inner_rtol=inner_rtol, inner_maxiter=inner_maxiter, levels=levels)
         self.U = _Field(self, "U_t")
         self.p = _Field(self, "p_t")

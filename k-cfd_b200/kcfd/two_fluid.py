@@ -87,8 +87,13 @@ class _Field:
 
 class TwoFluidSolver:
     """p_precond: the pressure correction's preconditioner, 'ilu0' (as every other system)
-    or 'amg' (the device multigrid, on the graph engine); precision 'mixed' stores the
-    multigrid hierarchy in FP32 (the Krylov iteration and every other system stay FP64)."""
+    or 'amg' (the device multigrid, on the graph engine). precision 'mixed': the ILU(0)
+    systems (momentum, volume fraction, energy, and p' with 'ilu0') run BiCGSTAB with
+    FP32 vectors and values and FP64 residuals, iterate and stopping test (the graph
+    engine's residual-replacement form on large meshes, FP32 inner iterations with FP64
+    refinement on small ones); the multigrid p' keeps an FP64 Krylov iteration over an
+    FP32 hierarchy, and an ILU(0) p' on a large mesh stays FP64. Every system still
+    stops on its FP64 relative residual."""
 
     def __init__(self, mesh, device="cuda", rtol=DIRECT_RTOL, maxiter=20000, p_precond="ilu0", precision="fp64"):
         torch = _lib.require_cuda()
@@ -153,13 +158,26 @@ class TwoFluidSolver:
         self._res = torch.zeros(4 * nd + 2 + 1 + 4 + 2, **f64)
         self._A = DeviceCSR(dm.t["indptr"], dm.t["indices"], self._vals)
         levels = mesh.cell_color
-        self._s1 = Solver(self._A, precond="ilu0", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels)
-        self._sg = Solver(self._A, precond="ilu0", nrhs=nd, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels)
+        if precision not in ("fp64", "mixed"):
+            raise ValueError(f"unknown precision {precision!r}")
+        mode = _lib.MODE_MIXED if precision == "mixed" else _lib.MODE_FP64
+        self.precision = precision
+        mixed = precision == "mixed"
+        # mixed on large meshes: the graph engine's FP32 form for the momentum, volume
+        # fraction and energy systems (well conditioned: every one has a time term)
+        t1 = 3 if (mixed and n > 40000) else 0
+        tg = 3 if (mixed and n * nd > 40000) else 0
+        self._s1 = Solver(self._A, precond="ilu0", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels,
+                          mode=mode, team=t1)
+        self._sg = Solver(self._A, precond="ilu0", nrhs=nd, rtol=rtol, atol=0.0, maxiter=maxiter, levels=levels,
+                          mode=mode, team=tg)
         if p_precond == "amg":
-            self._sp = Solver(self._A, precond="amg", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter,
-                              mode=_lib.MODE_MIXED if precision == "mixed" else _lib.MODE_FP64)
+            self._sp = Solver(self._A, precond="amg", nrhs=1, rtol=rtol, atol=0.0, maxiter=maxiter, mode=mode)
         elif p_precond == "ilu0":
-            self._sp = self._s1
+            # the pinned p' (diag[0] += 1e10) is not well conditioned: in the mixed form
+            # it keeps the FP64 Krylov iteration on large meshes
+            self._sp = self._s1 if not t1 else Solver(self._A, precond="ilu0", nrhs=1, rtol=rtol, atol=0.0,
+                                                      maxiter=maxiter, levels=levels)
         else:
             raise ValueError(f"unknown p' preconditioner {p_precond!r}")
         self._params = _lib.TfParams()
@@ -307,7 +325,7 @@ class TwoFluidSolver:
     def _solve(self, solver, x, rhs):
         solver.setup(self._A)
         solver.solve(self._A, rhs, x)
-        k = 1 if solver is self._sg else (2 if (solver is self._sp and solver is not self._s1) else 0)
+        k = 1 if solver is self._sg else (2 if (solver is self._sp and solver.precond == "amg") else 0)
         self.krylov[k] += solver.iters.max().to(self.krylov.dtype)
 
     def _simple_iteration(self):

@@ -637,10 +637,10 @@ def c4_measure(count=C4_TOTAL, steps=1, warmup=1, mode="fp64", plain=True, plain
     launch = t / steps
     peak = measured_peak()
     tiers = bs.tiers()
-    roof = {"bound": "hbm", "kernel": f"batch_cluster_kernel<MIXED={int(mixed)}, JACOBI> (systems of >= 131,072 rows, "
-                                      f"one thread-block cluster of {tiers['cluster_size']} CTAs each) + "
+    roof = {"bound": "hbm", "kernel": f"batch_cluster_kernel<MIXED={int(mixed)}, JACOBI> ({tiers['cluster']} systems on "
+                                      f"thread-block clusters of 2-{tiers['cluster_size']} CTAs graded by size) + "
                                       f"batch_kernel<MIXED={int(mixed)}, JACOBI, 512 | 256> (one CTA per system), "
-                                      "largest first, three size tiers",
+                                      "largest first, one persistent launch per tier",
             "unit_of_work": "one launch solving all systems", "achieved": round(byts / launch / 1e9, 1),
             "peak": peak[0], "unit": "GB/s", "frac": round(byts / launch / 1e9 / peak[0], 3),
             "peak_source": peak[1], "traffic": None, "launch_ms": round(launch * 1e3, 3)}

@@ -306,21 +306,25 @@ void kcfd_amg_destroy(kcfd_amg* h);
 /* Many independent systems (e.g. the pressure-correction systems of many meshes) of
  * uneven sizes solved together over packed CSR with per-system offsets: each team
  * takes the next system from a largest-first queue and solves it alone (FP64 or MIXED
- * BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule per system). Three
- * tiers run concurrently, one persistent launch each: systems of at least
- * cluster_rows rows are solved by the cluster_size CTAs of one thread-block cluster
- * (512 threads each, one per SM, rows split between them, bounded software
- * barriers); systems of at least big_rows rows by one 512-thread CTA; the rest by one
- * 256-thread CTA. A system's tier depends only on its own size (and, for the cluster
- * tier, on whether a cluster can be resident at all), so its result is the same alone
- * and in any mix. No counterpart API in the reference, which solves one system per
- * call (core/linear_solver.py:14-70); results per system equal that path's semantics. */
+ * BiCGSTAB, Jacobi or no preconditioner; the scipy stopping rule per system). The
+ * tiers run concurrently, one persistent launch each. Cluster tiers: a system is
+ * solved by the CTAs of one thread-block cluster (512 threads each, one per SM, rows
+ * split between them, bounded software barriers) -- graded (cluster_size 0): 8, 4 or
+ * 2 CTAs for systems of at least 8R, 4R or 2R rows, R = cluster_rows (0: 16384), so
+ * that the big systems get CTAs in proportion to their size; or one tier of
+ * cluster_size CTAs from cluster_rows rows (0: 131072). Then systems of at least
+ * big_rows rows are solved by one 512-thread CTA, the rest by one 256-thread CTA. A
+ * system's tier depends only on its own size (and on whether a cluster of its size
+ * can be resident at all), so its result is the same alone and in any mix. No
+ * counterpart API in the reference, which solves one system per call
+ * (core/linear_solver.py:14-70); results per system equal that path's semantics. */
 typedef struct kcfd_batch kcfd_batch;
 typedef struct {
     int32_t precond, stop, mode, maxiter, lanes, max_refine, inner_maxiter;
     int32_t big_rows;      /* tier threshold in rows: 0 default (16384), < 0 none      */
-    int32_t cluster_rows;  /* cluster tier threshold: 0 default (131072), < 0 none     */
-    int32_t cluster_size;  /* CTAs per cluster team: 0 default (4), 2..8               */
+    int32_t cluster_rows;  /* graded: R (0: 16384); one tier: its threshold (0:
+                              131072); < 0: no cluster tier                           */
+    int32_t cluster_size;  /* CTAs per cluster team: 0 graded, 2..8 one tier           */
     double  rtol, atol, inner_rtol;
     int32_t restarts;      /* KCFD_STOP_SCIPY: a system whose rho or omega breaks down
                               (|.| < eps^2) restarts from its current iterate with

@@ -2357,6 +2357,19 @@ int kcfd_solver_error(kcfd_solver* s, int32_t* err, void* stream) {
 }  // extern "C"
 
 // ---------------------------------------------------------- batched host side --
+// Graded cluster tiers: a system of at least 2R, 4R, 8R rows gets 2, 4, 8 CTAs. With
+// R chosen automatically (cluster_rows 0) R is the smallest of kGradedRows * 2^k for
+// which the cluster teams ask for at most kClusterDemand CTAs per SM in all: a small
+// batch then spreads its big systems over the GPU (its length is the slowest team's),
+// a large one keeps most systems on one CTA each (its length is its total work).
+// Measured on the Delaunay p' systems (FP64, Jacobi; solves/s): the first 128 of the
+// 1,024, one tier of 4 CTAs from 131,072 rows 31.2, graded R = 8192 64.0, 16384 59.7,
+// 24576 50.2; all 1,024: one tier 89.6, graded R = 8192 80.7, 16384 85.2, 24576 88.5.
+constexpr int kGradedRows = 8192;
+constexpr double kClusterDemand = 3.5;
+// queue counters: [0] big tier, [1] small tier, [2 + t] cluster tier t
+constexpr int kQueues = 5;
+
 struct kcfd_batch {
     kcfd_batch_opts_t o;
     int nsys = 0;
@@ -2372,28 +2385,37 @@ struct kcfd_batch {
     int* lev = nullptr;
     void* work = nullptr;
     double* r64 = nullptr;
-    // tiers: order[0..nhuge) cluster teams, then nbig big systems (512-thread CTAs),
-    // then the rest
+    // tiers: order[0..nhuge) cluster teams (cluster tier t: cl_n[t] systems from
+    // order[cl_first[t]], clusters of cl_size[t] CTAs, cl_ncl[t] clusters launched), then
+    // nbig big systems (512-thread CTAs), then the rest
+    static constexpr int kMaxClTiers = 3;
     int nhuge = 0, nbig = 0, grid_big = 0;
-    int csize = 0, ncl = 0;               // cluster tier: CTAs per cluster, clusters launched
-    unsigned int* cbar = nullptr;         // [ncl] barrier counters
-    int* cslot = nullptr;                 // [ncl] published queue entries
-    double* cpart = nullptr;              // [ncl][kSlots][kMaxK][csize]
+    int ntier = 0;
+    int cl_size[kMaxClTiers] = {}, cl_n[kMaxClTiers] = {}, cl_ncl[kMaxClTiers] = {}, cl_first[kMaxClTiers] = {};
+    unsigned int* cbar[kMaxClTiers] = {};  // [cl_ncl] barrier counters
+    int* cslot[kMaxClTiers] = {};          // [cl_ncl] published queue entries
+    double* cpart[kMaxClTiers] = {};       // [cl_ncl][kSlots][kMaxK][cl_size]
+    cudaStream_t cst[kMaxClTiers] = {};
+    cudaEvent_t cev[kMaxClTiers] = {};
     int* cerr = nullptr;
-    cudaStream_t side = nullptr, side2 = nullptr;
-    cudaEvent_t ev_fork = nullptr, ev_join = nullptr, ev_join2 = nullptr;
+    cudaStream_t side = nullptr;
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
 };
 
 namespace {
 int free_batch(kcfd_batch* b) {
     if (!b) return KCFD_OK;
     if (b->side) cudaStreamDestroy(b->side);
-    if (b->side2) cudaStreamDestroy(b->side2);
     if (b->ev_fork) cudaEventDestroy(b->ev_fork);
     if (b->ev_join) cudaEventDestroy(b->ev_join);
-    if (b->ev_join2) cudaEventDestroy(b->ev_join2);
-    void* ps[] = {b->sys,  b->order, b->queue, b->indptr, b->indices, b->vals32, b->dinv,
-                  b->lev,  b->work,  b->r64,   b->cbar,   b->cslot,   b->cpart,  b->cerr};
+    for (int t = 0; t < kcfd_batch::kMaxClTiers; ++t) {
+        if (b->cst[t]) cudaStreamDestroy(b->cst[t]);
+        if (b->cev[t]) cudaEventDestroy(b->cev[t]);
+        void* pt[] = {b->cbar[t], b->cslot[t], b->cpart[t]};
+        for (void* p : pt)
+            if (p) cudaFree(p);
+    }
+    void* ps[] = {b->sys, b->order, b->queue, b->indptr, b->indices, b->vals32, b->dinv, b->lev, b->work, b->r64, b->cerr};
     for (void* p : ps)
         if (p) cudaFree(p);
     delete b;
@@ -2488,9 +2510,13 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
     }
     b->n_total = ro;
     b->nnz_total = zo;
-    // largest first (longest-processing-time order for the dynamic queues); systems of
-    // at least cluster_rows rows go to cluster teams, then those of at least big_rows
-    // rows to 512-thread CTAs, the rest to 256-thread CTAs
+    // largest first (longest-processing-time order for the dynamic queues). Cluster
+    // teams: graded (cluster_size 0) -- a system of at least 8R, 4R or 2R rows gets a
+    // cluster of 8, 4 or 2 CTAs (R = cluster_rows, 0: kGradedRows), so that a team's
+    // rows per CTA, and so roughly its time per system, stay within a factor of two
+    // across the big systems; or one tier of cluster_size CTAs from cluster_rows rows.
+    // Then systems of at least big_rows rows go to 512-thread CTAs, the rest to
+    // 256-thread CTAs.
     const bool mixed = b->o.mode == KCFD_MODE_MIXED;
     const size_t vsz = mixed ? 4 : 8;
     int dev = 0, sms = 0;
@@ -2500,33 +2526,72 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
     for (int s = 0; s < nsys; ++s) order[s] = s;
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return nnz[x] > nnz[y]; });
     const int big_rows = b->o.big_rows == 0 ? 16384 : b->o.big_rows;
-    // defaults measured on 1,024 Delaunay p' systems of 2e3-2e5 rows (FP64, Jacobi):
-    // one CTA per system 74.3 systems/s; clusters of 4 from 131,072 rows 108.7 (of 8:
-    // 105.4; of 4 or 8 from 65,536 rows: 98.6, 92.2)
-    int cl_rows = b->o.cluster_rows == 0 ? 131072 : b->o.cluster_rows;
-    b->csize = b->o.cluster_size == 0 ? 4 : b->o.cluster_size;
-    if (b->csize < 2 || b->csize > 8) {
+    const int csize = b->o.cluster_size;
+    if (csize != 0 && (csize < 2 || csize > 8)) {
         free_batch(b);
-        set_error("kcfd_batch_create: cluster_size must be 0 (default 4) or 2..8");
+        set_error("kcfd_batch_create: cluster_size must be 0 (graded) or 2..8");
         return KCFD_BAD_INPUT;
     }
-    int ncl_max = 0;
-    if (cl_rows > 0) {
-        cudaLaunchAttribute at[1];
-        cudaLaunchConfig_t cfg = cluster_config(1, b->csize, nullptr, at);
-        if (cudaOccupancyMaxActiveClusters(&ncl_max, batch_cluster_ptr(mixed, b->o.precond), &cfg) != cudaSuccess)
-            ncl_max = 0;
-        cudaGetLastError();
-        if (ncl_max < 1) cl_rows = -1;  // no cluster can be resident: the big tier takes them
+    // candidate cluster tiers (largest teams first) and their row thresholds
+    int cand_size[kcfd_batch::kMaxClTiers], cand_rows[kcfd_batch::kMaxClTiers], ncand = 0;
+    if (b->o.cluster_rows >= 0) {
+        if (csize == 0) {
+            int64_t R = b->o.cluster_rows;
+            if (R == 0) {
+                R = kGradedRows;
+                for (;; R *= 2) {
+                    int64_t demand = 0;
+                    for (int s = 0; s < nsys; ++s) {
+                        const int64_t q = n[s] / R;
+                        demand += q >= 8 ? 8 : q >= 4 ? 4 : q >= 2 ? 2 : 0;
+                    }
+                    if (demand <= (int64_t)(kClusterDemand * sms) || R > INT32_MAX / 16) break;
+                }
+            }
+            for (int c = 8; c >= 2; c >>= 1) {
+                cand_size[ncand] = c;
+                cand_rows[ncand++] = (int)std::min<int64_t>((int64_t)c * R, INT32_MAX);
+            }
+        } else {
+            cand_size[0] = csize;
+            cand_rows[0] = b->o.cluster_rows == 0 ? 131072 : b->o.cluster_rows;
+            ncand = 1;
+        }
     }
-    auto tier = [&](int x) { return (cl_rows > 0 && n[x] >= cl_rows) ? 0 : (big_rows > 0 && n[x] >= big_rows) ? 1 : 2; };
+    // keep the tiers whose clusters can be resident (a dropped tier's systems fall to
+    // the next one down)
+    int ncl_max[kcfd_batch::kMaxClTiers];
+    b->ntier = 0;
+    for (int t = 0; t < ncand; ++t) {
+        int m = 0;
+        cudaLaunchAttribute at[1];
+        cudaLaunchConfig_t cfg = cluster_config(1, cand_size[t], nullptr, at);
+        if (cudaOccupancyMaxActiveClusters(&m, batch_cluster_ptr(mixed, b->o.precond), &cfg) != cudaSuccess) m = 0;
+        cudaGetLastError();
+        if (m < 1) continue;
+        b->cl_size[b->ntier] = cand_size[t];
+        cand_rows[b->ntier] = cand_rows[t];
+        ncl_max[b->ntier++] = m;
+    }
+    const int nt = b->ntier;
+    auto tier = [&](int x) {
+        for (int t = 0; t < nt; ++t)
+            if (n[x] >= cand_rows[t]) return t;
+        return (big_rows > 0 && n[x] >= big_rows) ? nt : nt + 1;
+    };
     std::stable_sort(order.begin(), order.end(), [&](int x, int y) { return tier(x) < tier(y); });
     b->nhuge = b->nbig = 0;
     for (int s = 0; s < nsys; ++s) {
-        b->nhuge += tier(s) == 0 ? 1 : 0;
-        b->nbig += tier(s) == 1 ? 1 : 0;
+        const int t = tier(s);
+        if (t < nt) b->cl_n[t]++;
+        b->nhuge += t < nt ? 1 : 0;
+        b->nbig += t == nt ? 1 : 0;
     }
-    b->ncl = std::min(b->nhuge, ncl_max);
+    for (int t = 0, first = 0; t < nt; ++t) {
+        b->cl_first[t] = first;
+        first += b->cl_n[t];
+        b->cl_ncl[t] = std::min(b->cl_n[t], ncl_max[t]);
+    }
     int per_sm = 0, per_sm_big = 0;
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, batch_kernel_ptr(mixed, b->o.precond, false), 256, 0);
     cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_big, batch_kernel_ptr(mixed, b->o.precond, true), 512, 0);
@@ -2535,12 +2600,10 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
     b->grid_big = std::max(1, std::min(std::max(b->nbig, 1), std::max(1, per_sm_big) * sms));
     bool ok = cudaMalloc(&b->sys, nsys * sizeof(BatchSys)) == cudaSuccess &&
               cudaMemcpy(b->sys, sys.data(), nsys * sizeof(BatchSys), cudaMemcpyHostToDevice) == cudaSuccess &&
-              upload(&b->order, order) && cudaMalloc(&b->queue, 3 * sizeof(int)) == cudaSuccess &&
+              upload(&b->order, order) && cudaMalloc(&b->queue, kQueues * sizeof(int)) == cudaSuccess &&
               cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) == cudaSuccess &&
-              cudaStreamCreateWithFlags(&b->side2, cudaStreamNonBlocking) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) == cudaSuccess &&
               cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) == cudaSuccess &&
-              cudaEventCreateWithFlags(&b->ev_join2, cudaEventDisableTiming) == cudaSuccess &&
               cudaMalloc(&b->indptr, po * 4) == cudaSuccess &&
               cudaMemcpy(b->indptr, indptr_host, po * 4, cudaMemcpyHostToDevice) == cudaSuccess &&
               cudaMalloc(&b->indices, zo * 4) == cudaSuccess &&
@@ -2548,11 +2611,16 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
               cudaMalloc(&b->dinv, ro * vsz) == cudaSuccess && cudaMalloc(&b->lev, 2 * nsys * sizeof(int)) == cudaSuccess &&
               cudaMalloc(&b->work, 9 * ro * vsz) == cudaSuccess;
     if (ok && mixed) ok = cudaMalloc(&b->vals32, zo * 4) == cudaSuccess && cudaMalloc(&b->r64, ro * 8) == cudaSuccess;
-    if (ok && b->ncl > 0)
-        ok = cudaMalloc(&b->cbar, b->ncl * sizeof(unsigned int)) == cudaSuccess &&
-             cudaMalloc(&b->cslot, b->ncl * sizeof(int)) == cudaSuccess &&
-             cudaMalloc(&b->cpart, (size_t)b->ncl * kSlots * kMaxK * b->csize * sizeof(double)) == cudaSuccess &&
-             cudaMalloc(&b->cerr, sizeof(int)) == cudaSuccess;
+    for (int t = 0; ok && t < nt; ++t) {
+        if (b->cl_n[t] == 0) continue;
+        const int c = b->cl_ncl[t];
+        ok = cudaMalloc(&b->cbar[t], c * sizeof(unsigned int)) == cudaSuccess &&
+             cudaMalloc(&b->cslot[t], c * sizeof(int)) == cudaSuccess &&
+             cudaMalloc(&b->cpart[t], (size_t)c * kSlots * kMaxK * b->cl_size[t] * sizeof(double)) == cudaSuccess &&
+             cudaStreamCreateWithFlags(&b->cst[t], cudaStreamNonBlocking) == cudaSuccess &&
+             cudaEventCreateWithFlags(&b->cev[t], cudaEventDisableTiming) == cudaSuccess;
+    }
+    if (ok && b->nhuge > 0) ok = cudaMalloc(&b->cerr, sizeof(int)) == cudaSuccess;
     if (!ok) {
         free_batch(b);
         set_error("kcfd_batch_create: device allocation failed (%lld rows, %lld entries)", ro, zo);
@@ -2578,8 +2646,12 @@ int kcfd_batch_tiers(const kcfd_batch* b, int32_t* tiers) {
     tiers[0] = b->nhuge;
     tiers[1] = b->nbig;
     tiers[2] = b->nsys - b->nhuge - b->nbig;
-    tiers[3] = b->ncl;
-    tiers[4] = b->csize;
+    tiers[3] = 0;
+    tiers[4] = 0;
+    for (int t = 0; t < b->ntier; ++t) {
+        tiers[3] += b->cl_n[t] > 0 ? b->cl_ncl[t] : 0;
+        if (b->cl_n[t] > 0) tiers[4] = std::max(tiers[4], b->cl_size[t]);
+    }
     return KCFD_OK;
 }
 
@@ -2617,21 +2689,19 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
     B.iters = iters;
     B.relres = relres;
     B.status = status;
-    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, 3 * sizeof(int), st));
-    if (b->ncl > 0) {
-        KCFD_CUDA(cudaMemsetAsync(b->cbar, 0, b->ncl * sizeof(unsigned int), st));
-        KCFD_CUDA(cudaMemsetAsync(b->cerr, 0, sizeof(int), st));
-    }
+    KCFD_CUDA(cudaMemsetAsync(b->queue, 0, kQueues * sizeof(int), st));
+    for (int t = 0; t < b->ntier; ++t)
+        if (b->cl_n[t] > 0) KCFD_CUDA(cudaMemsetAsync(b->cbar[t], 0, b->cl_ncl[t] * sizeof(unsigned int), st));
+    if (b->nhuge > 0) KCFD_CUDA(cudaMemsetAsync(b->cerr, 0, sizeof(int), st));
     B.nq = b->nsys;
     void* args[] = {&B};
     const int pgrid = std::max(1, std::min(b->nsys, 4 * b->grid));
     KCFD_CUDA(cudaLaunchKernel(B.mixed ? (void*)batch_prep_kernel<1> : (void*)batch_prep_kernel<0>, dim3(pgrid),
                                dim3(256), args, 0, st));
-    // cluster tier and big tier on side streams, forked from and joined back into the
-    // caller's; the cluster tier is launched first so that its clusters find free SMs
-    BatchArgs Bh = B, Bb = B, Bs = B;
-    Bh.queue = b->queue + 2;
-    Bh.nq = b->nhuge;
+    // cluster tiers and the big tier on side streams, forked from and joined back into
+    // the caller's; the cluster tiers are launched first (largest teams first) so that
+    // their clusters find free SMs
+    BatchArgs Bb = B, Bs = B;
     Bb.order = b->order + b->nhuge;
     Bb.nq = b->nbig;
     Bs.order = b->order + b->nhuge + b->nbig;
@@ -2639,21 +2709,24 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
     Bs.nq = b->nsys - b->nhuge - b->nbig;
     void* args_b[] = {&Bb};
     void* args_s[] = {&Bs};
-    if (b->nhuge > 0 || b->nbig > 0) {
-        KCFD_CUDA(cudaEventRecord(b->ev_fork, st));
-        KCFD_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
-        KCFD_CUDA(cudaStreamWaitEvent(b->side2, b->ev_fork, 0));
-    }
-    if (b->nhuge > 0) {
+    if (b->nhuge > 0 || b->nbig > 0) KCFD_CUDA(cudaEventRecord(b->ev_fork, st));
+    if (b->nbig > 0) KCFD_CUDA(cudaStreamWaitEvent(b->side, b->ev_fork, 0));
+    for (int t = 0; t < b->ntier; ++t) {
+        if (b->cl_n[t] == 0) continue;
+        KCFD_CUDA(cudaStreamWaitEvent(b->cst[t], b->ev_fork, 0));
+        BatchArgs Bh = B;
+        Bh.queue = b->queue + 2 + t;
+        Bh.order = b->order + b->cl_first[t];
+        Bh.nq = b->cl_n[t];
         ClusterCtl C;
-        C.bar = b->cbar;
-        C.slot = b->cslot;
-        C.partials = b->cpart;
+        C.bar = b->cbar[t];
+        C.slot = b->cslot[t];
+        C.partials = b->cpart[t];
         C.err = b->cerr;
         C.budget = 4000000000LL;  // ~2 s at 2 GHz per barrier wait
         void* args_h[] = {&Bh, &C};
         cudaLaunchAttribute at[1];
-        const cudaLaunchConfig_t cfg = cluster_config(b->ncl, b->csize, b->side2, at);
+        const cudaLaunchConfig_t cfg = cluster_config(b->cl_ncl[t], b->cl_size[t], b->cst[t], at);
         KCFD_CUDA(cudaLaunchKernelExC(&cfg, batch_cluster_ptr(B.mixed, B.precond), args_h));
     }
     if (b->nbig > 0)
@@ -2665,9 +2738,10 @@ int kcfd_batch_solve(kcfd_batch* b, const double* vals64, const double* rhs, dou
         KCFD_CUDA(cudaEventRecord(b->ev_join, b->side));
         KCFD_CUDA(cudaStreamWaitEvent(st, b->ev_join, 0));
     }
-    if (b->nhuge > 0) {
-        KCFD_CUDA(cudaEventRecord(b->ev_join2, b->side2));
-        KCFD_CUDA(cudaStreamWaitEvent(st, b->ev_join2, 0));
+    for (int t = 0; t < b->ntier; ++t) {
+        if (b->cl_n[t] == 0) continue;
+        KCFD_CUDA(cudaEventRecord(b->cev[t], b->cst[t]));
+        KCFD_CUDA(cudaStreamWaitEvent(st, b->cev[t], 0));
     }
     KCFD_CUDA(cudaGetLastError());
     return KCFD_OK;

@@ -30,10 +30,12 @@ class BatchOpts(C.Structure):
 class BatchSolver:
     """patterns: list of (indptr, indices) host arrays (one per system).
 
-    Tiers by system size: at least cluster_rows rows (0: 131072, negative: none) are
-    solved by a thread-block cluster of cluster_size CTAs (0: 4); at least big_rows
-    rows (0: 16384, negative: none) by one 512-thread CTA; the rest by one 256-thread
-    CTA. tiers() reports the split.
+    Tiers by system size. Cluster teams (one thread-block cluster per system):
+    graded with cluster_size 0 -- 8, 4 or 2 CTAs from 8R, 4R or 2R rows, R =
+    cluster_rows (0: 16384) -- or one tier of cluster_size CTAs from cluster_rows rows
+    (0: 131072); negative cluster_rows: none. Then at least big_rows rows (0: 16384,
+    negative: none) by one 512-thread CTA; the rest by one 256-thread CTA. tiers()
+    reports the split (cluster_size: the largest team).
 
     restarts: with the scipy stopping rule, a system whose rho or omega breaks down
     restarts from its current iterate (rhat = r, p = r) up to this many times (0: it

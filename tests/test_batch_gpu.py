@@ -108,14 +108,16 @@ def test_cluster_tier_same_result_alone_and_in_the_batch(batch):
     import torch
     from kcfd.batch import BatchSolver
     pats, vals, rhs, sizes = batch
-    full = BatchSolver(pats, mode="fp64", cluster_rows=2000)
+    # graded cluster teams with R = 1000: 2, 4 or 8 CTAs from 2000, 4000, 8000 rows
+    full = BatchSolver(pats, mode="fp64", cluster_rows=1000)
+    assert full.tiers()["cluster"] == int((full.n >= 2000).sum())
     x = torch.zeros(full.n_total, dtype=torch.float64, device="cuda")
     full.solve(torch.cat(vals), full.pack(rhs), x)
     xs = full.unpack(x)
     big = [k for k in range(len(pats)) if len(pats[k][0]) - 1 >= 2000][:3]
     assert big
     for k in big:
-        one = BatchSolver([pats[k]], mode="fp64", cluster_rows=2000)
+        one = BatchSolver([pats[k]], mode="fp64", cluster_rows=1000)
         assert one.tiers()["cluster"] == 1
         x1 = torch.zeros(one.n_total, dtype=torch.float64, device="cuda")
         one.solve(vals[k], one.pack([rhs[k]]), x1)

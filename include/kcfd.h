@@ -198,10 +198,13 @@ typedef struct {
     int32_t maxiter;     /* BiCGSTAB iterations (inner iterations in MIXED)   */
     int32_t team;        /* 0 auto, 1 one CTA per system, 2 whole grid (one
                             persistent cooperative kernel), 3 graph engine
-                            (FP64 only: phase kernels in one CUDA graph per solve
-                            with a device-side loop; inside a stream capture the
-                            solve runs on the team-2 kernel). Auto: 1 for
-                            n*nrhs <= 1024, 2 up to 40000 and for MIXED,
+                            (phase kernels in one CUDA graph per solve with a
+                            device-side loop; inside a stream capture the solve
+                            runs on the team-2 kernel; MIXED there: FP32 Krylov
+                            vectors and values, FP64 iterate, residual
+                            replacement against the FP64 matrix -- for well
+                            conditioned systems, so only when asked for). Auto:
+                            1 for n*nrhs <= 1024, 2 up to 40000 and for MIXED,
                             else 3.                                              
                             KCFD_ENGINE_EAGER=1 in the environment at creation
                             launches the engine's kernels from a host loop

@@ -203,3 +203,32 @@ def stream_handle(stream=None):
     import torch
     s = stream if stream is not None else torch.cuda.current_stream()
     return s.cuda_stream
+
+
+_deferred = []
+_deferred_lock = threading.Lock()
+
+
+def release(fn_name, handle):
+    """Destroy a native handle (kcfd_*_destroy by name). A destroy frees device memory,
+    which would invalidate a stream capture in progress on this thread (a handle
+    dropped by the garbage collector while a CUDA graph is being captured), so inside
+    a capture the handle is queued and destroyed at the next release outside one."""
+    capturing = False
+    try:
+        import torch
+        capturing = torch.cuda.is_available() and torch.cuda.is_current_stream_capturing()
+    except Exception:
+        capturing = False
+    with _deferred_lock:
+        if capturing:
+            _deferred.append((fn_name, handle))
+            return
+        pending = list(_deferred)
+        _deferred.clear()
+    for name, h in pending + [(fn_name, handle)]:
+        try:
+            getattr(lib(), name)(h)
+        except Exception:
+            pass
+

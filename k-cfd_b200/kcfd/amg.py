@@ -54,10 +54,7 @@ class AMG:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            try:
-                _lib.lib().kcfd_amg_destroy(h)
-            except Exception:
-                pass
+            _lib.release("kcfd_amg_destroy", h)
             self._h = None
 
     def setup(self, csr, stream=None):

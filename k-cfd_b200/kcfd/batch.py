@@ -82,10 +82,7 @@ class BatchSolver:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            try:
-                _lib.lib().kcfd_batch_destroy(h)
-            except Exception:
-                pass
+            _lib.release("kcfd_batch_destroy", h)
             self._h = None
 
     def solve(self, vals64, rhs, x, stream=None):

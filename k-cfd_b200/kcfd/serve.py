@@ -99,7 +99,7 @@ def footprint_bytes(ndim, N, precision="mixed", precond_p="ilu0"):
 
 
 class Case:
-    def __init__(self, req, precision="mixed", graph=True, precond_p="ilu0", rtol=1e-8, device="cuda",
+    def __init__(self, req, precision="fp64", graph=True, precond_p="ilu0", rtol=1e-8, device="cuda",
                  small_team=1):
         torch = _lib.require_cuda()
         from .mesh import build_mesh
@@ -119,7 +119,11 @@ class Case:
             # overlap on the device (0: the library's choice, best for one case alone);
             # the large ones take the grid-wide solvers either way
             team = small_team if m.n_cells * m.ndim <= 40000 else 0
-            s = SIMPLESolver(m, rho=1.0, mu=1.0 / req.Re, precision=precision,
+            # 'mixed' takes effect above 40,000 cells (the engine's FP32 momentum solve,
+            # the multigrid p' hierarchy in FP32); the small cases run latency-bound
+            # single-CTA solves, where FP32 storage saves nothing, in FP64
+            prec = precision if (precision != "mixed" or m.n_cells > 40000) else "fp64"
+            s = SIMPLESolver(m, rho=1.0, mu=1.0 / req.Re, precision=prec,
                              precond_p=p_precond_for(m.n_cells, precond_p), rtol=rtol, graph=graph, team=team)
             for nm in m.boundary_patches:
                 lid = [1.0] + [0.0] * (m.ndim - 1)
@@ -162,7 +166,7 @@ def work_estimate(req):
 
 class Server:
     def __init__(self, budget_bytes=150e9, max_active=64, iters_per_tick=10, max_iters=3000, cont_tol=1e-6,
-                 precision="mixed", graph=True, precond_p="ilu0", keep_fields=False, verbose=False,
+                 precision="fp64", graph=True, precond_p="ilu0", keep_fields=False, verbose=False,
                  policy="fifo", builders=1):
         self.budget = budget_bytes
         self.max_active = max_active

@@ -20,12 +20,14 @@ copy (written by the same kernels) for the inner iterations. On large meshes the
 momentum solve runs the graph engine's FP32 form (FP32 vectors and values, FP64
 iterate, residual replacement against the FP64 matrix); the p' solve keeps an FP64
 Krylov iteration over an FP32 multigrid hierarchy with precond_p='amg'; with ILU(0)
-or Jacobi it runs FP32 inner iterations with FP64 refinement up to 40,000 cells and
-FP64 above (FP32 inner iterations cannot resolve the pinned p' operator there).
+or Jacobi it runs FP32 inner iterations with FP64 refinement up to 4,096 cells and
+FP64 above (FP32 inner iterations cannot resolve the pinned p' operator on large
+meshes).
 """
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -39,7 +41,16 @@ class _Field:
     """values: host numpy view of a device tensor (read copies, assignment uploads)."""
 
     def __init__(self, owner, name):
-        self._owner, self._name = owner, name
+        # a weak reference: the solver holds its fields, so a strong one would make a
+        # cycle that keeps the solver's device memory until the garbage collector runs
+        self._ref, self._name = weakref.ref(owner), name
+
+    @property
+    def _owner(self):
+        o = self._ref()
+        if o is None:
+            raise ReferenceError("the solver of this field no longer exists")
+        return o
 
     @property
     def values(self):
@@ -110,11 +121,12 @@ class SIMPLESolver:
         if precond_p == "ilu0":
             levels = mesh.cell_color if ilu_order == "color" else mesh.level_natural
         # p' in the mixed form: an FP32 multigrid hierarchy under an FP64 Krylov iteration
-        # ('amg'); FP32 inner iterations with FP64 refinement up to 40,000 cells; FP64
+        # ('amg'); FP32 inner iterations with FP64 refinement up to 4,096 cells; FP64
         # above, where the FP32 inner iterations cannot resolve the pinned operator
-        # (measured: BREAKDOWN on a 256^2 cavity, and divergence of the engine's FP32
-        # recursion on the 128^3 cavity, with ILU(0) and with Jacobi)
-        mode_p = self.mode if (precond_p == "amg" or n <= 40000) else _lib.MODE_FP64
+        # (its conditioning grows with the mesh; measured: BREAKDOWN on a 256^2 cavity,
+        # and divergence of the engine's FP32 recursion on the 128^3 cavity, with ILU(0)
+        # and with Jacobi)
+        mode_p = self.mode if (precond_p == "amg" or n <= 4096) else _lib.MODE_FP64
         self.s_p = Solver(self.A_p, precond=precond_p, mode=mode_p, nrhs=1, maxiter=maxiter, rtol=rtol,
                           team=team, lanes=lanes, inner_rtol=inner_rtol, inner_maxiter=inner_maxiter, levels=levels)
         self.U = _Field(self, "U_t")

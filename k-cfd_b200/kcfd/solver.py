@@ -118,10 +118,7 @@ class Solver:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            try:
-                _lib.lib().kcfd_solver_destroy(h)
-            except Exception:
-                pass
+            _lib.release("kcfd_solver_destroy", h)
             self._h = None
 
     def set_tolerances(self, rtol=None, atol=None, maxiter=None):
@@ -220,8 +217,5 @@ class DeviceGraph:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            try:
-                _lib.lib().kcfd_graph_destroy(h)
-            except Exception:
-                pass
+            _lib.release("kcfd_graph_destroy", h)
             self._h = None

@@ -23,6 +23,7 @@ back to the host in one small copy for the reference's tolerance test.
 from __future__ import annotations
 
 import ctypes as C
+import weakref
 
 import numpy as np
 
@@ -38,7 +39,15 @@ class _Field:
     """Device field with the reference field interface (core/fields.py)."""
 
     def __init__(self, owner, name, ncomp):
-        self._o, self._name, self.ncomp = owner, name, ncomp
+        # weak: the solver holds its fields (a strong reference would be a cycle)
+        self._ref, self._name, self.ncomp = weakref.ref(owner), name, ncomp
+
+    @property
+    def _o(self):
+        o = self._ref()
+        if o is None:
+            raise ReferenceError("the solver of this field no longer exists")
+        return o
 
     @property
     def _t(self):

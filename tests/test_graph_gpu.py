@@ -42,3 +42,32 @@ def test_captured_spmv_and_solve_replay_bitwise():
         s.synchronize()
         assert torch.equal(y2, y_ref)
         assert torch.equal(xs, x_ref) and int(sv.iters[0]) == it_ref
+
+
+def test_handle_dropped_inside_a_capture_is_released_after_it():
+    """A solver handle destroyed while a CUDA graph is being captured on this thread
+    (e.g. by the garbage collector) would free device memory inside the capture and
+    invalidate it; its release is deferred to the next one outside the capture."""
+    import torch
+    from kcfd import _lib
+    from kcfd.solver import DeviceCSR, Solver
+    A, b = convdiff_system(channel_mesh(20, 10))
+    d = DeviceCSR.from_scipy(A)
+    doomed = Solver(d, precond="jacobi", rtol=1e-8, maxiter=100, team=1)
+    x = torch.randn(d.n, dtype=torch.float64, device="cuda")
+    y = torch.empty_like(x)
+    d.spmv(x, y)
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    g = torch.cuda.CUDAGraph()
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s):
+            d.spmv(x, y, stream=s)
+            del doomed                  # destroyed inside the capture
+            assert len(_lib._deferred) == 1
+    y.zero_()
+    g.replay()
+    torch.cuda.synchronize()
+    assert torch.equal(y, d.spmv(x))
+    Solver(d, precond="jacobi", rtol=1e-8, maxiter=100, team=1)   # created and dropped outside: flushes
+    assert len(_lib._deferred) == 0

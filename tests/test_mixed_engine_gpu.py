@@ -117,7 +117,7 @@ def test_mixed_engine_maxiter_and_repeat():
 def test_mixed_simple_on_the_engine():
     """SIMPLE's mixed form on a 256^2 cavity (65,536 cells): the momentum solve (2
     right-hand sides) runs the engine's FP32 form; p' runs FP64 with ILU(0) (above
-    40,000 cells) or an FP64 Krylov iteration over an FP32 hierarchy (multigrid); after
+    4,096 cells) or an FP64 Krylov iteration over an FP32 hierarchy (multigrid); after
     5 outer iterations every solve met its FP64 stopping test and the fields agree with
     the FP64 run within 1e-6 relative L2."""
     import torch

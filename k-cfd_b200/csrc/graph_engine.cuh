@@ -64,8 +64,12 @@ constexpr int kBlock = 256;
 constexpr int kSlotsG = 6;
 constexpr int kSlotK = 9;  // values per reduction slot (g_rr: 3 per right-hand side)
 constexpr double kEps2g = 4.930380657631324e-32;
-// MIXED: replace the recursive residual once it has fallen by this factor
-constexpr double kReplaceEps = 1e-2;
+// MIXED: replace the recursive residual once it has fallen by this factor. The drift
+// of an FP32 recursion is about eps32 times the residual at the last replacement, so
+// replacing every four decades keeps it near 1e-3 of the current residual; at 1e-2 a
+// momentum solve (a decade per iteration) replaced every other iteration, an FP64
+// residual each time (the 128^3 launch list: 30 us of 60 per Krylov iteration)
+constexpr double kReplaceEps = 1e-4;
 // MIXED: restart the recursion when the true residual exceeds the recursive one by this factor
 constexpr double kDriftRestart = 2.0;
 // MIXED: replace at least every this many iterations (an FP32 recursion on an

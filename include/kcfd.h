@@ -332,7 +332,11 @@ typedef struct {
     int32_t restarts;      /* KCFD_STOP_SCIPY: a system whose rho or omega breaks down
                               (|.| < eps^2) restarts from its current iterate with
                               rhat = r, p = r, up to this many times; 0 stops there with
-                              KCFD_BREAKDOWN as scipy does                            */
+                              KCFD_BREAKDOWN as scipy does. With restarts > 0 (FP64) a
+                              system that stops on its recursive residual is also
+                              checked against b - A x: up to 3 more passes start from
+                              the true residual (a pass that meets the tolerance at
+                              once ends with no iteration)                            */
 } kcfd_batch_opts_t;
 /* indptr_host: per system n[s]+1 local row pointers, concatenated; indices_host:
  * local column indices, concatenated (host arrays, copied to the device).          */

@@ -704,6 +704,9 @@ __device__ void permute_out(Team& tm, const SolveArgs& a) {
     });
 }
 
+// Verification passes of a batched FP64 solve (see solve_fp64).
+constexpr int kVerifyPasses = 3;
+
 // FP64 solve.
 template <int NRHS, int PREC, class Team>
 __device__ void solve_fp64(Team& tm, const SolveArgs& a, double* smem) {
@@ -715,9 +718,24 @@ __device__ void solve_fp64(Team& tm, const SolveArgs& a, double* smem) {
         permute_in<NRHS>(tm, a);
         if (!tm.sync()) return;
     }
-    bool ok = bicgstab_body<double, double, NRHS, PREC>(tm, a, a.vals64, x, b, false, w, a.stop, a.rtol, a.atol,
-                                                        a.maxiter, st, smem);
-    if (!ok) return;
+    // With breakdown restarts (the batched solver) a system that stopped on its recursive
+    // residual is checked against the true one: the next pass starts from r = b - A x
+    // and ends at once (no iteration) when that meets the tolerance, else it iterates on
+    // from the true residual. Iterations of all passes count against maxiter.
+    const bool verify = NRHS == 1 && a.max_restarts > 0 && a.stop == KCFD_STOP_SCIPY;
+    int used = 0;
+    for (int pass = 0;; ++pass) {
+        const bool ok = bicgstab_body<double, double, NRHS, PREC>(tm, a, a.vals64, x, b, false, w, a.stop, a.rtol,
+                                                                  a.atol, a.maxiter - used, st, smem);
+        if (!ok) return;
+        used += st.iters[0];
+        if (!verify || pass >= kVerifyPasses || st.status[0] != KCFD_OK || st.iters[0] == 0 || used >= a.maxiter) break;
+        // every member's last x update is in place before any member gathers x again
+        if (!tm.sync()) return;
+    }
+    __syncthreads();
+    if (verify && threadIdx.x == 0) st.iters[0] = used;
+    __syncthreads();
     if (a.perm) permute_out<NRHS>(tm, a);
     write_results<NRHS>(a, st, tm.rank);
 }

@@ -127,8 +127,9 @@ def test_cluster_tier_same_result_alone_and_in_the_batch(batch):
 def test_breakdown_restart():
     """Systems drawn like the 1,024-system batch (log-uniform cell counts, Delaunay
     triangles, seed 0): with restarts every system converges to the true residual; a
-    system that never breaks down takes the same path with or without restarts, so its
-    result is bitwise unchanged."""
+    system that never breaks down and whose true residual met the tolerance takes the
+    same path with or without restarts (the check of the true residual at convergence
+    ends at once), so its result is bitwise unchanged."""
     import torch
     from kcfd.batch import BatchSolver, p_prime_batch
     pats, vals, rhs, sizes = p_prime_batch(48, n_min=2000, n_max=20000, seed=0)
@@ -146,6 +147,9 @@ def test_breakdown_restart():
     for k in range(len(pats)):
         A = _csr(pats[k], vals[k])
         assert np.linalg.norm(rhs[k] - A @ x1[k]) / np.linalg.norm(rhs[k]) < 1.5e-8
-        if st0[k] == 0:
+        # b - A x of these systems (condition ~1e6) carries a rounding error of about 1 % of a
+        # 1e-8 residual, so the device may see a result within that margin of the tolerance
+        # on either side of it: only the clear cases are compared
+        if st0[k] == 0 and np.linalg.norm(rhs[k] - A @ x0[k]) < 0.9e-8 * np.linalg.norm(rhs[k]):
             np.testing.assert_array_equal(x0[k], x1[k])
     print(f"breakdowns without restarts: {int((st0 == 2).sum())} of {len(pats)}")

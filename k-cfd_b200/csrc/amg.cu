@@ -566,13 +566,17 @@ __global__ void __launch_bounds__(1024) k_gj(int nc, double* Mg, double* Invg, V
             prow[j] = (j < nc ? M[(size_t)k * nc + j] : Inv[(size_t)k * nc + j - nc]) * inv_p;
         for (int i = threadIdx.x; i < nc; i += blockDim.x) fcol[i] = M[(size_t)i * nc + k];
         __syncthreads();
+        // entries whose pivot-row factor is zero are left alone: the eliminated columns of M
+        // (j < k) and the columns of Inv that no step has touched yet, about half of [M | Inv]
         for (int i = ty; i < nc; i += nty) {
             const double f = fcol[i];
+            if (i != k && f == 0.0) continue;
             for (int j = tx; j < W; j += 32) {
                 double* A = j < nc ? M : Inv;
                 const size_t q = (size_t)i * nc + (j < nc ? j : j - nc);
-                if (i == k) A[q] = prow[j];
-                else if (f != 0.0) A[q] -= f * prow[j];
+                const double pj = prow[j];
+                if (i == k) A[q] = pj;
+                else if (pj != 0.0) A[q] -= f * pj;
             }
         }
         __syncthreads();

@@ -772,7 +772,8 @@ def run_c4(args):
 C5_METRIC = "served SIMPLE cavities/s (Poisson arrivals, continuous batching)"
 
 
-def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active=4, policy="sjf", serial=True):
+def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active=4, policy="sjf", serial=True,
+               small_team=1):
     """Poisson-arriving cavity requests (half 2D N^2, N in [32, 512]; half 3D N^3, N in
     [16, 96]; Re in [100, 1000]; seed 0) served by the continuous-batching loop
     (kcfd.serve.Server: HBM-budget admission, one stream and graph per case), each run
@@ -788,7 +789,8 @@ def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active
     torch.cuda.synchronize()
     dev = torch.cuda.current_device()
     with ClockSampler(dev) as cs:
-        res = Server(max_active=max_active, policy=policy, builders=2, precision="fp64", **common).run(reqs)
+        res = Server(max_active=max_active, policy=policy, builders=2, precision="fp64", small_team=small_team,
+                     **common).run(reqs)
     clocks = cs.summary()
     ours = summarize(res)
     d2h = int(sum(r.cells * (r.ndim + 1) * 8 for r in res))
@@ -816,7 +818,7 @@ def c5_measure(requests=40, rate=20.0, cont_tol=1e-2, max_iters=1500, max_active
 
 def run_c5(args):
     r = c5_measure(args.requests, args.rate, args.cont_tol, args.max_iters, args.max_active, args.policy,
-                   bool(args.plain))
+                   bool(args.plain), args.small_team)
     line = {
         "metric": C5_METRIC, "value": r["value"], "unit": "cases/s", "n_gpus": 1,
         "steps": r["requests"], "warmup": 2, "ms_per_step": round(1e3 / max(r["value"], 1e-9), 1),
@@ -1224,6 +1226,7 @@ def main():
     ap.add_argument("--cont-tol", type=float, default=1e-2, help="c5: continuity residual to serve to")
     ap.add_argument("--max-iters", type=int, default=1500, help="c5: outer iteration cap per case")
     ap.add_argument("--max-active", type=int, default=4, help="c5: resident cases at most")
+    ap.add_argument("--small-team", type=int, default=1, help="c5: solver team of the served small cases (1 or 0)")
     ap.add_argument("--policy", default="sjf", choices=["sjf", "fifo"], help="c5: admission order")
     ap.add_argument("--systems", type=int, default=1024, help="c4: number of systems")
     ap.add_argument("--c4-mode", default="fp64", choices=["fp64", "mixed"], help="c4: batched solve precision")

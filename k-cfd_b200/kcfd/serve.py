@@ -167,7 +167,7 @@ def work_estimate(req):
 class Server:
     def __init__(self, budget_bytes=150e9, max_active=64, iters_per_tick=10, max_iters=3000, cont_tol=1e-6,
                  precision="fp64", graph=True, precond_p="ilu0", keep_fields=False, verbose=False,
-                 policy="fifo", builders=1):
+                 policy="fifo", builders=1, small_team=1):
         self.budget = budget_bytes
         self.max_active = max_active
         self.k = iters_per_tick
@@ -180,6 +180,9 @@ class Server:
             raise ValueError(f"unknown admission policy {policy!r}")
         self.policy = policy
         self.builders = max(1, int(builders))
+        # solver team of the cases up to 40,000 unknowns when served beside others: 1 (one
+        # CTA per solve) or 0 (the library's choice, the grid kernel above 1,024 unknowns)
+        self.small_team = int(small_team)
 
     def run(self, requests, serial=False, case_factory=None):
         """Serve `requests` in real time (arrival times honoured). serial=True runs one
@@ -197,7 +200,7 @@ class Server:
             def build(r):
                 torch.cuda.set_device(dev)
                 # alone, a case takes the library's fastest single-case solvers
-                return Case(r, self.precision, self.graph, self.precond_p, small_team=0 if serial else 1)
+                return Case(r, self.precision, self.graph, self.precond_p, small_team=0 if serial else self.small_team)
 
             finish = torch.cuda.synchronize
         else:

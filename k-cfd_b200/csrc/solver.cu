@@ -1282,7 +1282,6 @@ struct kcfd_solver {
         int gmax = 0;
         int eager = 0;                     // host-driven loop instead of the graph
         bool pdl = true;                   // phase kernels with programmatic dependent launch
-        int unroll = 1;                    // BiCGSTAB iterations per trip of the loop body
         bool ready = false;                // args (and graph) built
         int mix = 0;                       // MIXED: FP32 vectors and values, FP64 x, b and residuals
         ge::Args args;
@@ -1679,7 +1678,7 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     KCFD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        for (int u = 0; u < g.unroll; ++u) ge_body<NRHS, PREC, T>(a, G, cs, g.pdl);
+        ge_body<NRHS, PREC, T>(a, G, cs, g.pdl);
         cudaGraph_t outg = nullptr;
         const cudaError_t e2 = cudaStreamEndCapture(cs, &outg);
         if (e == cudaSuccess) e = e2;
@@ -2042,8 +2041,6 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         s->g.eager = (ev && ev[0] == '1') ? 1 : 0;
         const char* pv = std::getenv("KCFD_ENGINE_PDL");
         s->g.pdl = !(pv && pv[0] == '0');
-        const char* uv = std::getenv("KCFD_ENGINE_UNROLL");
-        if (uv) s->g.unroll = std::max(1, std::min(8, std::atoi(uv)));
     }
     int lanes = opts->lanes;
     if (lanes <= 0) {

@@ -54,7 +54,10 @@ class AMG:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.release("kcfd_amg_destroy", h)
+            try:
+                _lib.release("kcfd_amg_destroy", h)
+            except Exception:   # interpreter shutdown: the module may be gone already
+                pass
             self._h = None
 
     def setup(self, csr, stream=None):

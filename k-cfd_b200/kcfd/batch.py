@@ -82,7 +82,10 @@ class BatchSolver:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.release("kcfd_batch_destroy", h)
+            try:
+                _lib.release("kcfd_batch_destroy", h)
+            except Exception:   # interpreter shutdown: the module may be gone already
+                pass
             self._h = None
 
     def solve(self, vals64, rhs, x, stream=None):

@@ -118,7 +118,10 @@ class Solver:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.release("kcfd_solver_destroy", h)
+            try:
+                _lib.release("kcfd_solver_destroy", h)
+            except Exception:   # interpreter shutdown: the module may be gone already
+                pass
             self._h = None
 
     def set_tolerances(self, rtol=None, atol=None, maxiter=None):
@@ -217,5 +220,8 @@ class DeviceGraph:
     def __del__(self):
         h = getattr(self, "_h", None)
         if h is not None and h.value:
-            _lib.release("kcfd_graph_destroy", h)
+            try:
+                _lib.release("kcfd_graph_destroy", h)
+            except Exception:   # interpreter shutdown: the module may be gone already
+                pass
             self._h = None

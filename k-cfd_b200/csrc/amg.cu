@@ -34,6 +34,7 @@
 #include <cstdint>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <thread>
 #include <vector>
 
@@ -878,11 +879,39 @@ int grid_for(const kcfd_amg* h, int64_t n) {
     return (int)std::max<int64_t>(1, std::min<int64_t>((n + 255) / 256, (int64_t)h->sm_count * 8));
 }
 
+// A grid-stride kernel's grid capped at the blocks that can be resident at once: a
+// grid above that runs a second, partial wave (the level-0 FP64 smoothing and
+// prolongation kernels take 40 registers, so 6 blocks of 256 threads per SM, where the
+// default grid is 8 per SM: a third of the rows ran in a tail at a quarter of the
+// occupancy). Occupancy per kernel function, looked up once.
+int resident_grid(const void* f, int grid, int block) {
+    static std::mutex mu;
+    static std::vector<std::pair<const void*, int>> cache;  // (function, blocks resident on the device)
+    int res = 0;
+    {
+        std::lock_guard<std::mutex> lk(mu);
+        for (const auto& e : cache)
+            if (e.first == f) res = e.second;
+    }
+    if (res == 0) {
+        int dev = 0, sms = 0, occ = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, block, 0) != cudaSuccess || occ < 1) {
+            (void)cudaGetLastError();
+            return grid;
+        }
+        res = occ * sms;
+        std::lock_guard<std::mutex> lk(mu);
+        cache.emplace_back(f, res);
+    }
+    return std::max(1, std::min(grid, res));
+}
+
 template <typename K, typename... Act>
 void launch(K k, int grid, int block, cudaStream_t st, bool pdl, Act... args) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
-    cfg.gridDim = dim3(grid);
+    cfg.gridDim = dim3(resident_grid((const void*)k, grid, block));
     cfg.blockDim = dim3(block);
     cfg.stream = st;
     cudaLaunchAttribute at[1];
@@ -911,9 +940,10 @@ int setup_t(kcfd_amg* h, const double* vals, cudaStream_t st) {
             k_diag<<<g, 256, 0, st>>>(lv.n, lv.ip, a, lv.dslot, lv.dinv, nullptr);
             const int gr = std::min(kRedGrid, g);
             k_pow_init<<<gr, 256, 0, st>>>(lv.n, h->powv[0], h->part, h->cnt, h->nrm2);
+            const int gp = resident_grid((const void*)k_pow_step<V>, gr, 256);
             for (int t = 0; t < h->o.power_iters; ++t) {
                 const int a_ = t & 1, b_ = a_ ^ 1;
-                k_pow_step<V><<<gr, 256, 0, st>>>(lv.n, lv.soff, lv.scol, (const V*)lv.sA, lv.dinv, h->powv[a_],
+                k_pow_step<V><<<gp, 256, 0, st>>>(lv.n, lv.soff, lv.scol, (const V*)lv.sA, lv.dinv, h->powv[a_],
                                                   h->nrm2 + a_, h->powv[b_], h->part, h->cnt, h->nrm2 + b_);
             }
             k_omega_pow<<<1, 1, 0, st>>>(h->nrm2 + (h->o.power_iters & 1), h->omega + l);

@@ -1084,7 +1084,9 @@ def run_c3(args):
         tm = time.perf_counter() - tm0
         errs = {k2: float(np.linalg.norm(getattr(sm, k2).values - v) / max(np.linalg.norm(v), 1e-300))
                 for k2, v in ref.items()}
+        t64 = sum(a.elapsed_time(b) for a, b in evs[:ncmp]) / 1e3
         mixed = {"value": round(ncmp / tm, 4), "unit": "steps/s", "steps": ncmp, "field_error": errs,
+                 "fp64_same_steps": round(ncmp / t64, 4) if t64 > 0 else None,
                  "desc": "the same workload in the mixed form: the momentum, volume-fraction and energy systems "
                          "(ILU(0)) on the graph engine's FP32 form (FP32 vectors and values, FP64 iterate, residual "
                          "replacement against the FP64 matrix, the same 1e-12 FP64 stopping test), the multigrid p' "

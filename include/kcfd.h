@@ -39,6 +39,12 @@ extern "C" {
 #define KCFD_STOP_GPU    1  /* core/gpu_solver.py:111-155: ||s||/||b||, ||r||/||b|| < tol,
                                1e-30 guards                                            */
 
+/* Krylov methods */
+#define KCFD_METHOD_BICGSTAB 0  /* scipy bicgstab (core/linear_solver.py:59)             */
+#define KCFD_METHOD_CG       1  /* scipy cg: solve_pressure_correction's iterative branch
+                                   (core/linear_solver.py:90-92); one right-hand side,
+                                   FP64, scipy stop, graph engine (team 0 or 3)          */
+
 /* precision modes */
 #define KCFD_MODE_FP64   0  /* plain FP64                                            */
 #define KCFD_MODE_MIXED  1  /* FP32 inner BiCGSTAB, FP64 residual + refinement + dots */
@@ -224,6 +230,7 @@ typedef struct {
                             this is the structural form)                        */
     int32_t amg_max_levels; /* KCFD_PREC_AMG: kcfd_amg_opts_t.max_levels (0: 12)    */
     int32_t amg_coarse_max; /* KCFD_PREC_AMG: kcfd_amg_opts_t.coarse_max (0: 128)   */
+    int32_t method;      /* KCFD_METHOD_* (0: BiCGSTAB)                             */
 } kcfd_solver_opts_t;
 /* KCFD_PREC_AMG: one right-hand side, graph engine only (team 0 or 3). The handle
  * builds a kcfd_amg hierarchy on the pattern at creation and refreshes it in

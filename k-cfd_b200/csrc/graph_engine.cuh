@@ -908,6 +908,198 @@ __global__ void __launch_bounds__(kBlock) g_rr(ArgsT<T> a) {
     }
 }
 
+// ---------------------------------------------------------------- CG (one rhs) --
+// Preconditioned conjugate gradients with scipy's loop (scipy.sparse.linalg.cg, the
+// reference's solve_pressure_correction, core/linear_solver.py:73-93): r = b - A x; each
+// iteration z = M^-1 r, rho = r.z, p = z (first) or z + (rho / rho_prev) p, q = A p,
+// alpha = rho / p.q, x += alpha p, r -= alpha q; done once ||r|| < max(atol, rtol ||b||),
+// tested before every iteration. FP64, one right-hand side. z lives in sh (r itself
+// without a preconditioner), q in v.
+
+__global__ void __launch_bounds__(kBlock) g_cg_init(Args a) {
+    St& S = *a.st;
+    double red[2] = {0.0, 0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double acc[1] = {0.0};
+        int base, w;
+        sell_row(a.A64, i, base, w);
+        sell_gather<1>(a.A64, base, w, a.x, acc);
+        const double bb = a.b[i], rr = bb - acc[0];
+        a.r[i] = rr;
+        red[0] += bb * bb;
+        red[1] += rr * rr;
+    }
+    if (last_block_sum<2>(a, 0, red) && threadIdx.x == 0) {
+        S.bnorm[0] = sqrt(red[0]);
+        S.rnorm[0] = sqrt(red[1]);
+        S.thr[0] = fmax(a.atol, a.rtol * S.bnorm[0]);
+        S.rho[0] = S.rho_prev[0] = S.alpha[0] = S.beta[0] = 0.0;
+        S.iters[0] = 0;
+        S.sconv[0] = 0;
+        S.status[0] = KCFD_OK;
+        S.zero_x[0] = S.bnorm[0] == 0.0;  // scipy returns b
+        S.done[0] = S.zero_x[0] || S.rnorm[0] < S.thr[0];
+        if (!isfinite(red[0]) || !isfinite(red[1])) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_BREAKDOWN;
+        }
+        if (!S.done[0] && a.maxiter <= 0) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_MAXITER;
+        }
+        S.it = 0;
+        S.trips = 0;
+        S.active = !S.done[0];
+        if (!a.eager) cudaGraphSetConditional(a.cond, S.active ? 1u : 0u);
+    }
+}
+
+// rho = r.z (Jacobi: z = D^-1 r, stored); beta.
+template <int PREC>
+__global__ void __launch_bounds__(kBlock) g_cg_rz(Args a) {
+    pdl_enter();
+    St& S = *a.st;
+    if (blockIdx.x == 0 && threadIdx.x == 0) S.trips += 1;
+    if (!S.active) return;
+    double red[1] = {0.0};
+    const int stride = gridDim.x * blockDim.x;
+    for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += 4 * stride) {
+        double R[4], Z[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * stride;
+            if (i >= a.n) continue;
+            R[u] = a.r[i];
+            if (PREC == KCFD_PREC_JACOBI) Z[u] = __ldg(a.dinv + i) * R[u];
+            else if (PREC == KCFD_PREC_NONE) Z[u] = R[u];
+            else Z[u] = a.sh[i];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * stride;
+            if (i >= a.n) continue;
+            if (PREC == KCFD_PREC_JACOBI) a.sh[i] = Z[u];
+            red[0] += R[u] * Z[u];
+        }
+    }
+    if (last_block_sum<1>(a, 1, red) && threadIdx.x == 0) {
+        S.rho[0] = red[0];
+        S.beta[0] = S.it > 0 ? S.rho[0] / S.rho_prev[0] : 0.0;
+        if (S.it > 0 && !isfinite(S.beta[0])) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_BREAKDOWN;
+            S.iters[0] = S.it;
+            S.active = 0;
+            if (!a.eager) cudaGraphSetConditional(a.cond, 0u);
+        }
+    }
+}
+
+// p = z (first iteration) or z + beta p.
+template <int PREC>
+__global__ void __launch_bounds__(kBlock) g_cg_p(Args a) {
+    pdl_enter();
+    const St& S = *a.st;
+    if (!S.active) return;
+    const double be = S.beta[0];
+    const bool first = S.it == 0;
+    const double* z = PREC == KCFD_PREC_NONE ? a.r : a.sh;
+    const int stride = gridDim.x * blockDim.x;
+    for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += 4 * stride) {
+        double Z[4], P[4];
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * stride;
+            if (i >= a.n) continue;
+            Z[u] = z[i];
+            P[u] = first ? 0.0 : a.p[i];
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const int i = i0 + u * stride;
+            if (i >= a.n) continue;
+            a.p[i] = first ? Z[u] : P[u] * be + Z[u];
+        }
+    }
+}
+
+// q = A p (in v), p.q, alpha.
+__global__ void __launch_bounds__(kBlock) g_cg_q(Args a) {
+    pdl_enter();
+    St& S = *a.st;
+    if (!S.active) return;
+    double red[1] = {0.0};
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < a.n; i += gridDim.x * blockDim.x) {
+        double acc[1] = {0.0};
+        int base, w;
+        sell_row(a.A, i, base, w);
+        sell_gather<1>(a.A, base, w, a.p, acc);
+        a.v[i] = acc[0];
+        red[0] += a.p[i] * acc[0];
+    }
+    if (last_block_sum<1>(a, 2, red) && threadIdx.x == 0) {
+        S.alpha[0] = S.rho[0] / red[0];
+        if (!isfinite(S.alpha[0])) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_BREAKDOWN;
+            S.iters[0] = S.it;
+            S.active = 0;
+            if (!a.eager) cudaGraphSetConditional(a.cond, 0u);
+        }
+    }
+}
+
+// x += alpha p, r -= alpha q, ||r||; the stopping tests and the loop condition.
+__global__ void __launch_bounds__(kBlock) g_cg_xr(Args a) {
+    pdl_enter();
+    St& S = *a.st;
+    if (!a.eager && blockIdx.x == 0 && threadIdx.x == 0 && S.trips > a.maxiter + 2) cudaGraphSetConditional(a.cond, 0u);
+    if (!S.active) return;
+    const double al = S.alpha[0];
+    double red[1] = {0.0};
+    const int stride = gridDim.x * blockDim.x;
+    for (int i0 = blockIdx.x * blockDim.x + threadIdx.x; i0 < a.n; i0 += 2 * stride) {
+        double X[2], P[2], R[2], Q[2];
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int i = i0 + u * stride;
+            if (i >= a.n) continue;
+            X[u] = a.x[i];
+            P[u] = a.p[i];
+            R[u] = a.r[i];
+            Q[u] = a.v[i];
+        }
+#pragma unroll
+        for (int u = 0; u < 2; ++u) {
+            const int i = i0 + u * stride;
+            if (i >= a.n) continue;
+            a.x[i] = X[u] + al * P[u];
+            const double rn = R[u] - al * Q[u];
+            a.r[i] = rn;
+            red[0] += rn * rn;
+        }
+    }
+    if (last_block_sum<1>(a, 4, red) && threadIdx.x == 0) {
+        S.rho_prev[0] = S.rho[0];
+        S.rnorm[0] = sqrt(red[0]);
+        S.it += 1;
+        S.iters[0] = S.it;
+        // scipy tests before an iteration only: after the last one it reports maxiter
+        if (!isfinite(S.rnorm[0])) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_BREAKDOWN;
+        } else if (S.it >= a.maxiter) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_MAXITER;
+        } else if (S.rnorm[0] < S.thr[0]) {
+            S.done[0] = 1;
+            S.status[0] = KCFD_OK;
+        }
+        S.active = !S.done[0];
+        if (!a.eager) cudaGraphSetConditional(a.cond, (S.active && S.trips <= a.maxiter + 2) ? 1u : 0u);
+    }
+}
+
 // Results; x = 0 for right-hand sides with b == 0 (scipy returns b), over the grid.
 template <int NRHS, typename T>
 __global__ void g_final(ArgsT<T> a) {

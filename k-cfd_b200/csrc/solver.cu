@@ -1544,13 +1544,60 @@ void ge_fill_values(kcfd_solver* s, const double* vals, cudaStream_t st) {
         ge::g_diff32<<<ge_fill_grid(s, s->n), 256, 0, st>>>(s->n, s->g.A, s->g.A32.val);
 }
 
+// CG (one right-hand side, FP64): grids of its phase kernels, and one loop trip.
+struct CgGrid {
+    int init, rz, p, q, xr;
+};
+
+template <int PREC>
+CgGrid cg_grids(int n, int sms, int gmax) {
+    auto g = [&](const void* f, int rows_per_thread) {
+        int occ = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, f, ge::kBlock, 0) != cudaSuccess || occ < 1) occ = 1;
+        const int64_t per = (int64_t)ge::kBlock * rows_per_thread;
+        const int64_t need = ((int64_t)n + per - 1) / per;
+        return (int)std::max<int64_t>(1, std::min<int64_t>({(int64_t)occ * sms, need, (int64_t)gmax}));
+    };
+    CgGrid r;
+    r.init = g((const void*)ge::g_cg_init, 1);
+    r.rz = g((const void*)ge::g_cg_rz<PREC>, 4);
+    r.p = g((const void*)ge::g_cg_p<PREC>, 4);
+    r.q = g((const void*)ge::g_cg_q, 1);
+    r.xr = g((const void*)ge::g_cg_xr, 2);
+    return r;
+}
+
+// z = M^-1 r (ILU sweeps from r into shat, or one V-cycle), rho and beta, p, q = A p
+// and alpha, then x, r and the tests. Jacobi's z is formed in g_cg_rz.
+template <int PREC>
+void cg_body(const ge::Args& a, const GeGrid& G, const CgGrid& C, cudaStream_t cs, bool pdl) {
+    if constexpr (PREC == KCFD_PREC_AMG) {
+        amg::vcycle((const kcfd_amg*)a.amg, a.r, a.sh, &a.st->active, cs, pdl);
+    } else if constexpr (PREC == KCFD_PREC_ILU0) {
+        for (int l = 1; l < a.nlev; ++l) ge_launch(ge::g_fwd<1, double>, G.fwd, cs, pdl, a, l, 1);
+        for (int l = a.nlev - 2; l >= 0; --l) ge_launch(ge::g_bwd<1, double>, G.bwd, cs, pdl, a, l, 1);
+    }
+    ge_launch(ge::g_cg_rz<PREC>, C.rz, cs, pdl, a);
+    ge_launch(ge::g_cg_p<PREC>, C.p, cs, pdl, a);
+    ge_launch(ge::g_cg_q, C.q, cs, pdl, a);
+    ge_launch(ge::g_cg_xr, C.xr, cs, pdl, a);
+}
+
 // Eager form: init, body trips in chunks with a host read of the active flag, final.
 template <int NRHS, int PREC, typename T>
 int ge_eager(kcfd_solver* s, cudaStream_t st) {
     const ge::ArgsT<T>& a = ge_args<T>(s);
     const GeGrid G = ge_grids<NRHS, PREC, T>(s->n, s->sm_count, s->g.gmax);
+    const bool cg = s->o.method == KCFD_METHOD_CG;
+    CgGrid C{};
     ge_fill_values<T>(s, s->g.vals_key, st);
-    ge::g_init<NRHS, T><<<G.init, ge::kBlock, 0, st>>>(a);
+    if constexpr (NRHS == 1 && !ge::is_mixed<T>()) {
+        if (cg) {
+            C = cg_grids<PREC>(s->n, s->sm_count, s->g.gmax);
+            ge::g_cg_init<<<C.init, ge::kBlock, 0, st>>>(a);
+        }
+    }
+    if (!cg) ge::g_init<NRHS, T><<<G.init, ge::kBlock, 0, st>>>(a);
     KCFD_CUDA(cudaGetLastError());
     constexpr int kChunk = 8;
     for (int trips = 0; trips <= a.maxiter + 2; trips += kChunk) {
@@ -1558,7 +1605,15 @@ int ge_eager(kcfd_solver* s, cudaStream_t st) {
         KCFD_CUDA(cudaMemcpyAsync(&active, &a.st->active, sizeof(int), cudaMemcpyDeviceToHost, st));
         KCFD_CUDA(cudaStreamSynchronize(st));
         if (!active) break;
-        for (int k = 0; k < kChunk; ++k) ge_body<NRHS, PREC, T>(a, G, st, s->g.pdl);
+        for (int k = 0; k < kChunk; ++k) {
+            if constexpr (NRHS == 1 && !ge::is_mixed<T>()) {
+                if (cg) {
+                    cg_body<PREC>(a, G, C, st, s->g.pdl);
+                    continue;
+                }
+            }
+            ge_body<NRHS, PREC, T>(a, G, st, s->g.pdl);
+        }
         KCFD_CUDA(cudaGetLastError());
     }
     ge::g_final<NRHS, T><<<ge_fill_grid(s, s->n), 256, 0, st>>>(a);
@@ -1657,11 +1712,20 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
         KCFD_CUDA(cudaGraphAddKernelNode(&n_diff, g.graph, &n_fill, 1, &kd));
         n_fill = n_diff;
     }
+    const bool cg = s->o.method == KCFD_METHOD_CG;
+    CgGrid C{};
     void* args[] = {&a};
     cudaKernelNodeParams kp;
     std::memset(&kp, 0, sizeof(kp));
     kp.func = (void*)ge::g_init<NRHS, T>;
     kp.gridDim = dim3(G.init);
+    if constexpr (NRHS == 1 && !ge::is_mixed<T>()) {
+        if (cg) {
+            C = cg_grids<PREC>(n, s->sm_count, g.gmax);
+            kp.func = (void*)ge::g_cg_init;
+            kp.gridDim = dim3(C.init);
+        }
+    }
     kp.blockDim = dim3(ge::kBlock);
     kp.kernelParams = args;
     KCFD_CUDA(cudaGraphAddKernelNode(&n_init, g.graph, &n_fill, 1, &kp));
@@ -1678,7 +1742,14 @@ int ge_build(kcfd_solver* s, const kcfd_csr_t* A) {
     KCFD_CUDA(cudaStreamCreateWithFlags(&cs, cudaStreamNonBlocking));
     cudaError_t e = cudaStreamBeginCaptureToGraph(cs, body, nullptr, nullptr, 0, cudaStreamCaptureModeThreadLocal);
     if (e == cudaSuccess) {
-        ge_body<NRHS, PREC, T>(a, G, cs, g.pdl);
+        bool done = false;
+        if constexpr (NRHS == 1 && !ge::is_mixed<T>()) {
+            if (cg) {
+                cg_body<PREC>(a, G, C, cs, g.pdl);
+                done = true;
+            }
+        }
+        if (!done) ge_body<NRHS, PREC, T>(a, G, cs, g.pdl);
         cudaGraph_t outg = nullptr;
         const cudaError_t e2 = cudaStreamEndCapture(cs, &outg);
         if (e == cudaSuccess) e = e2;
@@ -1968,6 +2039,12 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     KCFD_REQUIRE(!(opts->mode == KCFD_MODE_MIXED && opts->stop == KCFD_STOP_GPU),
                  "kcfd_solver_create: MIXED mode uses the scipy stopping rule");
     KCFD_REQUIRE(opts->maxiter >= 0, "kcfd_solver_create: maxiter < 0");
+    KCFD_REQUIRE(opts->method == KCFD_METHOD_BICGSTAB || opts->method == KCFD_METHOD_CG, "kcfd_solver_create: bad method");
+    const bool cg = opts->method == KCFD_METHOD_CG;
+    KCFD_REQUIRE(!cg || (opts->nrhs == 1 && opts->mode == KCFD_MODE_FP64 && opts->stop == KCFD_STOP_SCIPY &&
+                         (opts->team == 0 || opts->team == 3)),
+                 "kcfd_solver_create: CG takes one right-hand side, FP64 and the scipy stop rule, and runs on the "
+                 "graph engine (team 0 or 3)");
     auto* s = new kcfd_solver();
     s->o = *opts;
     // AMG: the Krylov iteration is FP64 on the graph engine; MIXED selects an FP32
@@ -2024,7 +2101,7 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
     // a 4,096-row p' system: one CTA 35 us per Krylov iteration, the grid kernel 18 us,
     // the graph engine 25 us. A caller that runs many small solves concurrently (the
     // served loop) asks for one CTA explicitly, so that they overlap.
-    int team = amg ? 3 : opts->team;
+    int team = (amg || cg) ? 3 : opts->team;
     if (team == 0) {
         const int64_t unk = (int64_t)n * nrhs;
         // MIXED stays on the persistent kernel (FP32 inner iterations, FP64 refinement
@@ -2167,6 +2244,8 @@ int kcfd_solver_create(const kcfd_csr_t* A, const kcfd_solver_opts_t* opts, cons
         lptr = {0, n};
         s->nlev = 1;
     }
+    if (cg && opts->precond == KCFD_PREC_ILU0 && s->nlev < 2)
+        return fail("kcfd_solver_create: CG with ILU(0) needs a matrix with at least two ILU levels");
     // team 3 keeps the grid kernel's launch shape too: it factors ILU(0) with the
     // grid factor kernel and solves on the grid kernel inside stream captures
     void* kern = amg ? nullptr : solve_kernel_ptr(mixed, nrhs, opts->precond, team >= 2, s->block);

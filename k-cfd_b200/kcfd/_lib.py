@@ -17,6 +17,7 @@ STATUS_NAMES = {0: "OK", 1: "MAXITER", 2: "BREAKDOWN", 3: "BAD_INPUT", 4: "CUDA_
 PREC = {"none": 0, "jacobi": 1, "ilu0": 2, "amg": 3}
 STOP_SCIPY, STOP_GPU = 0, 1
 MODE_FP64, MODE_MIXED = 0, 1
+METHOD_BICGSTAB, METHOD_CG = 0, 1
 
 i32, i64, f64, vp = C.c_int32, C.c_int64, C.c_double, C.c_void_p
 P_i32, P_i64, P_f64 = C.POINTER(C.c_int32), C.POINTER(C.c_int64), C.POINTER(C.c_double)
@@ -48,7 +49,7 @@ class SolverOpts(C.Structure):
     _fields_ = [("precond", i32), ("stop", i32), ("mode", i32), ("nrhs", i32), ("maxiter", i32), ("team", i32),
                 ("lanes", i32), ("block", i32), ("rtol", f64), ("atol", f64), ("inner_rtol", f64),
                 ("max_refine", i32), ("inner_maxiter", i32), ("fill_level", i32), ("amg_max_levels", i32),
-                ("amg_coarse_max", i32)]
+                ("amg_coarse_max", i32), ("method", i32)]
 
 
 class AmgOpts(C.Structure):

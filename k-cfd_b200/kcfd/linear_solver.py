@@ -133,7 +133,29 @@ def solve_linear_system(system, x0=None, method="direct", tol=1e-8, maxiter=1000
 
 def solve_pressure_correction(system, method="direct", tol=1e-6, maxiter=2000, preconditioner="none",
                               **precond_kwargs):
-    """core/linear_solver.py:73-93. The reference uses CG (atol=tol) for the iterative
-    branch; the device path uses BiCGSTAB with the same absolute threshold."""
-    m = "direct" if method == "direct" else "bicgstab"
-    return solve_linear_system(system, None, m, tol, maxiter, "b200", preconditioner, **precond_kwargs)
+    """core/linear_solver.py:73-93: 'direct' as solve_linear_system; any other method runs
+    scipy's conjugate gradients from x0 = 0 with atol=tol (and scipy's default rtol) and
+    the given preconditioner, on the device (the graph engine's CG)."""
+    if method == "direct":
+        return solve_linear_system(system, None, "direct", tol, maxiter, "b200", preconditioner, **precond_kwargs)
+    torch = _lib.require_cuda()
+    rtol = precond_kwargs.pop("rtol", SCIPY_DEFAULT_RTOL)
+    d, b, levels = _as_device(system)
+    levels = precond_kwargs.pop("levels", levels)
+    prec, fill = preconditioner, 0
+    if prec == "iluk":
+        prec, fill, levels = "ilu0", int(precond_kwargs.pop("fill_level", 1)), None
+        precond_kwargs.pop("fill_factor", None)
+    amg_kw = {}
+    if prec == "amg":
+        amg_kw = {"amg_max_levels": int(precond_kwargs.pop("max_levels", 0)),
+                  "amg_coarse_max": min(int(precond_kwargs.pop("max_coarse", 0)), 256)}
+    x = torch.zeros(d.n, dtype=torch.float64, device=b.device)
+    s = Solver(d, precond=prec, stop=_lib.STOP_SCIPY, maxiter=maxiter, rtol=float(rtol), atol=float(tol),
+               levels=levels, fill_level=fill, method="cg", **amg_kw)
+    s.setup(d)
+    it, rr, st = s.solve(d, b, x)
+    status = int(st[0])
+    if status not in (_lib.OK, _lib.MAXITER, _lib.BREAKDOWN):
+        raise _lib.KcfdError(status, "device solve failed")
+    return x.cpu().numpy()

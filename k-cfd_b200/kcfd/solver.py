@@ -76,6 +76,8 @@ class DeviceCSR:
 class Solver:
     """BiCGSTAB handle for one pattern.
 
+    method: 'bicgstab' or 'cg' (scipy's conjugate gradients: one right-hand side, FP64, the
+    scipy stop rule, on the graph engine).
     precond: 'none' | 'jacobi' | 'ilu0' | 'amg' (smoothed-aggregation multigrid, one right-hand
     side, graph engine; mode MIXED keeps the Krylov iteration FP64 and stores the multigrid
     hierarchy in FP32); stop: _lib.STOP_SCIPY | _lib.STOP_GPU;
@@ -88,7 +90,7 @@ class Solver:
 
     def __init__(self, csr, precond="jacobi", stop=_lib.STOP_SCIPY, mode=_lib.MODE_FP64, nrhs=1, maxiter=1000,
                  rtol=1e-8, atol=0.0, team=0, lanes=0, block=0, inner_rtol=1e-3, max_refine=60, levels=None,
-                 inner_maxiter=400, fill_level=0, amg_max_levels=0, amg_coarse_max=0):
+                 inner_maxiter=400, fill_level=0, amg_max_levels=0, amg_coarse_max=0, method="bicgstab"):
         torch = _lib.require_cuda()
         if precond not in _lib.PREC:
             raise ValueError(f"Unknown preconditioner: {precond}")
@@ -99,6 +101,10 @@ class Solver:
         o.inner_maxiter = int(inner_maxiter)
         o.fill_level = int(fill_level)
         o.amg_max_levels, o.amg_coarse_max = int(amg_max_levels), int(amg_coarse_max)
+        if method not in ("bicgstab", "cg"):
+            raise ValueError(f"Unknown Krylov method: {method}")
+        o.method = _lib.METHOD_CG if method == "cg" else _lib.METHOD_BICGSTAB
+        self.method = method
         self.opts = o
         self.n, self.nrhs, self.mode = csr.n, nrhs, mode
         self.precond = precond

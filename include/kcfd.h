@@ -349,6 +349,11 @@ typedef struct {
  * local column indices, concatenated (host arrays, copied to the device).          */
 int  kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const int32_t* indptr_host,
                        const int32_t* indices_host, const kcfd_batch_opts_t* opts, kcfd_batch** out);
+/* The team each system of a batch would get on a device with sm_count SMs (host only, no
+ * device call; every cluster size taken as resident): team[s] = CTAs of its thread-block
+ * cluster (2, 4 or 8), 1 for one 512-thread CTA, 0 for one 256-thread CTA. The same rule
+ * as kcfd_batch_create. No counterpart in the reference (batching is this library's).  */
+int  kcfd_batch_plan(int32_t nsys, const int32_t* n, const kcfd_batch_opts_t* opts, int32_t sm_count, int32_t* team);
 void kcfd_batch_destroy(kcfd_batch* b);
 /* info[0..3] = nsys, total rows, total entries, CTAs per launch */
 int  kcfd_batch_info(const kcfd_batch* b, int64_t* info);

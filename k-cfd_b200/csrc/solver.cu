@@ -2536,6 +2536,37 @@ void* batch_cluster_ptr(int mixed, int precond) {
     return precond == KCFD_PREC_JACOBI ? (void*)batch_cluster_kernel<0, KCFD_PREC_JACOBI>
                                        : (void*)batch_cluster_kernel<0, KCFD_PREC_NONE>;
 }
+// The cluster tiers a batch asks for (largest teams first): their team sizes and row
+// thresholds; graded (cluster_size 0) or one tier. Host only: whether a cluster of a
+// size can be resident is checked by the caller.
+int cluster_candidates(int nsys, const int32_t* n, const kcfd_batch_opts_t& o, int sms, int* cand_size, int* cand_rows) {
+    int ncand = 0;
+    if (o.cluster_rows < 0) return 0;
+    if (o.cluster_size == 0) {
+        int64_t R = o.cluster_rows;
+        if (R == 0) {
+            R = kGradedRows;
+            for (;; R *= 2) {
+                int64_t demand = 0;
+                for (int s = 0; s < nsys; ++s) {
+                    const int64_t q = n[s] / R;
+                    demand += q >= 8 ? 8 : q >= 4 ? 4 : q >= 2 ? 2 : 0;
+                }
+                if (demand <= (int64_t)(kClusterDemand * sms) || R > INT32_MAX / 16) break;
+            }
+        }
+        for (int c = 8; c >= 2; c >>= 1) {
+            cand_size[ncand] = c;
+            cand_rows[ncand++] = (int)std::min<int64_t>((int64_t)c * R, INT32_MAX);
+        }
+    } else {
+        cand_size[0] = o.cluster_size;
+        cand_rows[0] = o.cluster_rows == 0 ? 131072 : o.cluster_rows;
+        ncand = 1;
+    }
+    return ncand;
+}
+
 cudaLaunchConfig_t cluster_config(int clusters, int csize, cudaStream_t st, cudaLaunchAttribute* at) {
     cudaLaunchConfig_t cfg;
     std::memset(&cfg, 0, sizeof(cfg));
@@ -2630,31 +2661,8 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
         return KCFD_BAD_INPUT;
     }
     // candidate cluster tiers (largest teams first) and their row thresholds
-    int cand_size[kcfd_batch::kMaxClTiers], cand_rows[kcfd_batch::kMaxClTiers], ncand = 0;
-    if (b->o.cluster_rows >= 0) {
-        if (csize == 0) {
-            int64_t R = b->o.cluster_rows;
-            if (R == 0) {
-                R = kGradedRows;
-                for (;; R *= 2) {
-                    int64_t demand = 0;
-                    for (int s = 0; s < nsys; ++s) {
-                        const int64_t q = n[s] / R;
-                        demand += q >= 8 ? 8 : q >= 4 ? 4 : q >= 2 ? 2 : 0;
-                    }
-                    if (demand <= (int64_t)(kClusterDemand * sms) || R > INT32_MAX / 16) break;
-                }
-            }
-            for (int c = 8; c >= 2; c >>= 1) {
-                cand_size[ncand] = c;
-                cand_rows[ncand++] = (int)std::min<int64_t>((int64_t)c * R, INT32_MAX);
-            }
-        } else {
-            cand_size[0] = csize;
-            cand_rows[0] = b->o.cluster_rows == 0 ? 131072 : b->o.cluster_rows;
-            ncand = 1;
-        }
-    }
+    int cand_size[kcfd_batch::kMaxClTiers], cand_rows[kcfd_batch::kMaxClTiers];
+    const int ncand = cluster_candidates(nsys, n, b->o, sms, cand_size, cand_rows);
     // keep the tiers whose clusters can be resident (a dropped tier's systems fall to
     // the next one down)
     int ncl_max[kcfd_batch::kMaxClTiers];
@@ -2728,6 +2736,25 @@ int kcfd_batch_create(int32_t nsys, const int32_t* n, const int32_t* nnz, const 
 }
 
 void kcfd_batch_destroy(kcfd_batch* b) { free_batch(b); }
+
+int kcfd_batch_plan(int32_t nsys, const int32_t* n, const kcfd_batch_opts_t* opts, int32_t sm_count, int32_t* team) {
+    KCFD_REQUIRE(n && opts && team, "kcfd_batch_plan: NULL argument");
+    KCFD_REQUIRE(nsys > 0 && sm_count > 0, "kcfd_batch_plan: nsys and sm_count must be > 0");
+    KCFD_REQUIRE(opts->cluster_size == 0 || (opts->cluster_size >= 2 && opts->cluster_size <= 8),
+                 "kcfd_batch_plan: cluster_size must be 0 (graded) or 2..8");
+    int cand_size[kcfd_batch::kMaxClTiers], cand_rows[kcfd_batch::kMaxClTiers];
+    const int ncand = cluster_candidates(nsys, n, *opts, sm_count, cand_size, cand_rows);
+    const int big_rows = opts->big_rows == 0 ? 16384 : opts->big_rows;
+    for (int s = 0; s < nsys; ++s) {
+        team[s] = (big_rows > 0 && n[s] >= big_rows) ? 1 : 0;
+        for (int t = 0; t < ncand; ++t)
+            if (n[s] >= cand_rows[t]) {
+                team[s] = cand_size[t];
+                break;
+            }
+    }
+    return KCFD_OK;
+}
 
 int kcfd_batch_info(const kcfd_batch* b, int64_t* info) {
     KCFD_REQUIRE(b && info, "kcfd_batch_info: NULL argument");

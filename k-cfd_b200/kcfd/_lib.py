@@ -126,6 +126,7 @@ SIGNATURES = {
     "kcfd_op_cells": (i32, [vp, i32, f64, f64, vp, vp, vp, vp, vp, vp]),
     "kcfd_muscl_correction": (i32, [vp, i32, vp, vp, vp, vp, vp]),
     "kcfd_batch_create": (i32, [i32, vp, vp, vp, vp, vp, C.POINTER(vp)]),
+    "kcfd_batch_plan": (i32, [i32, vp, vp, i32, vp]),
     "kcfd_batch_destroy": (None, [vp]),
     "kcfd_batch_info": (i32, [vp, P_i64]),
     "kcfd_batch_tiers": (i32, [vp, P_i32]),

@@ -106,6 +106,19 @@ class BatchSolver:
         return [v[self.row_off[s]:self.row_off[s + 1]] for s in range(self.nsys)]
 
 
+def plan_teams(sizes, sm_count=148, cluster_rows=0, cluster_size=0, big_rows=0):
+    """The team each system of a batch of these row counts gets (kcfd_batch_plan, host
+    only): CTAs of its thread-block cluster (2, 4, 8), 1 for one 512-thread CTA, 0 for one
+    256-thread CTA."""
+    n = np.ascontiguousarray(sizes, dtype=np.int32)
+    o = BatchOpts()
+    o.cluster_rows, o.cluster_size, o.big_rows = int(cluster_rows), int(cluster_size), int(big_rows)
+    team = np.zeros(len(n), dtype=np.int32)
+    _lib.check(_lib.lib().kcfd_batch_plan(len(n), n.ctypes.data, C.byref(o), int(sm_count), team.ctypes.data),
+               "kcfd_batch_plan")
+    return team
+
+
 def lpt_shards(weights, nranks):
     """Greedy longest-processing-time assignment of systems to ranks (largest first,
     each to the currently lightest rank). Returns a list of index lists."""

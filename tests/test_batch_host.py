@@ -30,3 +30,30 @@ def test_lpt_shards_cover_every_system_once():
         assert flat == list(range(1024))
         loads = [sizes[s].sum() for s in shards]
         assert max(loads) - min(loads) <= sizes.max()
+
+
+def test_graded_teams_follow_the_batch():
+    """kcfd_batch_plan (host only, the rule kcfd_batch_create applies), on the C4 size
+    distribution: a 128-system batch spreads its big systems over clusters of 8, 4 and 2
+    CTAs (R = 8192 rows), the full 1,024 keeps all but the largest on one CTA (R = 65536:
+    clusters of 2 from 131,072 rows) -- R is the smallest 8192 * 2^k whose cluster teams ask
+    for at most 3.5 CTAs per SM."""
+    from kcfd.batch import p_prime_sizes, plan_teams
+    sizes = np.asarray(p_prime_sizes(1024, 2000, 200000, 0))
+    t128 = plan_teams(sizes[:128])
+    n = sizes[:128]
+    assert ((t128 >= 2).sum(), (t128 == 1).sum(), (t128 == 0).sum()) == (75, 0, 53)
+    np.testing.assert_array_equal(t128, np.where(n >= 8 * 8192, 8, np.where(n >= 4 * 8192, 4,
+                                                                            np.where(n >= 2 * 8192, 2, 0))))
+    t1024 = plan_teams(sizes)
+    np.testing.assert_array_equal(t1024, np.where(sizes >= 131072, 2, np.where(sizes >= 16384, 1, 0)))
+
+    def demand(n, R):
+        q = n // R
+        return int(np.where(q >= 8, 8, np.where(q >= 4, 4, np.where(q >= 2, 2, 0))).sum())
+    assert demand(sizes, 32768) > 3.5 * 148 >= demand(sizes, 65536)
+    assert demand(n, 8192) <= 3.5 * 148
+    # one tier of 4 CTAs from 131,072 rows; no clusters at all
+    t4 = plan_teams(sizes, cluster_size=4)
+    np.testing.assert_array_equal(t4 == 4, sizes >= 131072)
+    assert (plan_teams(sizes, cluster_rows=-1) <= 1).all()

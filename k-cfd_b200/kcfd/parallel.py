@@ -204,11 +204,17 @@ class HaloExchange:
 
 
 class DistributedBiCGSTAB:
-    """scipy's BiCGSTAB loop (stop at ||r|| < max(atol, rtol ||b||)) with Jacobi, over
-    the ranks of a group. vals: this rank's entries (plan.src order); b: its rows.
-    spmv(x_ext, y) computes y = A_local x_ext; default: the device kernel."""
+    """scipy's BiCGSTAB loop (stop at ||r|| < max(atol, rtol ||b||)) over the ranks of a
+    group. vals: this rank's entries (plan.src order); b: its rows. spmv(x_ext, y) computes
+    y = A_local x_ext; default: the device kernel.
 
-    def __init__(self, plan, vals, group=None, spmv=None, device=None):
+    precond: 'jacobi', or 'block_ilu0' -- ILU(0) of this rank's diagonal block (its own
+    rows and columns; the couplings to other ranks' rows are left out of the
+    preconditioner, block Jacobi over the ranks), so a preconditioner apply needs no
+    exchange. local_precond(r, z) -> z replaces the block's apply; default: the device
+    ILU(0) (kcfd_solver_apply_precond)."""
+
+    def __init__(self, plan, vals, group=None, spmv=None, device=None, precond="jacobi", local_precond=None):
         import torch
         self.torch = torch
         self.plan = plan
@@ -230,6 +236,36 @@ class DistributedBiCGSTAB:
             csr.n = plan.n_own
             spmv = lambda x, y: csr.spmv(x, y)
         self._spmv = spmv
+        if precond not in ("jacobi", "block_ilu0"):
+            raise ValueError(f"unknown distributed preconditioner {precond!r}")
+        self.precond = precond
+        if precond == "block_ilu0" and local_precond is None:
+            local_precond = self._device_block_ilu0(ip, np.asarray(plan.local_indices), v)
+        self._local_precond = local_precond
+
+    def _device_block_ilu0(self, ip, ix, v):
+        """The device ILU(0) of the own diagonal block (columns < n_own, natural-order levels)."""
+        torch = self.torch
+        from .solver import DeviceCSR, Solver
+        n = self.plan.n_own
+        keep = ix < n
+        rows_of = np.repeat(np.arange(n), np.diff(ip))
+        bip = np.zeros(n + 1, dtype=np.int32)
+        np.add.at(bip, rows_of[keep] + 1, 1)
+        bip = np.cumsum(bip).astype(np.int32)
+        csr = DeviceCSR(torch.from_numpy(bip).to(self.device),
+                        torch.from_numpy(np.ascontiguousarray(ix[keep], dtype=np.int32)).to(self.device),
+                        torch.from_numpy(np.ascontiguousarray(v[keep], dtype=np.float64)).to(self.device))
+        csr.n = n
+        s = Solver(csr, precond="ilu0")
+        s.setup(csr)
+        self._block = (csr, s)
+        return lambda r, z: s.apply_precond(csr, r, z)
+
+    def _apply(self, q):
+        if self.precond == "jacobi":
+            return self.dinv * q
+        return self._local_precond(q.contiguous(), self.torch.empty_like(q))
 
     def _dot(self, a, b):
         t = (a * b).sum().reshape(1)
@@ -273,7 +309,7 @@ class DistributedBiCGSTAB:
                 pvec = (pvec - omega * v) * beta + r
             else:
                 pvec = r.clone()
-            ph = self.dinv * pvec
+            ph = self._apply(pvec)
             v = self._matvec(ph, x_ext, torch.empty_like(b))
             rv = self._dot(rt, v)
             if rv == 0:
@@ -283,7 +319,7 @@ class DistributedBiCGSTAB:
             if self._dot(r, r) ** 0.5 < atol:
                 x = x + alpha * ph
                 return x, 0, it + 1
-            sh = self.dinv * r
+            sh = self._apply(r)
             t = self._matvec(sh, x_ext, torch.empty_like(b))
             omega = self._dot(t, r) / self._dot(t, t)
             x = x + alpha * ph + omega * sh

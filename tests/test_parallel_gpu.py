@@ -37,6 +37,11 @@ def test_one_rank_device_solve():
         assert np.linalg.norm(x.cpu().numpy() - xd) / np.linalg.norm(xd) < 1e-8
         _, info_o, its_o = bicgstab_scipy(A, b, np.zeros(len(b)), rtol=1e-10, atol=0.0, maxiter=3000, M=jacobi(A))
         assert abs(its - its_o) <= max(2, its_o // 10), (its, its_o)
+        # the block ILU(0) on the device (one rank: the block is the whole matrix)
+        s2 = DistributedBiCGSTAB(p, vals, precond="block_ilu0")
+        x2, info2, its2 = s2.solve(torch.from_numpy(b).cuda(), rtol=1e-10, maxiter=3000)
+        assert info2 == 0 and its2 < its, (its2, its)
+        assert np.linalg.norm(x2.cpu().numpy() - xd) / np.linalg.norm(xd) < 1e-8
     finally:
         if own:
             dist.destroy_process_group()

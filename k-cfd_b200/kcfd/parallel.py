@@ -22,12 +22,14 @@ parallel/mpi_solver.py:56-103):
   peers' rows with one all_to_all_single per exchange (NCCL on GPUs, gloo on CPU);
   each rank packs its send rows with index_select.
 - DistributedBiCGSTAB: scipy's BiCGSTAB loop with Jacobi (the reference's
-  preconditioner 'jacobi'), every dot product an all_reduce over the group, one halo
-  exchange before each local SpMV. The local SpMV is the device kernel
-  (kcfd_spmv_f64 on the extended local CSR); a caller may pass another operator.
+  preconditioner 'jacobi') or block-Jacobi ILU(0), the dot products all_reduced over
+  the group, one halo exchange before each local SpMV. The local SpMV is the device
+  kernel (kcfd_spmv_f64 on the extended local CSR); a caller may pass another operator.
 
-A partitioned solve needs one exchange per SpMV and two to three scalar all_reduces
-per half-step; ranks take the same collective steps in the same order.
+A partitioned solve needs one exchange per SpMV and three all_reduces per iteration:
+the dot products that do not depend on one another are reduced together as one short
+vector, (||r||, rt.r), (rt.v) and (||s||, t.s, t.t). Ranks take the same collective
+steps in the same order.
 """
 from __future__ import annotations
 
@@ -268,9 +270,17 @@ class DistributedBiCGSTAB:
         return self._local_precond(q.contiguous(), self.torch.empty_like(q))
 
     def _dot(self, a, b):
-        t = (a * b).sum().reshape(1)
-        self.torch.distributed.all_reduce(t, group=self.group)
-        return float(t.item())
+        return self._dots((a, b))[0]
+
+    def _dots(self, *pairs):
+        """The global dot products of the pairs with one all_reduce (one host sync). The
+        local sums keep the elementwise-product-then-sum form, so each value rounds as a
+        single dot's did (late in a tight solve rho = rt.r sits near scipy's absolute
+        eps**2 breakdown test, where the last bits decide)."""
+        torch = self.torch
+        t = torch.stack([(a * b).sum() for a, b in pairs])
+        torch.distributed.all_reduce(t, group=self.group)
+        return t.tolist()
 
     def _matvec(self, x_own, x_ext, y):
         x_ext[: self.plan.n_own].copy_(x_own)
@@ -297,9 +307,9 @@ class DistributedBiCGSTAB:
         rho_prev = omega = alpha = None
         pvec = v = None
         for it in range(maxiter):
-            if self._dot(r, r) ** 0.5 < atol:
+            rr, rho = self._dots((r, r), (rt, r))
+            if rr ** 0.5 < atol:
                 return x, 0, it
-            rho = self._dot(rt, r)
             if abs(rho) < eps2:
                 return x, -10, it
             if it > 0:
@@ -316,12 +326,15 @@ class DistributedBiCGSTAB:
                 return x, -11, it + 1
             alpha = rho / rv
             r = r - alpha * v
-            if self._dot(r, r) ** 0.5 < atol:
-                x = x + alpha * ph
-                return x, 0, it + 1
+            # ||s|| is reduced with (t, s) and (t, t): the half-step exit costs one more
+            # product on the last iteration, and the loop one all_reduce less per iteration
             sh = self._apply(r)
             t = self._matvec(sh, x_ext, torch.empty_like(b))
-            omega = self._dot(t, r) / self._dot(t, t)
+            ss, ts, tt = self._dots((r, r), (t, r), (t, t))
+            if ss ** 0.5 < atol:
+                x = x + alpha * ph
+                return x, 0, it + 1
+            omega = ts / tt
             x = x + alpha * ph + omega * sh
             r = r - omega * t
             rho_prev = rho

@@ -99,12 +99,21 @@ def _solve_worker(rank, world, port, out, precond="jacobi"):
             return z
     solver = DistributedBiCGSTAB(p, vals, spmv=spmv, device=torch.device("cpu"), precond=precond,
                                  local_precond=local)
-    x, info, its = solver.solve(torch.from_numpy(b[p.rows].copy()), rtol=1e-10, maxiter=2000)
+    reduce, calls = dist.all_reduce, []
+
+    def counted(*a, **k):
+        calls.append(1)
+        return reduce(*a, **k)
+    dist.all_reduce = counted
+    try:
+        x, info, its = solver.solve(torch.from_numpy(b[p.rows].copy()), rtol=1e-10, maxiter=2000)
+    finally:
+        dist.all_reduce = reduce
     full = torch.zeros(n, dtype=torch.float64)
     full[torch.from_numpy(p.rows)] = x
     dist.all_reduce(full)
     if rank == 0:
-        out.put((full.numpy().tolist(), info, its))
+        out.put((full.numpy().tolist(), info, its, len(calls)))
     dist.barrier()
     dist.destroy_process_group()
 
@@ -125,8 +134,8 @@ def test_two_rank_block_ilu0():
     """Block-Jacobi ILU(0) over the two ranks (each factors its own diagonal block, no
     exchange in an apply) converges to the direct solution in fewer iterations than
     Jacobi."""
-    x, info, its = _run_two_ranks("block_ilu0", 29700 + (os.getpid() + 500) % 1000)
-    xj, infoj, itsj = _run_two_ranks("jacobi", 29700 + (os.getpid() + 700) % 1000)
+    x, info, its, _ = _run_two_ranks("block_ilu0", 29700 + (os.getpid() + 500) % 1000)
+    xj, infoj, itsj, _ = _run_two_ranks("jacobi", 29700 + (os.getpid() + 700) % 1000)
     A, b = convdiff_system(channel_mesh(24, 18))
     xd = spla.spsolve(sparse.csc_matrix(A), b)
     assert info == 0 and infoj == 0
@@ -142,12 +151,14 @@ def test_two_rank_distributed_bicgstab():
     ps = [ctx.Process(target=_solve_worker, args=(r, 2, port, q)) for r in range(2)]
     for p in ps:
         p.start()
-    x, info, its = q.get(timeout=180)
+    x, info, its, n_reduce = q.get(timeout=180)
     for p in ps:
         p.join(timeout=120)
     A, b = convdiff_system(channel_mesh(24, 18))
     x = np.asarray(x)
     assert info == 0
+    # ||b|| and x.x, then three all_reduces per iteration (one more if the exit is at the top)
+    assert n_reduce <= 3 * its + 3, (n_reduce, its)
     xd = spla.spsolve(sparse.csc_matrix(A), b)
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-8
     _, info_o, its_o = bicgstab_scipy(A, b, np.zeros(len(b)), rtol=1e-10, atol=0.0, maxiter=2000, M=jacobi(A))

@@ -87,6 +87,46 @@ def test_noalloc_matches_handle_two_calls_in_a_row():
     np.testing.assert_array_equal(xn, first[0])
 
 
+def test_noalloc_records_into_a_cuda_graph():
+    """After one call on the device, a call records into a torch CUDA graph in global
+    capture mode, where a device allocation or a symbol look-up would invalidate the
+    capture; each replay gives the eager call's x, iterations and status bit for bit."""
+    import torch
+    from kcfd import _lib
+    from kcfd.solver import DeviceCSR
+    A, b = convdiff_system(channel_mesh(20, 20))
+    d = DeviceCSR.from_scipy(A)
+    x_ref, it_ref, st_ref = _noalloc(d, b, np.zeros(len(b)), "jacobi", 1e-10)   # the first call, before capture
+    assert st_ref == 0
+    bd = torch.from_numpy(np.ascontiguousarray(b)).cuda()
+    xd = torch.zeros_like(bd)
+    it = torch.zeros(1, dtype=torch.int32, device="cuda")
+    rr = torch.zeros(1, dtype=torch.float64, device="cuda")
+    st = torch.zeros(1, dtype=torch.int32, device="cuda")
+    desc = d.desc()
+    torch.cuda.synchronize()
+    g = torch.cuda.CUDAGraph()
+    s = torch.cuda.Stream()
+    s.wait_stream(torch.cuda.current_stream())
+    rc = []
+    with torch.cuda.stream(s):
+        with torch.cuda.graph(g, stream=s, capture_error_mode="global"):
+            rc.append(_lib.lib().kcfd_bicgstab_noalloc(
+                C.byref(desc), _lib.ptr(bd), _lib.ptr(xd), _lib.PREC["jacobi"], _lib.STOP_SCIPY, 1e-10, 0.0,
+                5000, _lib.ptr(it), _lib.ptr(rr), _lib.ptr(st), _lib.stream_handle(s)))
+    assert rc == [_lib.OK], _lib.last_error()
+    for _ in range(2):
+        xd.zero_()
+        it.zero_()
+        st.fill_(-1)
+        torch.cuda.synchronize()
+        g.replay()
+        torch.cuda.synchronize()
+        assert int(st[0]) == st_ref and int(it[0]) == it_ref
+        np.testing.assert_array_equal(xd.cpu().numpy(), x_ref)
+    del g
+
+
 def test_noalloc_rejects_oversized_systems():
     from kcfd import _lib
     from kcfd.solver import DeviceCSR

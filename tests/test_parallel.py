@@ -163,3 +163,50 @@ def test_two_rank_distributed_bicgstab():
     assert np.linalg.norm(x - xd) / np.linalg.norm(xd) < 1e-8
     _, info_o, its_o = bicgstab_scipy(A, b, np.zeros(len(b)), rtol=1e-10, atol=0.0, maxiter=2000, M=jacobi(A))
     assert info_o == 0 and abs(its - its_o) <= max(2, its_o // 10), (its, its_o)
+
+
+def _exchange_worker(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    from kcfd.parallel import HaloExchange
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        A, _ = convdiff_system(channel_mesh(24, 18))
+        A = sparse.csr_matrix(A)
+        n = A.shape[0]
+        part = np.random.default_rng(7).integers(0, world, n)   # scattered: every rank talks to every peer
+        p = HaloPlan(A.indptr, A.indices, part, rank)
+        x = np.sin(np.arange(n) * 0.37) + 2.0
+        x_ext = torch.zeros(p.n_own + p.n_ghost, dtype=torch.float64)
+        x_ext[: p.n_own] = torch.from_numpy(x[p.rows])
+        HaloExchange(p).exchange(x_ext)
+        Al = sparse.csr_matrix((A.data[p.src], p.local_indices, p.local_indptr), shape=(p.n_own, p.n_own + p.n_ghost))
+        ok_ghost = np.array_equal(x_ext[p.n_own:].numpy(), x[p.ghosts])
+        ok_prod = np.allclose(Al @ x_ext.numpy(), (A @ x)[p.rows], rtol=1e-14, atol=0.0)
+        out.put((rank, bool(ok_ghost), bool(ok_prod), p.n_own, p.n_ghost, sorted(p.recv), sorted(p.send)))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_three_rank_exchange_on_a_scattered_partition():
+    """Three gloo ranks, cells scattered over them at random (ragged counts, every rank
+    exchanging with both peers): after one exchange every ghost holds its owner's value and
+    every rank's local product equals its rows of the global product."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + (os.getpid() + 300) % 1000
+    ps = [ctx.Process(target=_exchange_worker, args=(r, 3, port, q)) for r in range(3)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=180) for _ in range(3))
+    for p in ps:
+        p.join(timeout=120)
+    assert [r[0] for r in res] == [0, 1, 2]
+    for rank, ok_ghost, ok_prod, n_own, n_ghost, recv, send in res:
+        assert ok_ghost and ok_prod, (rank, ok_ghost, ok_prod)
+        peers = [q for q in range(3) if q != rank]
+        assert recv == peers and send == peers, (rank, recv, send)
+    assert sum(r[3] for r in res) == 24 * 18 and len({r[3] for r in res}) > 1

@@ -334,7 +334,10 @@ class DistributedBiCGSTAB:
             if ss ** 0.5 < atol:
                 x = x + alpha * ph
                 return x, 0, it + 1
-            omega = ts / tt
+            # t = 0 (s = 0 under a zero stop threshold, or a singular operator): omega = 0,
+            # and the next iteration ends in one of scipy's breakdowns (-10 when s = 0,
+            # else -11) instead of a division by zero
+            omega = ts / tt if tt != 0.0 else 0.0
             x = x + alpha * ph + omega * sh
             r = r - omega * t
             rho_prev = rho

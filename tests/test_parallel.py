@@ -210,3 +210,47 @@ def test_three_rank_exchange_on_a_scattered_partition():
         peers = [q for q in range(3) if q != rank]
         assert recv == peers and send == peers, (rank, recv, send)
     assert sum(r[3] for r in res) == 24 * 18 and len({r[3] for r in res}) > 1
+
+
+def _exact_worker(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+    from kcfd.parallel import DistributedBiCGSTAB
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        n = 6
+        A = sparse.csr_matrix(sparse.identity(n) * 2.0)    # solved exactly in one half-step
+        part = (np.arange(n) * world) // n
+        p = HaloPlan(A.indptr, A.indices, part, rank)
+        Al = sparse.csr_matrix((A.data[p.src], p.local_indices, p.local_indptr), shape=(p.n_own, p.n_own + p.n_ghost))
+
+        def spmv(x_ext, y):
+            y.copy_(torch.from_numpy(Al @ x_ext.numpy()))
+            return y
+        s = DistributedBiCGSTAB(p, torch.from_numpy(A.data[p.src].copy()), spmv=spmv, device=torch.device("cpu"))
+        b = torch.ones(p.n_own, dtype=torch.float64)
+        x, info, its = s.solve(b, rtol=0.0, atol=0.0, maxiter=5)
+        out.put((rank, x.tolist(), info, its))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_zero_threshold_exact_solve_ends_without_dividing_by_zero():
+    """With rtol = atol = 0 an exactly solved system (s = 0, t = 0) ends, with the exact
+    solution, as scipy's loop orders it: rho = rt.r = 0 at the next iteration (-10),
+    on every rank alike, without dividing by t.t = 0."""
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = 29700 + (os.getpid() + 900) % 1000
+    ps = [ctx.Process(target=_exact_worker, args=(r, 2, port, q)) for r in range(2)]
+    for p in ps:
+        p.start()
+    res = sorted(q.get(timeout=180) for _ in range(2))
+    for p in ps:
+        p.join(timeout=120)
+    for rank, x, info, its in res:
+        assert info == -10 and its == 1, (rank, info, its)
+        assert np.allclose(x, 0.5, rtol=0, atol=0), x
